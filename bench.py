@@ -1,0 +1,451 @@
+"""Benchmark: HashGraph build + intersect on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload large|large_zipf|small|capacity_lf1|capacity_lf05|capacity_lf2]
+
+One step = build table A from n keys resident in HBM, then intersect n query
+keys against it (pairs emitted).  Metric: build & intersect keys/s = n (keys
+per set) / (t_build + t_intersect).  Default workload (N=1): A = 2^28 uint64
+keys uniform (seed 3), queries = 2^28 uint64 keys with 25% drawn from A,
+n_buckets = 2^28.  Under torchrun every rank runs its own replica (weak
+scaling; no data-path collective); the step time is the max over ranks.
+
+Prints ONE JSON line on rank 0.  `--impl reference` times the CPU
+implementation of the same algorithm (the oracle's multithreaded build +
+probe, on all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "build & intersect keys/sec on 1 B200, % of HBM roofline; batched/served p50/p99"
+UNIT = "keys/s"
+
+WORKLOADS = {
+    # name: (key_bytes, n, n_buckets_fn, kind, seed_a, seed_q, overlap, with_index)
+    "large": (8, 1 << 28, lambda n: n, "uniform", 3, 30, 0.25, False),
+    "small": (4, 1 << 20, lambda n: n, "uniform", 1, 2, 0.5, False),
+    "capacity_lf1": (4, 1 << 30, lambda n: n, "uniform", 4, 40, 0.1, True),
+    "capacity_lf05": (4, 1 << 30, lambda n: 2 * n, "uniform", 4, 40, 0.1, True),
+    "capacity_lf2": (4, 1 << 30, lambda n: n // 2, "uniform", 4, 40, 0.1, True),
+}
+
+
+def describe(name, kb, n, B, kind, overlap, with_index):
+    kt = "u64" if kb == 8 else "u32"
+    lg = n.bit_length() - 1
+    if kind == "zipf":
+        q = f"queries 2^{lg} {kt} Zipf(1.1) over a 2^24-key universe (independent seed), count only"
+        a = f"A = 2^{lg} {kt} Zipf(1.1) over a 2^24-key universe"
+    else:
+        q = f"queries 2^{lg} {kt} with {int(overlap * 100)}% drawn from A, pairs emitted"
+        a = f"A = 2^{lg} {kt} uniform"
+    return (f"{name}: build {a}{' + index' if with_index else ''} into {B} buckets, then intersect "
+            f"{q}")
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas; barrier and max-over-ranks only)
+# ---------------------------------------------------------------------------
+def dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        if torch.cuda.is_available():
+            torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def algorithmic_bytes(phase, kb, n, nq, B, with_index, pairs):
+    """Bytes each kernel's role must move (its inputs read once, outputs
+    written once); the per-unit figures are stated in DESIGN.md."""
+    rec = kb + (4 if with_index else 0)
+    return {
+        "part_scatter": n * kb + n * rec,
+        "part_local": n * rec + n * rec + 4 * (B + 1),
+        "count": n * kb,
+        "scan": 8 * B,
+        "scatter": n * kb + n * rec,
+        "probe_emit": nq * kb + n * kb + 4 * (B + 1) + 8 * pairs,
+        "probe_count": nq * kb + n * kb + 4 * (B + 1),
+    }.get(phase)
+
+
+def run_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    import hashgraph_b200 as hg
+
+    kb, n, bfn, kind, seed_a, seed_q, overlap, with_index = WORKLOADS[args.workload]
+    n = args.n or n
+    B = bfn(n)
+    emit = kind != "zipf"
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    hg.lib()
+    # inputs, generated on the device (same definitions as the oracle)
+    if kind == "zipf":
+        cdf = hg.zipf_cdf(1 << 24, 1.1, device=dev)
+        a_keys = hg.gen_zipf(n, kb, cdf, seed_a)
+        q_keys = hg.gen_zipf(n, kb, cdf, seed_q)
+        del cdf
+    else:
+        a_keys = hg.gen_uniform(n, kb, seed_a, device=dev)
+        q_keys = hg.gen_overlap(n, a_keys, overlap, seed_q)
+    nq = q_keys.numel()
+    table = hg.Table(B, kb, with_index, n, dev)
+    pair_cap = nq if emit else 0
+    ws_n = hg.lib().hg_intersect_workspace_size
+    import ctypes
+    wsz = ctypes.c_size_t(0)
+    hg.check(ws_n(B, nq, kb, int(emit), ctypes.byref(wsz)))
+    ws = torch.empty(max(wsz.value, 1), dtype=torch.uint8, device=dev)
+    count = torch.zeros(1, dtype=torch.int64, device=dev)
+    pairs = torch.empty((max(pair_cap, 1), 2), dtype=torch.int32, device=dev) if emit else None
+    L = hg.lib()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+
+    def step(a_src, q_src):
+        table.rebuild(a_src, stream)
+        hg.check(L.hg_intersect_into(
+            ctypes.c_void_p(table.offsets.data_ptr()), ctypes.c_void_p(table.keys.data_ptr()),
+            ctypes.c_void_p(table.idx.data_ptr()) if table.idx is not None else None, table.n, B, kb,
+            ctypes.c_void_p(q_src.data_ptr()), nq, None,
+            ctypes.c_void_p(pairs.data_ptr()) if emit else None, pair_cap,
+            ctypes.c_void_p(count.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(), sptr),
+            "intersect")
+
+    for _ in range(args.warmup):
+        step(a_keys, q_keys)
+    torch.cuda.synchronize(dev)
+    n_matches = int(count.item())
+    if hg.device_error() != 0:
+        raise RuntimeError("device error during warm-up")
+
+    # ---- timed region: inputs resident in HBM (2^28 x 8 B per set >> 126 MB L2)
+    hg.profile_enable(True)
+    hg.profile_read()
+    clocks = ClockSampler(local)
+    launches0 = hg.launch_count()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps)]
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    time.sleep(0.3)
+    for k in range(args.steps):
+        ev[2 * k].record(stream)
+        step(a_keys, q_keys)
+        ev[2 * k + 1].record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    launches = hg.launch_count() - launches0
+    clk = clocks.stop()
+    phases = hg.profile_read()
+    hg.profile_enable(False)
+    step_ms = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
+    total_ms = sum(step_ms)
+    total_ms_max = max_over_ranks(total_ms, world)
+    if hg.device_error() != 0:
+        raise RuntimeError("device error during timed steps")
+
+    per_phase = {}
+    for name, ms in phases:
+        per_phase.setdefault(name, []).append(ms)
+    phase_avg = {k: sum(v) / len(v) for k, v in per_phase.items()}
+    phase_share = {k: sum(v) / max(total_ms, 1e-9) for k, v in per_phase.items()}
+    dom = max(per_phase, key=lambda k: sum(per_phase[k]))
+    peak, peak_kind = load_peaks()
+    alg = algorithmic_bytes(dom, kb, n, nq, B, with_index, n_matches)
+    achieved = alg / (phase_avg[dom] * 1e-3) / 1e9 if alg else None
+    build_ms = sum(v for k, v in phase_avg.items() if not k.startswith("probe"))
+    probe_ms = sum(v for k, v in phase_avg.items() if k.startswith("probe"))
+    # compulsory bytes of the step (build + probe form of intersect)
+    rec = kb + (4 if with_index else 0)
+    build_bytes = n * kb + n * rec + 4 * (B + 1)
+    isect_bytes = nq * kb + n * rec + 4 * (B + 1) + (8 * n_matches if emit else 0) + 8
+    step_s = total_ms / args.steps * 1e-3
+    value = sum_over_ranks(n * args.steps, world) / (total_ms_max * 1e-3)
+
+    # ---- end to end through the public API from pinned host buffers
+    e2e = None
+    if not args.skip_e2e:
+        h_a = torch.empty(a_keys.shape, dtype=a_keys.dtype, pin_memory=True)
+        h_q = torch.empty(q_keys.shape, dtype=q_keys.dtype, pin_memory=True)
+        h_a.copy_(a_keys)
+        h_q.copy_(q_keys)
+        h_count = torch.empty(1, dtype=torch.int64, pin_memory=True)
+        h_pairs = torch.empty((max(pair_cap, 1), 2), dtype=torch.int32, pin_memory=True) if emit else None
+        d_a = torch.empty_like(a_keys)
+        d_q = torch.empty_like(q_keys)
+        d2h = 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.steps):
+            d_a.copy_(h_a, non_blocking=True)
+            d_q.copy_(h_q, non_blocking=True)
+            step(d_a, d_q)
+            h_count.copy_(count, non_blocking=True)
+            stream.synchronize()
+            c = int(h_count.item())
+            d2h += 8
+            if emit and c:
+                h_pairs[:c].copy_(pairs[:c], non_blocking=True)
+                d2h += c * 8
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+        e2e = {"value": sum_over_ranks(n * args.steps, world) / (e2e_ms * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": int(a_keys.numel() * kb + q_keys.numel() * kb),
+               "d2h_bytes_per_step": int(d2h // args.steps)}
+        del h_a, h_q, h_pairs, d_a, d_q
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cpu = cpu_baseline(args.workload, n_sample=args.cpu_sample)
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64" if kb == 8 else "u32",
+        "data": "synthetic (seeded splitmix64 keys generated on the device; definitions shared with the oracle)",
+        "config": {"workload": describe(args.workload, kb, n, B, kind, overlap, with_index), "n": n, "nq": nq,
+                   "n_buckets": B, "key_bytes": kb, "with_index": with_index, "emit_pairs": emit,
+                   "matches": n_matches, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (each set %d MiB vs 126 MB L2); no flush" % (n * kb >> 20)},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "peak_source": peak_kind, "algorithmic_bytes": alg,
+                     "avg_launch_ms": phase_avg[dom]},
+        "step_roofline": {"compulsory_bytes": build_bytes + isect_bytes,
+                          "achieved_gbs": (build_bytes + isect_bytes) / step_s / 1e9,
+                          "frac_of_measured_hbm": (build_bytes + isect_bytes) / step_s / 1e9 / peak,
+                          "frac_of_8tbs": (build_bytes + isect_bytes) / step_s / 1e9 / 8000.0,
+                          "build_ms": build_ms, "intersect_ms": probe_ms,
+                          "build_keys_per_s": n / (build_ms * 1e-3) if build_ms else None,
+                          "build_frac_of_measured_hbm": build_bytes / (build_ms * 1e-3) / 1e9 / peak if build_ms else None,
+                          "intersect_frac_of_measured_hbm": isect_bytes / (probe_ms * 1e-3) / 1e9 / peak if probe_ms else None},
+        "phases_ms": phase_avg, "phase_share": phase_share,
+        "clocks": clk, "e2e": e2e, "gpu_launches": launches, "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline / reference arm
+# ---------------------------------------------------------------------------
+def cpu_run(workload, n_sample, repeats=3):
+    import numpy as np
+
+    import oracle
+    kb, n_full, bfn, kind, seed_a, seed_q, overlap, with_index = WORKLOADS[workload]
+    n = min(n_sample, n_full)
+    B = max(1, int(bfn(n_full) * n // n_full))
+    threads = oracle.max_threads()
+    if kind == "zipf":
+        cdf = oracle.zipf_cdf(1 << 24, 1.1)
+        a = oracle.gen_zipf(n, kb, cdf, seed_a)
+        q = oracle.gen_zipf(n, kb, cdf, seed_q)
+    else:
+        a = oracle.gen_uniform(n, kb, seed_a)
+        q = oracle.gen_overlap(n, a, overlap, seed_q)
+    cap = n if kind != "zipf" else 0
+    best = None
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        off, k, i = oracle.build(a, B, with_index, threads=threads)
+        t1 = time.perf_counter()
+        c, _ = oracle.intersect(off, k, i, q, pair_cap=cap, threads=threads)
+        t2 = time.perf_counter()
+        dt = t2 - t0
+        if best is None or dt < best[0]:
+            best = (dt, t1 - t0, t2 - t1, c)
+    return n, B, threads, best
+
+
+def cpu_baseline(workload, n_sample):
+    n, B, threads, (dt, tb, ti, c) = cpu_run(workload, n_sample)
+    return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} keys per set into {B} buckets (same generators and load factor), best of 3; "
+                      f"build {tb:.3f} s + intersect {ti:.3f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import oracle
+    kb, n, bfn, kind, seed_a, seed_q, overlap, with_index = WORKLOADS[args.workload]
+    n = args.n or n
+    B = bfn(n)
+    ns = min(args.cpu_sample, n)
+    times = []
+    cores = oracle.max_threads()
+    for k in range(args.warmup + args.steps):
+        nn, BB, cores, (dt, tb, ti, c) = cpu_run(args.workload, ns, repeats=1)
+        if k >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = ns * len(times) / total
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / len(times) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64" if kb == 8 else "u32",
+        "data": "synthetic (seeded splitmix64 keys; same generators as our arm)",
+        "config": {"workload": describe(args.workload, kb, n, B, kind, overlap, with_index), "n": n,
+                   "n_buckets": B, "key_bytes": kb, "with_index": with_index},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{ns} keys per set into {max(1, B * ns // n)} buckets per step "
+                                   "(the reference has no CPU build/intersect; this is the oracle's "
+                                   "multithreaded restatement of its algorithm)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="large")
+    ap.add_argument("--n", type=int, default=0, help="override keys per set (parity/profiling runs)")
+    ap.add_argument("--cpu-sample", type=int, default=1 << 26)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        run_reference(args, rank, world)
+        return
+    rank, world, local = dist_setup(args.gpus)
+    try:
+        run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

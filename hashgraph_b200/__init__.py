@@ -1,0 +1,230 @@
+"""hashgraph_b200 -- B200 (sm_100a) HashGraph build + intersect.
+
+A HashGraph is a hash table stored as CSR: ``offsets[n_buckets+1]`` and the
+keys binned by ``murmur3(low 32 bits of key) % n_buckets`` (optionally with the
+input position of every key).  The compute runs in hand-written CUDA kernels
+behind the C ABI of ``include/hashgraph_b200.h``; this module binds that ABI
+with ctypes and uses torch only to own device memory and streams.  The
+reference's C++ class API (SingleHashGraph / MultiHashGraph) is kept by the C++
+wrappers in ``include/hashgraph_b200/``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from ._capi import (ERR_DEVICE_TIMEOUT, ERR_PAIR_CAPACITY, HGError, build_library, check, lib,
+                    status_str)
+
+__all__ = [
+    "HGError", "Table", "build_library", "lib", "hash_keys", "intersect", "device_error",
+    "gen_uniform", "gen_overlap", "gen_zipf", "zipf_cdf", "PATH_AUTO", "PATH_DIRECT",
+    "PATH_PARTITIONED", "ERR_PAIR_CAPACITY", "ERR_DEVICE_TIMEOUT", "status_str",
+    "profile_enable", "profile_read", "launch_count",
+]
+
+PATH_AUTO, PATH_DIRECT, PATH_PARTITIONED = -1, 0, 1
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _key_bytes(t) -> int:
+    torch = _torch()
+    if t.dtype in (torch.int32, torch.uint32):
+        return 4
+    if t.dtype in (torch.int64, torch.uint64):
+        return 8
+    raise TypeError(f"keys must be a 32- or 64-bit integer tensor, got {t.dtype}")
+
+
+def _ptr(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _check_cuda(t, name):
+    if t is not None and not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if t is not None and not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+def hash_keys(keys) -> list:
+    """Host murmur3 (low 32 bits, seed 0) of python ints, via the C ABI."""
+    return [int(lib().hg_hash(int(k) & 0xFFFFFFFFFFFFFFFF)) for k in keys]
+
+
+def device_error(stream=None) -> int:
+    """Synchronise the stream and read/clear the device error word."""
+    code = ctypes.c_int32(0)
+    check(lib().hg_device_error(_stream(stream), ctypes.byref(code)), "hg_device_error")
+    return int(code.value)
+
+
+def profile_enable(on: bool = True) -> None:
+    """Per-phase CUDA-event timing inside the library (stream-ordered)."""
+    check(lib().hg_profile_enable(int(on)), "hg_profile_enable")
+
+
+def profile_read(cap: int = 4096) -> list:
+    """[(phase name, ms)] recorded since the last read, in launch order."""
+    names = (ctypes.c_char_p * cap)()
+    ms = (ctypes.c_float * cap)()
+    n = ctypes.c_int(0)
+    check(lib().hg_profile_read(cap, ctypes.byref(n), names, ms), "hg_profile_read")
+    return [(names[i].decode(), float(ms[i])) for i in range(min(n.value, cap))]
+
+
+def launch_count() -> int:
+    return int(lib().hg_launch_count())
+
+
+def build_workspace_bytes(n: int, key_bytes: int, n_buckets: int, with_index: bool,
+                          path: int = PATH_AUTO) -> int:
+    out = ctypes.c_size_t(0)
+    check(lib().hg_build_workspace_size_path(n, key_bytes, n_buckets, int(with_index), path,
+                                             ctypes.byref(out)), "workspace size")
+    return int(out.value)
+
+
+class Table:
+    """A built HashGraph whose arrays are torch CUDA tensors.
+
+    ``offsets`` (int32 storage of uint32 values, n_buckets+1), ``keys``
+    (int32/int64 storage of uint32/uint64 keys in CSR order) and ``idx``
+    (int32 storage of uint32 input positions, or None).
+    """
+
+    def __init__(self, n_buckets: int, key_bytes: int, with_index: bool, capacity: int,
+                 device=None, path: int = PATH_AUTO):
+        torch = _torch()
+        self.device = torch.device(device or "cuda")
+        self.n_buckets = int(n_buckets)
+        self.key_bytes = int(key_bytes)
+        self.with_index = bool(with_index)
+        self.capacity = int(capacity)
+        self.path = path
+        self.n = 0
+        kdt = torch.int32 if key_bytes == 4 else torch.int64
+        self.offsets = torch.empty(self.n_buckets + 1, dtype=torch.int32, device=self.device)
+        self.keys = torch.empty(max(self.capacity, 1), dtype=kdt, device=self.device)
+        self.idx = (torch.empty(max(self.capacity, 1), dtype=torch.int32, device=self.device)
+                    if with_index else None)
+        ws = build_workspace_bytes(self.capacity, key_bytes, n_buckets, with_index, path)
+        self.workspace = torch.empty(ws, dtype=torch.uint8, device=self.device)
+
+    @classmethod
+    def build(cls, keys, n_buckets: int, with_index: bool = False, path: int = PATH_AUTO,
+              stream=None) -> "Table":
+        _check_cuda(keys, "keys")
+        t = cls(n_buckets, _key_bytes(keys), with_index, keys.numel(), keys.device, path)
+        t.rebuild(keys, stream)
+        return t
+
+    def rebuild(self, keys, stream=None) -> "Table":
+        """Rebuild in place from `keys` (numel <= capacity), stream-ordered."""
+        _check_cuda(keys, "keys")
+        if _key_bytes(keys) != self.key_bytes:
+            raise HGError(-8, "key width differs from the table's")
+        n = keys.numel()
+        if n > self.capacity:
+            raise HGError(-6, f"{n} keys exceed capacity {self.capacity}")
+        check(lib().hg_build_into_path(
+            _ptr(keys), n, self.key_bytes, self.n_buckets, _ptr(self.offsets), _ptr(self.keys),
+            _ptr(self.idx), _ptr(self.workspace), self.workspace.numel(), self.path,
+            _stream(stream)), "hg_build_into")
+        self.n = n
+        return self
+
+    def view_keys(self):
+        return self.keys[: self.n]
+
+    def view_idx(self):
+        return None if self.idx is None else self.idx[: self.n]
+
+    def intersect(self, queries, query_idx=None, emit: bool = True, pair_cap: int | None = None,
+                  stream=None):
+        return intersect(self, queries, query_idx, emit, pair_cap, stream)
+
+
+def intersect(a: Table, queries, query_idx=None, emit: bool = True, pair_cap: int | None = None,
+              stream=None):
+    """Probe `queries` against table `a`.
+
+    Returns (count, pairs): `count` a 1-element int64 CUDA tensor holding the
+    exact number of matches; `pairs` an int32 CUDA tensor [pair_cap, 2] of
+    (a_ref, q_ref) or None when emit is False.  Only min(count, pair_cap)
+    rows are meaningful.
+    """
+    torch = _torch()
+    _check_cuda(queries, "queries")
+    if _key_bytes(queries) != a.key_bytes:
+        raise HGError(-8, "query key width differs from the table's")
+    nq = queries.numel()
+    if pair_cap is None:
+        pair_cap = nq
+    ws_n = ctypes.c_size_t(0)
+    check(lib().hg_intersect_workspace_size(a.n_buckets, nq, a.key_bytes, int(emit),
+                                            ctypes.byref(ws_n)), "intersect workspace")
+    ws = torch.empty(max(int(ws_n.value), 1), dtype=torch.uint8, device=a.device)
+    count = torch.empty(1, dtype=torch.int64, device=a.device)
+    pairs = torch.empty((max(int(pair_cap), 1), 2), dtype=torch.int32, device=a.device) if emit else None
+    check(lib().hg_intersect_into(
+        _ptr(a.offsets), _ptr(a.keys), _ptr(a.idx), a.n, a.n_buckets, a.key_bytes, _ptr(queries),
+        nq, _ptr(query_idx), _ptr(pairs), int(pair_cap) if emit else 0, _ptr(count), _ptr(ws),
+        ws.numel(), _stream(stream)), "hg_intersect_into")
+    return count, pairs
+
+
+# ---------------------------------------------------------------------------
+# Workload generators (device)
+# ---------------------------------------------------------------------------
+def _empty_keys(n, key_bytes, device):
+    torch = _torch()
+    return torch.empty(max(n, 1), dtype=torch.int32 if key_bytes == 4 else torch.int64,
+                       device=device)[:n]
+
+
+def gen_uniform(n: int, key_bytes: int, seed: int, device="cuda", stream=None):
+    out = _empty_keys(n, key_bytes, device)
+    check(lib().hg_gen_uniform(_ptr(out), n, key_bytes, seed, _stream(stream)), "hg_gen_uniform")
+    return out
+
+
+def overlap_count(n: int, n_a: int, frac: float) -> int:
+    """Number of keys drawn from A: round-half-away(frac * n), capped at n and n_a."""
+    import math
+    x = frac * n
+    m = int(math.floor(x + 0.5)) if x >= 0 else 0
+    return max(0, min(m, n, n_a))
+
+
+def gen_overlap(n: int, a_keys, frac: float, seed: int, stream=None):
+    kb = _key_bytes(a_keys)
+    out = _empty_keys(n, kb, a_keys.device)
+    m = overlap_count(n, a_keys.numel(), frac)
+    check(lib().hg_gen_overlap(_ptr(out), n, kb, _ptr(a_keys), a_keys.numel(), m, seed,
+                               _stream(stream)), "hg_gen_overlap")
+    return out
+
+
+def zipf_cdf(universe: int, s: float, device="cuda"):
+    import numpy as np
+    torch = _torch()
+    cdf = np.empty(universe, dtype=np.uint64)
+    check(lib().hg_zipf_cdf(cdf.ctypes.data_as(ctypes.c_void_p), universe, float(s)), "hg_zipf_cdf")
+    return torch.from_numpy(cdf.view(np.int64)).to(device)
+
+
+def gen_zipf(n: int, key_bytes: int, cdf, seed: int, stream=None):
+    out = _empty_keys(n, key_bytes, cdf.device)
+    check(lib().hg_gen_zipf(_ptr(out), n, key_bytes, _ptr(cdf), cdf.numel(), seed,
+                            _stream(stream)), "hg_gen_zipf")
+    return out

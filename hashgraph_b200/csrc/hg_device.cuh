@@ -1,0 +1,116 @@
+// hg_device.cuh -- device primitives shared by the HashGraph kernels (sm_100a).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda/atomic>
+
+#include "hashgraph_b200.h"
+
+namespace hg {
+
+constexpr unsigned FULL_MASK = 0xffffffffu;
+
+// murmur3_x86_32 of the key's low 4 bytes, seed 0.  The reference hashes
+// len = sizeof(int) bytes starting at &key (include/SingleHashGraphOperators.cuh:31-69,
+// include/MultiHashGraphDeviceOperators.cuh:37-73), so a 64-bit key contributes
+// only its low 32 bits; with len = 4 the function is one body block, the
+// length xor and the fmix32 finaliser.
+__host__ __device__ __forceinline__ uint32_t murmur3_low32(uint64_t key) {
+  uint32_t k = static_cast<uint32_t>(key);
+  k *= 0xcc9e2d51u;
+  k = (k << 15) | (k >> 17);
+  k *= 0x1b873593u;
+  uint32_t h = (k << 13) | (k >> 19);  // (seed 0) ^ k, rotated
+  h = h * 5u + 0xe6546b64u;
+  h ^= 4u;
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+
+// Exact `h % d` for 32-bit h and a divisor fixed per launch: the published
+// direct-remainder method of Lemire, Kaser and Kurz ("Faster remainder by
+// direct computation", 2019).  magic = floor((2^64-1)/d) + 1; the remainder is
+// the high 64 bits of (magic*h mod 2^64) * d.  d >= 2^32 (one bucket per hash
+// value or more) means bucket = h.
+struct BucketMap {
+  uint64_t magic;
+  uint32_t d;
+  uint32_t wide;  // 1 when n_buckets >= 2^32
+
+  static BucketMap make(uint64_t n_buckets) {
+    BucketMap m;
+    if (n_buckets >= (1ull << 32)) {
+      m.magic = 0; m.d = 0; m.wide = 1;
+    } else {
+      m.d = static_cast<uint32_t>(n_buckets);
+      m.magic = UINT64_MAX / m.d + 1;
+      m.wide = 0;
+    }
+    return m;
+  }
+  __host__ __device__ __forceinline__ uint32_t of_hash(uint32_t h) const {
+    if (wide) return h;
+#ifdef __CUDA_ARCH__
+    return static_cast<uint32_t>(__umul64hi(magic * h, static_cast<uint64_t>(d)));
+#else
+    return static_cast<uint32_t>((static_cast<__uint128_t>(magic * h) * d) >> 64);
+#endif
+  }
+  __host__ __device__ __forceinline__ uint32_t of_key(uint64_t key) const {
+    return of_hash(murmur3_low32(key));
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Device-side error word (one per device).  Kernels record the first failure
+// (a look-back wait that ran out, a pair buffer that was too small, ...); the
+// host reads and clears it with hg_device_error().  Defined here: the library
+// is one translation unit (hg_lib.cu).
+// ---------------------------------------------------------------------------
+__device__ int32_t g_device_error = 0;
+
+__device__ __forceinline__ void record_error(int32_t code) {
+  atomicCAS(reinterpret_cast<int*>(&g_device_error), 0, code);
+}
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Warp-aggregated atomicAdd(ctr + slot, 1): lanes whose `slot` agree elect one
+// leader (lowest lane) that adds the group size; every lane gets its own
+// position.  Lanes with valid == false take no part.  All 32 lanes of the warp
+// must call this together.
+template <typename CtrT>
+__device__ __forceinline__ CtrT warp_aggregated_inc(CtrT* ctr, uint32_t slot, bool valid) {
+  const uint64_t tag = valid ? static_cast<uint64_t>(slot) : (1ull << 40);
+  const unsigned peers = __match_any_sync(FULL_MASK, tag);
+  const unsigned leader = __ffs(peers) - 1;
+  const unsigned rank = __popc(peers & lanemask_lt());
+  CtrT base = 0;
+  if (valid && lane_id() == leader) base = atomicAdd(ctr + slot, static_cast<CtrT>(__popc(peers)));
+  base = __shfl_sync(FULL_MASK, base, leader);
+  return base + static_cast<CtrT>(rank);
+}
+
+// Warp-aggregated increment without a returned position (counting only).
+template <typename CtrT>
+__device__ __forceinline__ void warp_aggregated_count(CtrT* ctr, uint32_t slot, bool valid) {
+  const uint64_t tag = valid ? static_cast<uint64_t>(slot) : (1ull << 40);
+  const unsigned peers = __match_any_sync(FULL_MASK, tag);
+  if (valid && lane_id() == static_cast<unsigned>(__ffs(peers) - 1))
+    atomicAdd(ctr + slot, static_cast<CtrT>(__popc(peers)));
+}
+
+// Streaming loads for data touched once.
+template <typename T>
+__device__ __forceinline__ T ld_stream(const T* p) { return __ldcs(p); }
+
+}  // namespace hg

@@ -1,0 +1,7 @@
+// hg_lib.cu -- single translation unit of libhashgraph_b200.so.  The kernels
+// share one __device__ error word, so the sources are compiled together
+// rather than with relocatable device code.
+#include "hg_build.cu"
+#include "hg_probe.cu"
+#include "hg_gen.cu"
+#include "hg_api.cu"

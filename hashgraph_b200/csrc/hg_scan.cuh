@@ -1,0 +1,117 @@
+// hg_scan.cuh -- block scans and the decoupled look-back device-wide scan.
+//
+// Replaces the reference's cub::DeviceScan::ExclusiveSum over bucket counts
+// (src/SingleHashGraph.cu:167-173, src/MultiHashGraph.cu:353-366) and the
+// cub::DeviceReduce::Sum + ExclusiveSum pair over intersect counts
+// (src/MultiHashGraph.cu:691-715).  One pass: every tile publishes its
+// aggregate, then warp 0 walks back over predecessor tiles (32 at a time)
+// until it meets an inclusive prefix (Merrill & Garland, "Single-pass
+// Parallel Prefix Scan with Decoupled Look-back", 2016).  Tiles are numbered
+// by an atomic ticket so every predecessor has started.  The wait is bounded:
+// after LOOKBACK_SPIN_LIMIT polls the tile records HG_ERR_DEVICE_TIMEOUT and
+// returns instead of hanging.
+#pragma once
+#include "hg_device.cuh"
+
+namespace hg {
+
+// status word: [63:62] flag, [61:0] value
+constexpr uint64_t ST_AGGREGATE = 1ull << 62;
+constexpr uint64_t ST_PREFIX = 2ull << 62;
+constexpr uint64_t ST_VALUE = (1ull << 62) - 1;
+constexpr uint32_t LOOKBACK_SPIN_LIMIT = 1u << 22;
+
+__device__ __forceinline__ uint64_t ld_acquire(const uint64_t* p) {
+  cuda::atomic_ref<const unsigned long long, cuda::thread_scope_device> r(
+      *reinterpret_cast<const unsigned long long*>(p));
+  return r.load(cuda::memory_order_acquire);
+}
+__device__ __forceinline__ void st_release(uint64_t* p, uint64_t v) {
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(
+      *reinterpret_cast<unsigned long long*>(p));
+  r.store(v, cuda::memory_order_release);
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_MASK, v, o);
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_inclusive_scan(T v) {
+  const unsigned lane = lane_id();
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T u = __shfl_up_sync(FULL_MASK, v, o);
+    if (lane >= static_cast<unsigned>(o)) v += u;
+  }
+  return v;
+}
+
+// Exclusive scan of one value per thread across the block.  `scratch` holds
+// at least BLOCK/32 + 1 elements.  Returns the exclusive prefix; *total gets
+// the block sum.  Contains __syncthreads().
+template <int BLOCK, typename T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T* scratch, T* total) {
+  constexpr int NW = BLOCK / 32;
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+  T inc = warp_inclusive_scan(v);
+  if (lane == 31) scratch[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    T w = lane < NW ? scratch[lane] : T(0);
+    T wi = warp_inclusive_scan(w);
+    if (lane < NW) scratch[lane] = wi - w;
+    if (lane == NW - 1) scratch[NW] = wi;
+  }
+  __syncthreads();
+  T excl = scratch[warp] + inc - v;
+  *total = scratch[NW];
+  __syncthreads();
+  return excl;
+}
+
+// Decoupled look-back for `tile` with block aggregate `agg`.  Must be called
+// by all 32 lanes of exactly one warp.  Returns the exclusive prefix of the
+// tile (the same value in every lane) and publishes the inclusive prefix.
+__device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint64_t tile,
+                                                       uint64_t agg) {
+  const unsigned lane = lane_id();
+  if (tile == 0) {
+    if (lane == 0) st_release(status, ST_PREFIX | (agg & ST_VALUE));
+    return 0;
+  }
+  if (lane == 0) st_release(status + tile, ST_AGGREGATE | (agg & ST_VALUE));
+  uint64_t excl = 0;
+  int64_t pred = static_cast<int64_t>(tile) - 1;
+  uint32_t spins = 0;
+  unsigned sleep_ns = 8;
+  while (true) {
+    const int64_t j = pred - static_cast<int64_t>(lane);
+    uint64_t s = j >= 0 ? ld_acquire(status + j) : ST_PREFIX;
+    while (__any_sync(FULL_MASK, (s >> 62) == 0)) {
+      if (++spins > LOOKBACK_SPIN_LIMIT) {
+        record_error(HG_ERR_DEVICE_TIMEOUT);
+        return excl;
+      }
+      __nanosleep(sleep_ns);
+      if (sleep_ns < 256) sleep_ns <<= 1;
+      if ((s >> 62) == 0) s = ld_acquire(status + j);
+    }
+    const unsigned pfx = __ballot_sync(FULL_MASK, (s >> 62) == 2);
+    if (pfx) {
+      const unsigned first = __ffs(pfx) - 1;
+      uint64_t v = lane <= first ? (s & ST_VALUE) : 0;
+      excl += warp_sum(v);
+      break;
+    }
+    excl += warp_sum(s & ST_VALUE);
+    pred -= 32;
+  }
+  if (lane == 0) st_release(status + tile, ST_PREFIX | ((excl + agg) & ST_VALUE));
+  return excl;
+}
+
+}  // namespace hg

@@ -1,0 +1,196 @@
+/*
+ * hashgraph_b200.h -- C ABI of the B200 (sm_100a) HashGraph build + intersect path.
+ *
+ * A HashGraph is a hash table stored as a CSR graph: bucket b of a table with
+ * n_buckets buckets holds the keys whose murmur3_x86_32 hash (of the key's low
+ * 32 bits, seed 0) modulo n_buckets equals b.  The table is three SoA arrays in
+ * device memory:
+ *     offsets[n_buckets + 1]  uint32   bucket b is [offsets[b], offsets[b+1])
+ *     keys[n]                 uint32 or uint64 (key_bytes 4 or 8)
+ *     idx[n]                  uint32   input position of each key (optional)
+ *
+ * Conventions for every entry point:
+ *   - All device pointers are plain CUDA device addresses; no framework types.
+ *   - Calls are stream-ordered and asynchronous on `stream` (NULL = legacy
+ *     default stream) unless stated; the returned status covers argument
+ *     checks and launch errors.  Failures detected on the device (a bounded
+ *     wait that ran out, a pair buffer too small) are recorded in a per-device
+ *     error word read by hg_device_error().
+ *   - Nothing the caller owns is freed or resized.  Buffers the library
+ *     allocates belong to an hg_table and are released by hg_table_free().
+ *   - n < 2^32, 1 <= n_buckets <= 2^32.
+ *
+ * Reference interfaces replaced (alokpathy/hashgraph, path:line):
+ *   SingleHashGraph::build               src/SingleHashGraph.cu:216-232
+ *   MultiHashGraph::build (gpuCount = 1) src/MultiHashGraph.cu:408-629
+ *   MultiHashGraph::intersect            src/MultiHashGraph.cu:631-740
+ *   hash_murmur                          include/SingleHashGraphOperators.cuh:31-69
+ * The C++ classes of include/hashgraph_b200/ keep the reference's class API on
+ * top of these calls.
+ */
+#ifndef HASHGRAPH_B200_H
+#define HASHGRAPH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* hg_stream_t;
+typedef int32_t hg_status;
+
+#define HG_OK                   0
+#define HG_ERR_INVALID_ARGUMENT (-1)
+#define HG_ERR_CUDA             (-2)
+#define HG_ERR_OUT_OF_MEMORY    (-3)
+#define HG_ERR_PAIR_CAPACITY    (-4) /* more matches than pair_cap: count is exact, pairs truncated */
+#define HG_ERR_DEVICE_TIMEOUT   (-5) /* a bounded device-side wait gave up */
+#define HG_ERR_TOO_LARGE        (-6) /* n >= 2^32 or n_buckets > 2^32, or workspace too small */
+#define HG_ERR_NO_DEVICE        (-7)
+#define HG_ERR_KEY_WIDTH        (-8) /* key_bytes not 4 or 8, or tables of different key width */
+#define HG_ERR_BUCKET_MISMATCH  (-9) /* tables built with different n_buckets */
+
+/* Human-readable text for a status code (static storage). */
+const char* hg_status_str(hg_status status);
+
+/* Library version, e.g. "hashgraph_b200 0.1 sm_100a". */
+const char* hg_version(void);
+
+/* Host form of the bucket hash: murmur3_x86_32 of the low 32 bits of `key`,
+ * seed 0.  Replaces the __host__ side of hash_murmur
+ * (include/SingleHashGraphOperators.cuh:31-69). */
+uint32_t hg_hash(uint64_t key);
+
+/* Reads (then clears) the per-device error word after synchronising `stream`.
+ * *code receives HG_OK or the first HG_ERR_* recorded by a kernel. */
+hg_status hg_device_error(hg_stream_t stream, hg_status* code);
+
+/* ------------------------------------------------------------------------
+ * Build with caller-owned outputs and workspace.
+ * ---------------------------------------------------------------------- */
+
+/* Device scratch bytes hg_build_into needs for this shape. */
+hg_status hg_build_workspace_size(uint64_t n, int key_bytes, uint64_t n_buckets, int with_index,
+                                  size_t* bytes);
+
+/* Builds the CSR of `d_keys` (n keys of key_bytes each) into caller buffers.
+ * d_offsets: n_buckets+1 uint32; d_keys_out: n keys; d_idx_out: n uint32 or
+ * NULL (no index).  Replaces SingleHashGraph::build (src/SingleHashGraph.cu:216-232:
+ * hashValuesD, lrbCountHashD, scans, lrbRehashD, lrbCountHashGlobalD,
+ * lrbCopyToGraphD) and the per-GPU build of MultiHashGraph::build
+ * (src/MultiHashGraph.cu:408-629, lrbBuildMultiTable :303-375).  Bucket
+ * contents are the reference's; the order inside a bucket is unspecified,
+ * as in the reference. */
+hg_status hg_build_into(const void* d_keys, uint64_t n, int key_bytes, uint64_t n_buckets,
+                        uint32_t* d_offsets, void* d_keys_out, uint32_t* d_idx_out,
+                        void* d_workspace, size_t workspace_bytes, hg_stream_t stream);
+
+/* Same as hg_build_into / hg_build_workspace_size with the build path fixed:
+ * path 0 = direct (one count pass with global per-bucket counters, a scan,
+ * one scatter pass: the reference's non-LRB buildTable,
+ * src/SingleHashGraph.cu:187-213), 1 = partitioned (bucket-range partition
+ * pass, then one shared-memory build per partition: the role of the
+ * reference's LRB build, src/SingleHashGraph.cu:129-181, chosen there by
+ * #define LRB_BUILD, :64), -1 = planner's choice. */
+hg_status hg_build_workspace_size_path(uint64_t n, int key_bytes, uint64_t n_buckets, int with_index,
+                                       int path, size_t* bytes);
+hg_status hg_build_into_path(const void* d_keys, uint64_t n, int key_bytes, uint64_t n_buckets,
+                             uint32_t* d_offsets, void* d_keys_out, uint32_t* d_idx_out,
+                             void* d_workspace, size_t workspace_bytes, int path, hg_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Library-owned tables.
+ * ---------------------------------------------------------------------- */
+typedef struct hg_table hg_table;
+
+/* Allocates a table able to hold up to `capacity` keys in n_buckets buckets,
+ * with its build workspace.  No build happens. */
+hg_status hg_table_create(uint64_t capacity, int key_bytes, uint64_t n_buckets, int with_index,
+                          hg_table** out);
+
+/* (Re)builds `table` from n <= capacity device keys. */
+hg_status hg_table_build(hg_table* table, const void* d_keys, uint64_t n, hg_stream_t stream);
+
+/* hg_table_create(n, ...) + hg_table_build. */
+hg_status hg_build(const void* d_keys, uint64_t n, int key_bytes, uint64_t n_buckets,
+                   int with_index, hg_table** out, hg_stream_t stream);
+
+/* Device views of a built table (any output pointer may be NULL). */
+hg_status hg_table_view(const hg_table* table, const uint32_t** d_offsets, const void** d_keys,
+                        const uint32_t** d_idx, uint64_t* n, uint64_t* n_buckets, int* key_bytes);
+
+/* Bytes of device memory the table holds (arrays + workspace). */
+hg_status hg_table_device_bytes(const hg_table* table, size_t* bytes);
+
+void hg_table_free(hg_table* table);
+
+/* ------------------------------------------------------------------------
+ * Intersect.  Multiset join on equal keys, bucket by bucket, as
+ * MultiHashGraph::intersect (src/MultiHashGraph.cu:631-740, simpleIntersect
+ * include/MultiHashGraphDeviceOperators.cuh:513-543): every (a, q) with
+ * key(a) == key(q) is one match, so duplicates multiply.
+ *
+ * Pairs are written as uint32 [a_ref, q_ref] couples into d_pairs[2*pair_cap]:
+ *   a_ref = A's idx[j] when A has an index, else the CSR position j in A;
+ *   q_ref = d_query_idx[i] when given, else the query position i.
+ * *d_count (uint64, device) receives the exact number of matches even when it
+ * exceeds pair_cap; then only pair_cap pairs are written and the device error
+ * word records HG_ERR_PAIR_CAPACITY.  d_pairs == NULL counts only.
+ * ---------------------------------------------------------------------- */
+
+/* Device scratch bytes for hg_intersect_into. */
+hg_status hg_intersect_workspace_size(uint64_t n_buckets, uint64_t nq, int key_bytes,
+                                      int emit_pairs, size_t* bytes);
+
+/* Probes nq query keys (same key width as A) against table A. */
+hg_status hg_intersect_into(const uint32_t* d_a_offsets, const void* d_a_keys,
+                            const uint32_t* d_a_idx, uint64_t n_a, uint64_t n_buckets,
+                            int key_bytes, const void* d_query, uint64_t nq,
+                            const uint32_t* d_query_idx, uint32_t* d_pairs, uint64_t pair_cap,
+                            unsigned long long* d_count, void* d_workspace,
+                            size_t workspace_bytes, hg_stream_t stream);
+
+/* Same, on an hg_table; allocates its scratch per call (stream-ordered). */
+hg_status hg_intersect(const hg_table* a, const void* d_query, uint64_t nq,
+                       const uint32_t* d_query_idx, uint32_t* d_pairs, uint64_t pair_cap,
+                       unsigned long long* d_count, hg_stream_t stream);
+
+/* Table-vs-table form of MultiHashGraph::intersect: the keys of B (in B's CSR
+ * order) are the queries; q_ref is B's idx (or B's CSR position). */
+hg_status hg_intersect_tables(const hg_table* a, const hg_table* b, uint32_t* d_pairs,
+                              uint64_t pair_cap, unsigned long long* d_count, hg_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Instrumentation (no counterpart in the reference, which prints host wall
+ * times under HOST_PROFILE, src/MultiHashGraph.cu:55-57,431-615).
+ * ---------------------------------------------------------------------- */
+/* Turns per-phase CUDA-event timing on/off and drops unread records.  Events
+ * are recorded on the launching stream; no host synchronisation is added. */
+hg_status hg_profile_enable(int on);
+/* Waits for and returns up to `cap` recorded phases (name, milliseconds) in
+ * launch order; *count gets the number recorded.  Clears the records. */
+hg_status hg_profile_read(int cap, int* count, const char** names, float* ms);
+/* Kernels this library has launched in this process. */
+unsigned long long hg_launch_count(void);
+
+/* ------------------------------------------------------------------------
+ * Seeded workload generators (device), matching the oracle's definitions.
+ * ---------------------------------------------------------------------- */
+/* key[i] = splitmix-stream(seed, 0, i) (top 32 bits for 4-byte keys). */
+hg_status hg_gen_uniform(void* d_out, uint64_t n, int key_bytes, uint64_t seed, hg_stream_t stream);
+/* n keys: n_from_a of them distinct draws from d_a (n_a keys), the rest fresh,
+ * shuffled by a seeded bijection. */
+hg_status hg_gen_overlap(void* d_out, uint64_t n, int key_bytes, const void* d_a, uint64_t n_a,
+                         uint64_t n_from_a, uint64_t seed, hg_stream_t stream);
+/* Zipf draws through a u64 fixed-point CDF table (universe entries, device). */
+hg_status hg_gen_zipf(void* d_out, uint64_t n, int key_bytes, const uint64_t* d_cdf,
+                      uint64_t universe, uint64_t seed, hg_stream_t stream);
+/* Host: fills cdf[universe] for Zipf(s). */
+hg_status hg_zipf_cdf(uint64_t* cdf, uint64_t universe, double s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HASHGRAPH_B200_H */

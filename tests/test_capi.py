@@ -1,0 +1,91 @@
+"""CPU checks of the C-ABI library: it loads, exports every symbol the headers
+declare, and its host-side logic (hash, argument checks, planning) behaves.
+No call here launches device work."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "hashgraph_b200.h")
+
+
+def declared_functions(path):
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(hg_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+@pytest.fixture(scope="module")
+def capi():
+    from hashgraph_b200 import _capi
+    _capi.build_library()
+    return _capi
+
+
+def test_library_exports_every_declared_symbol(capi):
+    names = declared_functions(HEADER)
+    assert len(names) >= 20
+    L = ctypes.CDLL(capi.LIB_PATH)
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    # and the binding declares a signature for each
+    assert set(names) <= set(capi.SIGNATURES), set(names) - set(capi.SIGNATURES)
+
+
+def test_host_hash_matches_oracle(capi):
+    L = capi.lib()
+    keys = oracle.gen_uniform(2048, 8, 77)
+    ours = np.array([L.hg_hash(int(k)) for k in keys], dtype=np.uint32)
+    np.testing.assert_array_equal(ours, oracle.murmur(keys))
+    assert L.hg_hash(0) == 0x2362F9DE
+
+
+def test_status_strings(capi):
+    L = capi.lib()
+    for code in capi.STATUS_NAMES:
+        assert L.hg_status_str(code)
+    assert b"sm_100a" in L.hg_version()
+
+
+def test_argument_checks_without_device(capi):
+    L = capi.lib()
+    out = ctypes.c_size_t(0)
+    assert L.hg_build_workspace_size(1000, 3, 1000, 0, ctypes.byref(out)) == -8
+    assert L.hg_build_workspace_size(1000, 4, 0, 0, ctypes.byref(out)) == -1
+    assert L.hg_build_workspace_size(1 << 32, 4, 1000, 0, ctypes.byref(out)) == -6
+    assert L.hg_build_workspace_size(1000, 4, (1 << 32) + 1, 0, ctypes.byref(out)) == -6
+    assert L.hg_build_workspace_size(1000, 4, 1000, 0, None) == -1
+    assert L.hg_intersect_workspace_size(1000, 10, 5, 1, ctypes.byref(out)) == -8
+    assert L.hg_build_into(None, 10, 8, 10, None, None, None, None, 0, None) == -1
+    assert L.hg_table_create(10, 8, 10, 0, None) == -1
+    assert L.hg_zipf_cdf(None, 10, 1.1) == -1
+
+
+def test_workspace_plans(capi):
+    L = capi.lib()
+    out = ctypes.c_size_t(0)
+    # direct path: only scan status and flags
+    assert L.hg_build_workspace_size_path(1 << 20, 4, 1 << 20, 0, 0, ctypes.byref(out)) == 0
+    direct = out.value
+    assert direct < (1 << 20)
+    # partitioned path: partition buffers hold every key (+ index) with slack
+    assert L.hg_build_workspace_size_path(1 << 20, 4, 1 << 20, 1, 1, ctypes.byref(out)) == 0
+    part = out.value
+    assert (1 << 20) * 8 <= part < (1 << 20) * 8 * 1.5
+    # the planner picks the partitioned path for a 2^28 x u64 table
+    assert L.hg_build_workspace_size(1 << 28, 8, 1 << 28, 0, ctypes.byref(out)) == 0
+    assert out.value >= (1 << 28) * 8
+
+
+def test_zipf_cdf_matches_oracle(capi):
+    L = capi.lib()
+    U = 1 << 12
+    ours = np.empty(U, dtype=np.uint64)
+    assert L.hg_zipf_cdf(ours.ctypes.data_as(ctypes.c_void_p), U, 1.1) == 0
+    np.testing.assert_array_equal(ours, oracle.zipf_cdf(U, 1.1))

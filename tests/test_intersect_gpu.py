@@ -1,0 +1,129 @@
+"""GPU parity of intersect (probe + count + pair emission) against the oracle.
+
+The bar: the match count is exact, and the sorted (a_ref, q_ref) pairs equal
+the oracle's sorted pairs (the reference's multiset-join semantics)."""
+import numpy as np
+import pytest
+
+import oracle
+from tests.conftest import from_np_u, to_np_u
+
+pytestmark = pytest.mark.gpu
+
+
+def _sorted_pairs(p):
+    p = np.asarray(p, dtype=np.uint32).reshape(-1, 2).astype(np.uint64)
+    return np.sort(p[:, 0] << np.uint64(32) | p[:, 1])
+
+
+def _oracle_pairs(a_keys_np, B, with_index, q_np):
+    off, k, i = oracle.build(a_keys_np, B, True)
+    c, pairs = oracle.intersect(off, k, i, q_np, pair_cap=max(q_np.size * 64, 1))
+    return c, pairs
+
+
+@pytest.mark.parametrize("path", [0, 1])
+@pytest.mark.parametrize("kb", [4, 8])
+@pytest.mark.parametrize("na,nq,B,frac", [(1 << 16, 1 << 16, 1 << 16, 0.5), (70_001, 30_000, 12_345, 0.25),
+                                          (5000, 90_000, 1 << 14, 1.0), (1 << 15, 1 << 15, 1, 0.1)])
+def test_intersect_pairs_with_index(hg, path, kb, na, nq, B, frac):
+    a = oracle.gen_uniform(na, kb, 31 + na)
+    q = oracle.gen_overlap(nq, a, frac, 37 + nq)
+    t = hg.Table.build(from_np_u(a), B, with_index=True, path=path)
+    count, pairs = t.intersect(from_np_u(q), pair_cap=nq * 2)
+    c = int(count.item())
+    oc, op = _oracle_pairs(a, B, True, q)
+    assert c == oc
+    np.testing.assert_array_equal(_sorted_pairs(to_np_u(pairs[:c], 4)), _sorted_pairs(op))
+    assert hg.device_error() == 0
+
+
+@pytest.mark.parametrize("kb", [4, 8])
+def test_intersect_without_index_refers_to_csr_positions(hg, kb):
+    a = oracle.gen_uniform(40_000, kb, 5)
+    q = oracle.gen_overlap(40_000, a, 0.5, 6)
+    t = hg.Table.build(from_np_u(a), 40_000, with_index=False)
+    count, pairs = t.intersect(from_np_u(q))
+    c = int(count.item())
+    p = to_np_u(pairs[:c], 4)
+    csr_keys = to_np_u(t.view_keys(), kb)
+    # a_ref is a CSR position in A holding the query's key
+    assert np.all(csr_keys[p[:, 0]] == q[p[:, 1]])
+    oc, op = _oracle_pairs(a, 40_000, True, q)
+    assert c == oc
+    np.testing.assert_array_equal(np.sort(q[p[:, 1]]), np.sort(q[op[:, 1]]))
+
+
+def test_intersect_duplicates_multiply(hg):
+    """Multiset join: k copies in A and m in the queries give k*m matches."""
+    a = (oracle.gen_uniform(30_000, 8, 8) % np.uint64(200)).astype(np.uint64)
+    q = (oracle.gen_uniform(20_000, 8, 9) % np.uint64(300)).astype(np.uint64)
+    t = hg.Table.build(from_np_u(a), 4096, with_index=True)
+    expect = oracle.join_count(a, q)
+    count, _ = t.intersect(from_np_u(q), emit=False)
+    assert int(count.item()) == expect
+    count, pairs = t.intersect(from_np_u(q), pair_cap=expect)
+    assert int(count.item()) == expect
+    oc, op = _oracle_pairs(a, 4096, True, q)
+    np.testing.assert_array_equal(_sorted_pairs(to_np_u(pairs, 4)), _sorted_pairs(op))
+
+
+def test_intersect_pair_capacity(hg):
+    """Too small a pair buffer: exact count, pairs truncated, error recorded."""
+    a = oracle.gen_uniform(1 << 15, 4, 10)
+    q = oracle.gen_overlap(1 << 15, a, 0.75, 11)
+    t = hg.Table.build(from_np_u(a), 1 << 15, with_index=True)
+    full, _ = t.intersect(from_np_u(q), emit=False)
+    c = int(full.item())
+    assert hg.device_error() == 0
+    cap = c // 3
+    count, pairs = t.intersect(from_np_u(q), pair_cap=cap)
+    assert int(count.item()) == c
+    assert hg.device_error() == hg.ERR_PAIR_CAPACITY
+    p = to_np_u(pairs[:cap], 4)
+    assert np.all(a[p[:, 0]] == q[p[:, 1]])
+    assert hg.device_error() == 0
+
+
+def test_intersect_empty_inputs(hg):
+    import torch
+    a = oracle.gen_uniform(1000, 8, 1)
+    t = hg.Table.build(from_np_u(a), 1000, with_index=True)
+    count, _ = t.intersect(torch.empty(0, dtype=torch.int64, device="cuda"))
+    assert int(count.item()) == 0
+    t0 = hg.Table.build(torch.empty(0, dtype=torch.int64, device="cuda"), 1000, with_index=True)
+    count, _ = t0.intersect(from_np_u(a))
+    assert int(count.item()) == 0
+
+
+def test_intersect_tables_matches_reference_semantics(hg):
+    """Table-vs-table form (MultiHashGraph::intersect): B's CSR keys are the
+    queries; the matched-key multiset equals the reference's output of B keys."""
+    import ctypes
+
+    import torch
+    L = hg.lib()
+    a = oracle.gen_uniform(50_000, 8, 21)
+    b = oracle.gen_overlap(60_000, a, 0.5, 22)
+    da, db = from_np_u(a), from_np_u(b)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ta, tb = ctypes.c_void_p(), ctypes.c_void_p()
+    assert L.hg_build(ctypes.c_void_p(da.data_ptr()), a.size, 8, 1 << 16, 0, ctypes.byref(ta), s) == 0
+    assert L.hg_build(ctypes.c_void_p(db.data_ptr()), b.size, 8, 1 << 16, 1, ctypes.byref(tb), s) == 0
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    pairs = torch.empty((b.size, 2), dtype=torch.int32, device="cuda")
+    assert L.hg_intersect_tables(ta, tb, ctypes.c_void_p(pairs.data_ptr()), b.size,
+                                 ctypes.c_void_p(cnt.data_ptr()), s) == 0
+    c = int(cnt.item())
+    assert c == oracle.join_count(a, b)
+    p = to_np_u(pairs[:c], 4)
+    # A's 64-bit keys are distinct, so each B key matches once if it is in A;
+    # q_ref is B's input position because B was built with an index
+    assert np.unique(a).size == a.size
+    np.testing.assert_array_equal(np.sort(b[p[:, 1]]), np.sort(b[np.isin(b, a)]))
+    # mismatched bucket counts are refused, as the reference refuses them
+    tc = ctypes.c_void_p()
+    assert L.hg_build(ctypes.c_void_p(da.data_ptr()), a.size, 8, 1000, 0, ctypes.byref(tc), s) == 0
+    assert L.hg_intersect_tables(ta, tc, None, 0, ctypes.c_void_p(cnt.data_ptr()), s) == -9
+    for t in (ta, tb, tc):
+        L.hg_table_free(t)

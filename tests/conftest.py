@@ -47,3 +47,17 @@ def from_np_u(a, device="cuda"):
     if a.dtype == np.uint64:
         return torch.from_numpy(a.view(np.int64).copy()).to(device)
     raise TypeError(a.dtype)
+
+
+def device_array(ptr: int, count: int, np_dtype):
+    """Copy `count` elements at device address `ptr` to a numpy array (via
+    __cuda_array_interface__, so torch never owns the memory)."""
+    import torch
+
+    class _View:
+        pass
+
+    v = _View()
+    v.__cuda_array_interface__ = {"shape": (count,), "typestr": np.dtype(np_dtype).str,
+                                  "data": (int(ptr), False), "version": 2}
+    return torch.as_tensor(v, device="cuda").cpu().numpy().copy()

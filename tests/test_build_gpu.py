@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import oracle
-from tests.conftest import from_np_u, to_np_u
+from tests.conftest import device_array, from_np_u, to_np_u
 
 pytestmark = pytest.mark.gpu
 
@@ -108,12 +108,9 @@ def test_library_owned_table_api(hg):
                            ctypes.byref(B), ctypes.byref(kb)) == 0
     assert (n.value, B.value, kb.value) == (keys.size, 50_000, 8)
     torch.cuda.synchronize()
-    off = np.empty(50_001, np.uint32)
-    got_k = np.empty(keys.size, np.uint64)
-    got_i = np.empty(keys.size, np.uint32)
-    cudart = torch.cuda.cudart()
-    for host, dev, nbytes in ((off, po, off.nbytes), (got_k, pk, got_k.nbytes), (got_i, pi, got_i.nbytes)):
-        assert cudart.cudaMemcpy(host.ctypes.data, dev.value, nbytes, 2) == 0  # device-to-host
+    off = device_array(po.value, 50_001, np.uint32)
+    got_k = device_array(pk.value, keys.size, np.uint64)
+    got_i = device_array(pi.value, keys.size, np.uint32)
     o_off, o_k, o_i = oracle.build(keys, 50_000, True)
     np.testing.assert_array_equal(off, o_off)
     kc, ic = oracle.canonicalize(off, got_k, got_i)

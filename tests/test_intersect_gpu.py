@@ -18,7 +18,8 @@ def _sorted_pairs(p):
 
 def _oracle_pairs(a_keys_np, B, with_index, q_np):
     off, k, i = oracle.build(a_keys_np, B, True)
-    c, pairs = oracle.intersect(off, k, i, q_np, pair_cap=max(q_np.size * 64, 1))
+    c, _ = oracle.intersect(off, k, i, q_np, pair_cap=0)
+    c, pairs = oracle.intersect(off, k, i, q_np, pair_cap=max(c, 1))
     return c, pairs
 
 

@@ -172,18 +172,30 @@ def sum_over_ranks(x, world):
 # our arm
 # ---------------------------------------------------------------------------
 def algorithmic_bytes(phase, kb, n, nq, B, with_index, pairs):
-    """Bytes each kernel's role must move (its inputs read once, outputs
+    """Bytes each kernel's role must move (its inputs read once, its outputs
     written once); the per-unit figures are stated in DESIGN.md."""
     rec = kb + (4 if with_index else 0)
+    qrec = kb + 4
     return {
-        "part_scatter": n * kb + n * rec,
-        "part_local": n * rec + n * rec + 4 * (B + 1),
+        # build
+        "multisplit": n * kb + n * rec,
+        "split": 2 * n * rec,
+        "fine_build": 2 * n * rec + 4 * (B + 1),
         "count": n * kb,
         "scan": 8 * B,
         "scatter": n * kb + n * rec,
-        "probe_emit": nq * kb + n * kb + 4 * (B + 1) + 8 * pairs,
-        "probe_count": nq * kb + n * kb + 4 * (B + 1),
+        # intersect
+        "probe_multisplit": nq * kb + nq * qrec,
+        "probe_split": 2 * nq * qrec,
+        "fine_probe_emit": nq * qrec + n * rec + 4 * (B + 1) + 8 * pairs,
+        "fine_probe_count": nq * qrec + n * rec + 4 * (B + 1),
+        "probe_emit": nq * kb + n * rec + 4 * (B + 1) + 8 * pairs,
+        "probe_count": nq * kb + n * rec + 4 * (B + 1),
     }.get(phase)
+
+
+def is_probe_phase(name):
+    return "probe" in name
 
 
 def run_ours(args, rank, world, local):
@@ -211,11 +223,9 @@ def run_ours(args, rank, world, local):
     nq = q_keys.numel()
     table = hg.Table(B, kb, with_index, n, dev)
     pair_cap = nq if emit else 0
-    ws_n = hg.lib().hg_intersect_workspace_size
     import ctypes
-    wsz = ctypes.c_size_t(0)
-    hg.check(ws_n(B, nq, kb, int(emit), ctypes.byref(wsz)))
-    ws = torch.empty(max(wsz.value, 1), dtype=torch.uint8, device=dev)
+    table.n = n  # the probe plan depends on the table's size
+    ws = torch.empty(max(hg.intersect_workspace_bytes(table, nq, emit), 1), dtype=torch.uint8, device=dev)
     count = torch.zeros(1, dtype=torch.int64, device=dev)
     pairs = torch.empty((max(pair_cap, 1), 2), dtype=torch.int32, device=dev) if emit else None
     L = hg.lib()
@@ -273,8 +283,8 @@ def run_ours(args, rank, world, local):
     peak, peak_kind = load_peaks()
     alg = algorithmic_bytes(dom, kb, n, nq, B, with_index, n_matches)
     achieved = alg / (phase_avg[dom] * 1e-3) / 1e9 if alg else None
-    build_ms = sum(v for k, v in phase_avg.items() if not k.startswith("probe"))
-    probe_ms = sum(v for k, v in phase_avg.items() if k.startswith("probe"))
+    build_ms = sum(sum(v) for k, v in per_phase.items() if not is_probe_phase(k)) / args.steps
+    probe_ms = sum(sum(v) for k, v in per_phase.items() if is_probe_phase(k)) / args.steps
     # compulsory bytes of the step (build + probe form of intersect)
     rec = kb + (4 if with_index else 0)
     build_bytes = n * kb + n * rec + 4 * (B + 1)

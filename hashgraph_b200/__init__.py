@@ -150,12 +150,19 @@ class Table:
         return None if self.idx is None else self.idx[: self.n]
 
     def intersect(self, queries, query_idx=None, emit: bool = True, pair_cap: int | None = None,
-                  stream=None):
-        return intersect(self, queries, query_idx, emit, pair_cap, stream)
+                  stream=None, path: int = PATH_AUTO):
+        return intersect(self, queries, query_idx, emit, pair_cap, stream, path)
+
+
+def intersect_workspace_bytes(a: "Table", nq: int, emit: bool, path: int = PATH_AUTO) -> int:
+    out = ctypes.c_size_t(0)
+    check(lib().hg_intersect_workspace_size_path(a.n, int(a.with_index), a.n_buckets, nq, a.key_bytes,
+                                                 int(emit), path, ctypes.byref(out)), "intersect workspace")
+    return int(out.value)
 
 
 def intersect(a: Table, queries, query_idx=None, emit: bool = True, pair_cap: int | None = None,
-              stream=None):
+              stream=None, path: int = PATH_AUTO):
     """Probe `queries` against table `a`.
 
     Returns (count, pairs): `count` a 1-element int64 CUDA tensor holding the
@@ -170,16 +177,14 @@ def intersect(a: Table, queries, query_idx=None, emit: bool = True, pair_cap: in
     nq = queries.numel()
     if pair_cap is None:
         pair_cap = nq
-    ws_n = ctypes.c_size_t(0)
-    check(lib().hg_intersect_workspace_size(a.n_buckets, nq, a.key_bytes, int(emit),
-                                            ctypes.byref(ws_n)), "intersect workspace")
-    ws = torch.empty(max(int(ws_n.value), 1), dtype=torch.uint8, device=a.device)
+    ws = torch.empty(max(intersect_workspace_bytes(a, nq, emit, path), 1), dtype=torch.uint8,
+                     device=a.device)
     count = torch.empty(1, dtype=torch.int64, device=a.device)
     pairs = torch.empty((max(int(pair_cap), 1), 2), dtype=torch.int32, device=a.device) if emit else None
-    check(lib().hg_intersect_into(
+    check(lib().hg_intersect_into_path(
         _ptr(a.offsets), _ptr(a.keys), _ptr(a.idx), a.n, a.n_buckets, a.key_bytes, _ptr(queries),
         nq, _ptr(query_idx), _ptr(pairs), int(pair_cap) if emit else 0, _ptr(count), _ptr(ws),
-        ws.numel(), _stream(stream)), "hg_intersect_into")
+        ws.numel(), path, _stream(stream)), "hg_intersect_into")
     return count, pairs
 
 

@@ -41,6 +41,7 @@ _pp = ctypes.POINTER(ctypes.c_void_p)
 SIGNATURES = {
     "hg_status_str": (ctypes.c_char_p, [_i32]),
     "hg_version": (ctypes.c_char_p, []),
+    "hg_last_error": (ctypes.c_char_p, []),
     "hg_hash": (ctypes.c_uint32, [_u64]),
     "hg_device_error": (_i32, [_p, ctypes.POINTER(_i32)]),
     "hg_build_workspace_size": (_i32, [_u64, _int, _u64, _int, ctypes.POINTER(_sz)]),
@@ -54,7 +55,11 @@ SIGNATURES = {
                              ctypes.POINTER(_int)]),
     "hg_table_device_bytes": (_i32, [_p, ctypes.POINTER(_sz)]),
     "hg_table_free": (None, [_p]),
-    "hg_intersect_workspace_size": (_i32, [_u64, _u64, _int, _int, ctypes.POINTER(_sz)]),
+    "hg_intersect_workspace_size": (_i32, [_u64, _int, _u64, _u64, _int, _int, ctypes.POINTER(_sz)]),
+    "hg_intersect_workspace_size_path": (_i32, [_u64, _int, _u64, _u64, _int, _int, _int,
+                                                ctypes.POINTER(_sz)]),
+    "hg_intersect_into_path": (_i32, [_p, _p, _p, _u64, _u64, _int, _p, _u64, _p, _p, _u64, _p, _p,
+                                      _sz, _int, _p]),
     "hg_intersect_into": (_i32, [_p, _p, _p, _u64, _u64, _int, _p, _u64, _p, _p, _u64, _p, _p,
                                  _sz, _p]),
     "hg_intersect": (_i32, [_p, _p, _u64, _p, _p, _u64, _p, _p]),
@@ -105,7 +110,12 @@ def lib() -> ctypes.CDLL:
 
 def check(status: int, what: str = "") -> None:
     if status != HG_OK:
-        raise HGError(status, what)
+        detail = ""
+        try:
+            detail = lib().hg_last_error().decode()
+        except Exception:
+            pass
+        raise HGError(status, f"{what} [{detail}]" if detail else what)
 
 
 def status_str(status: int) -> str:

@@ -47,6 +47,8 @@ extern "C" const char* hg_status_str(hg_status s) {
 
 extern "C" const char* hg_version(void) { return "hashgraph_b200 0.1 sm_100a"; }
 
+extern "C" const char* hg_last_error(void) { return last_error_buffer(); }
+
 extern "C" uint32_t hg_hash(uint64_t key) { return murmur3_low32(key); }
 
 extern "C" hg_status hg_device_error(hg_stream_t stream, hg_status* code) {
@@ -221,14 +223,38 @@ extern "C" hg_status hg_table_device_bytes(const hg_table* t, size_t* bytes) {
 // ---------------------------------------------------------------------------
 // Intersect
 // ---------------------------------------------------------------------------
-extern "C" hg_status hg_intersect_workspace_size(uint64_t n_buckets, uint64_t nq, int key_bytes, int emit_pairs,
-                                                 size_t* bytes) {
+extern "C" hg_status hg_intersect_workspace_size(uint64_t n_a, int a_has_index, uint64_t n_buckets, uint64_t nq,
+                                                 int key_bytes, int emit_pairs, size_t* bytes) {
   if (!bytes) return HG_ERR_INVALID_ARGUMENT;
   ProbePlan plan;
-  hg_status st = plan_probe(n_buckets, nq, key_bytes, emit_pairs != 0, &plan);
+  hg_status st = plan_probe(n_a, a_has_index != 0, n_buckets, nq, key_bytes, emit_pairs != 0, &plan);
   if (st != HG_OK) return st;
   *bytes = plan.total;
   return HG_OK;
+}
+
+extern "C" hg_status hg_intersect_workspace_size_path(uint64_t n_a, int a_has_index, uint64_t n_buckets, uint64_t nq,
+                                                      int key_bytes, int emit_pairs, int path, size_t* bytes) {
+  if (!bytes) return HG_ERR_INVALID_ARGUMENT;
+  ProbePlan plan;
+  hg_status st = plan_probe(n_a, a_has_index != 0, n_buckets, nq, key_bytes, emit_pairs != 0, &plan, path);
+  if (st != HG_OK) return st;
+  *bytes = plan.total;
+  return HG_OK;
+}
+
+extern "C" hg_status hg_intersect_into_path(const uint32_t* d_a_offsets, const void* d_a_keys, const uint32_t* d_a_idx,
+                                            uint64_t n_a, uint64_t n_buckets, int key_bytes, const void* d_query,
+                                            uint64_t nq, const uint32_t* d_query_idx, uint32_t* d_pairs,
+                                            uint64_t pair_cap, unsigned long long* d_count, void* d_workspace,
+                                            size_t workspace_bytes, int path, hg_stream_t stream) {
+  if (!d_a_offsets || !d_count || (nq > 0 && !d_query) || (n_a > 0 && !d_a_keys)) return HG_ERR_INVALID_ARGUMENT;
+  ProbePlan plan;
+  hg_status st = plan_probe(n_a, d_a_idx != nullptr, n_buckets, nq, key_bytes, d_pairs != nullptr, &plan, path);
+  if (st != HG_OK) return st;
+  if (workspace_bytes < plan.total || (!d_workspace && plan.total)) return HG_ERR_TOO_LARGE;
+  return launch_probe(plan, d_a_offsets, d_a_keys, d_a_idx, d_query, d_query_idx, d_pairs, pair_cap, d_count,
+                      d_workspace, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" hg_status hg_intersect_into(const uint32_t* d_a_offsets, const void* d_a_keys, const uint32_t* d_a_idx,
@@ -236,14 +262,8 @@ extern "C" hg_status hg_intersect_into(const uint32_t* d_a_offsets, const void* 
                                        uint64_t nq, const uint32_t* d_query_idx, uint32_t* d_pairs,
                                        uint64_t pair_cap, unsigned long long* d_count, void* d_workspace,
                                        size_t workspace_bytes, hg_stream_t stream) {
-  if (!d_a_offsets || !d_count || (nq > 0 && !d_query) || (n_a > 0 && !d_a_keys)) return HG_ERR_INVALID_ARGUMENT;
-  if (n_a >= (1ull << 32)) return HG_ERR_TOO_LARGE;
-  ProbePlan plan;
-  hg_status st = plan_probe(n_buckets, nq, key_bytes, d_pairs != nullptr, &plan);
-  if (st != HG_OK) return st;
-  if (workspace_bytes < plan.total || (!d_workspace && plan.total)) return HG_ERR_TOO_LARGE;
-  return launch_probe(plan, d_a_offsets, d_a_keys, d_a_idx, d_query, d_query_idx, d_pairs, pair_cap, d_count,
-                      d_workspace, reinterpret_cast<cudaStream_t>(stream));
+  return hg_intersect_into_path(d_a_offsets, d_a_keys, d_a_idx, n_a, n_buckets, key_bytes, d_query, nq, d_query_idx,
+                                d_pairs, pair_cap, d_count, d_workspace, workspace_bytes, -1, stream);
 }
 
 extern "C" hg_status hg_intersect(const hg_table* a, const void* d_query, uint64_t nq, const uint32_t* d_query_idx,
@@ -251,7 +271,8 @@ extern "C" hg_status hg_intersect(const hg_table* a, const void* d_query, uint64
                                   hg_stream_t stream) {
   if (!a || !a->built) return HG_ERR_INVALID_ARGUMENT;
   size_t bytes = 0;
-  hg_status st = hg_intersect_workspace_size(a->n_buckets, nq, a->key_bytes, d_pairs != nullptr, &bytes);
+  hg_status st = hg_intersect_workspace_size(a->n, a->with_index, a->n_buckets, nq, a->key_bytes, d_pairs != nullptr,
+                                             &bytes);
   if (st != HG_OK) return st;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   void* ws = nullptr;

@@ -30,8 +30,12 @@
 //   the decision is taken on the device, so the launch sequence is fixed.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "hg_device.cuh"
+#include "hg_cluster.cuh"
 #include "hg_plan.h"
 #include "hg_prof.cuh"
 #include "hg_scan.cuh"
@@ -115,6 +119,7 @@ __global__ void __launch_bounds__(256) k_scatter(const KeyT* __restrict__ keys, 
 
 // In-place exclusive scan of data[0..count) (uint32 values, total < 2^32).
 // first_slot (optional) receives 0; total_out (optional) receives the sum.
+// Persistent: each CTA takes tiles in ticket order until none is left.
 template <int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK) k_scan_u32(uint32_t* __restrict__ data, uint64_t count,
                                                     uint64_t* __restrict__ status, unsigned* ticket,
@@ -125,50 +130,54 @@ __global__ void __launch_bounds__(BLOCK) k_scan_u32(uint32_t* __restrict__ data,
   __shared__ uint32_t s[TILE + TILE / 32];
   __shared__ uint32_t red[BLOCK / 32 + 1];
   __shared__ uint64_t s_tile, s_prefix;
-  if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
-  __syncthreads();
-  const uint64_t tile = s_tile;
-  const uint64_t base = tile * TILE;
-#pragma unroll
-  for (int k = 0; k < ITEMS; k++) {
-    const int si = k * BLOCK + threadIdx.x;
-    const uint64_t i = base + si;
-    s[si + si / 32] = i < count ? data[i] : 0u;
-  }
-  __syncthreads();
-  uint32_t v[ITEMS];
-  uint32_t sum = 0;
-#pragma unroll
-  for (int k = 0; k < ITEMS; k++) {
-    const int si = threadIdx.x * ITEMS + k;
-    v[k] = s[si + si / 32];
-    sum += v[k];
-  }
-  uint32_t tile_total;
-  const uint32_t excl = block_exclusive_scan<BLOCK>(sum, red, &tile_total);
-  if (threadIdx.x < 32) {
-    const uint64_t p = lookback_exclusive(status, tile, tile_total);
-    if (threadIdx.x == 0) s_prefix = p;
-  }
-  __syncthreads();
-  uint32_t run = static_cast<uint32_t>(s_prefix) + excl;
-#pragma unroll
-  for (int k = 0; k < ITEMS; k++) {
-    const int si = threadIdx.x * ITEMS + k;
-    s[si + si / 32] = run;
-    run += v[k];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < ITEMS; k++) {
-    const int si = k * BLOCK + threadIdx.x;
-    const uint64_t i = base + si;
-    if (i < count) data[i] = s[si + si / 32];
-  }
   const uint64_t ntiles = (count + TILE - 1) / TILE;
-  if (threadIdx.x == 0) {
-    if (tile == 0 && first_slot) *first_slot = 0u;
-    if (tile == ntiles - 1 && total_out) *total_out = static_cast<uint32_t>(s_prefix) + tile_total;
+  while (true) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    if (tile >= ntiles) break;
+    const uint64_t base = tile * TILE;
+#pragma unroll
+    for (int k = 0; k < ITEMS; k++) {
+      const int si = k * BLOCK + threadIdx.x;
+      const uint64_t i = base + si;
+      s[si + si / 32] = i < count ? data[i] : 0u;
+    }
+    __syncthreads();
+    uint32_t v[ITEMS];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < ITEMS; k++) {
+      const int si = threadIdx.x * ITEMS + k;
+      v[k] = s[si + si / 32];
+      sum += v[k];
+    }
+    uint32_t tile_total;
+    const uint32_t excl = block_exclusive_scan<BLOCK>(sum, red, &tile_total);
+    if (threadIdx.x < 32) {
+      const uint64_t p = lookback_exclusive(status, tile, tile_total);
+      if (threadIdx.x == 0) s_prefix = p;
+    }
+    __syncthreads();
+    uint32_t run = static_cast<uint32_t>(s_prefix) + excl;
+#pragma unroll
+    for (int k = 0; k < ITEMS; k++) {
+      const int si = threadIdx.x * ITEMS + k;
+      s[si + si / 32] = run;
+      run += v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < ITEMS; k++) {
+      const int si = k * BLOCK + threadIdx.x;
+      const uint64_t i = base + si;
+      if (i < count) data[i] = s[si + si / 32];
+    }
+    if (threadIdx.x == 0) {
+      if (tile == 0 && first_slot) *first_slot = 0u;
+      if (tile == ntiles - 1 && total_out) *total_out = static_cast<uint32_t>(s_prefix) + tile_total;
+    }
+    __syncthreads();
   }
 }
 
@@ -180,109 +189,256 @@ __global__ void k_fill_u32(uint32_t* p, uint64_t count, uint32_t value, const ui
 }
 
 // ---------------------------------------------------------------------------
-// Partitioned path
+// Partitioned path (cluster kernels)
 // ---------------------------------------------------------------------------
-template <typename KeyT, int V, bool WITH_IDX>
-__global__ void __launch_bounds__(256) k_part_scatter(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
-                                                      uint32_t part_log2, uint64_t cap,
-                                                      uint32_t* __restrict__ pcount, KeyT* __restrict__ pkeys,
-                                                      uint32_t* __restrict__ pidx, uint32_t* flags) {
-  const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-  const uint64_t nchunks = (n + 32ull * V - 1) / (32ull * V);
+
+// Pass 1: cluster multisplit.  A cluster of CL CTAs takes a tile of
+// CL*TILE consecutive keys (TILE = BLOCK*KPT, held in registers); every CTA
+// ranks its keys per coarse partition with shared-memory atomics, the cluster
+// sums the per-CTA histograms over DSMEM (CTA c owns partitions
+// [c*P/CL, (c+1)*P/CL)), each owner reserves the cluster's run in partition
+// p with ONE global atomic and hands every CTA its start, and each CTA writes
+// its keys partition-sorted (shared-memory counting sort) so the runs leave
+// as coalesced stores.
+// Dynamic smem: hist[P] | lp[P] | start[P] | sk[TILE] | si[TILE] | sp[TILE] (u16)
+template <typename KeyT, bool WITH_IDX, int BLOCK, int KPT>
+__global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict__ keys, const uint32_t* __restrict__ key_idx,
+                                                      uint64_t n, BucketMap bm, uint32_t coarse_log2, uint32_t n_parts,
+                                                      uint64_t cap, uint32_t* __restrict__ pcount,
+                                                      KeyT* __restrict__ pkeys, uint32_t* __restrict__ pidx,
+                                                      uint32_t* flags) {
+  constexpr uint32_t TILE = BLOCK * KPT;
+  cg::cluster_group cluster = cg::this_cluster();
+  const unsigned CL = cluster.num_blocks();
+  const unsigned rank = cluster.block_rank();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t* hist = reinterpret_cast<uint32_t*>(smem_raw);
+  uint32_t* lp = hist + n_parts;
+  uint32_t* start = lp + n_parts;
+  KeyT* sk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(n_parts) * 12, 16));
+  uint32_t* si = reinterpret_cast<uint32_t*>(sk + TILE);
+  uint16_t* sp = reinterpret_cast<uint16_t*>(WITH_IDX ? reinterpret_cast<unsigned char*>(si + TILE)
+                                                      : reinterpret_cast<unsigned char*>(si));
+  __shared__ uint32_t wsum[BLOCK / 32 + 1];
+  const uint64_t cluster_id = blockIdx.x / CL, nclusters = gridDim.x / CL;
+  const uint64_t ctile = uint64_t(CL) * TILE;
+  const uint64_t ntiles = (n + ctile - 1) / ctile;
+  const uint32_t per = (n_parts + CL - 1) / CL;
+  const uint32_t p0 = min(n_parts, rank * per), p1 = min(n_parts, p0 + per);
   bool overflow = false;
-  for (uint64_t c = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; c < nchunks;
-       c += warps) {
-    KeyT k[V];
-    bool ok[V];
-    const uint64_t base = c * 32ull * V;
-    load_chunk<KeyT, V>(keys, n, base, k, ok);
+  for (uint64_t ct = cluster_id; ct < ntiles; ct += nclusters) {
+    const uint64_t base = ct * ctile + uint64_t(rank) * TILE;
+    const uint32_t cnt = base < n ? static_cast<uint32_t>(umin64(TILE, n - base)) : 0u;
+    for (uint32_t j = threadIdx.x; j < n_parts; j += BLOCK) hist[j] = 0u;
+    KeyT k[KPT];
+    uint32_t pr[KPT];
 #pragma unroll
-    for (int j = 0; j < V; j++) {
-      const uint32_t p = bm.of_key(k[j]) >> part_log2;
-      const uint32_t slot = warp_aggregated_inc(pcount, p, ok[j]);
-      if (ok[j]) {
-        if (slot < cap) {
-          const uint64_t at = static_cast<uint64_t>(p) * cap + slot;
-          pkeys[at] = k[j];
-          if constexpr (WITH_IDX) pidx[at] = static_cast<uint32_t>(base + lane_id() * V + j);
-        } else {
-          overflow = true;
-        }
+    for (int u = 0; u < KPT; u++) {
+      const uint32_t r = u * BLOCK + threadIdx.x;
+      k[u] = r < cnt ? __ldcs(keys + base + r) : KeyT(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < KPT; u++) {
+      const uint32_t r = u * BLOCK + threadIdx.x;
+      if (r < cnt) {
+        const uint32_t p = bm.of_key(k[u]) >> coarse_log2;
+        pr[u] = (p << 16) | atomicAdd(&hist[p], 1u);
       }
     }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < n_parts; j += BLOCK) lp[j] = hist[j];
+    __syncthreads();
+    block_scan_segments<BLOCK>(lp, n_parts, 0u, 0u, wsum, [](uint32_t, uint32_t) {});
+    cluster.sync();
+    // owners: sum the cluster's histograms for their partitions and reserve
+    for (uint32_t p = p0 + threadIdx.x; p < p1; p += BLOCK) {
+      uint32_t h[16];
+      uint32_t tot = 0;
+      for (unsigned c = 0; c < CL; c++) {
+        h[c] = cluster.map_shared_rank(hist, c)[p];
+        tot += h[c];
+      }
+      uint32_t run = tot ? atomicAdd(pcount + p, tot) : 0u;
+      if (uint64_t(run) + tot > cap) overflow = true;
+      for (unsigned c = 0; c < CL; c++) {
+        cluster.map_shared_rank(start, c)[p] = run;
+        run += h[c];
+      }
+    }
+    cluster.sync();
+#pragma unroll
+    for (int u = 0; u < KPT; u++) {
+      const uint32_t r = u * BLOCK + threadIdx.x;
+      if (r < cnt) {
+        const uint32_t p = pr[u] >> 16;
+        const uint32_t pos = lp[p] + (pr[u] & 0xffffu);
+        sk[pos] = k[u];
+        sp[pos] = static_cast<uint16_t>(p);
+        if constexpr (WITH_IDX) si[pos] = key_idx ? key_idx[base + r] : static_cast<uint32_t>(base + r);
+      }
+    }
+    __syncthreads();
+    for (uint32_t s = threadIdx.x; s < cnt; s += BLOCK) {
+      const uint32_t p = sp[s];
+      const uint64_t off = uint64_t(start[p]) + (s - lp[p]);
+      if (off < cap) {
+        pkeys[uint64_t(p) * cap + off] = sk[s];
+        if constexpr (WITH_IDX) pidx[uint64_t(p) * cap + off] = si[s];
+      } else {
+        overflow = true;
+      }
+    }
+    __syncthreads();
   }
   if (overflow) atomicOr(flags, FLAG_OVERFLOW);
 }
 
-// One CTA per partition (grid-stride over partitions).  Dynamic shared memory:
-// 2^part_log2 uint32 counters.
+// Pass 2: split every coarse partition S ways into fine partitions of W
+// buckets.  One CTA per tile of a coarse partition's records: a
+// shared-memory counting sort by fine partition, one global atomic per
+// (tile, fine partition) to reserve the run, coalesced run writes.
+// Dynamic smem: hist[S] | lp[S] | base[S] | pr[tile] | sk[tile] | si[tile]
 template <typename KeyT, bool WITH_IDX, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_part_local(const KeyT* __restrict__ pkeys, const uint32_t* __restrict__ pidx,
-                                                      const uint32_t* __restrict__ pstart, uint64_t n_parts,
-                                                      uint64_t cap, uint32_t part_log2, BucketMap bm,
-                                                      uint64_t n_buckets, uint32_t* __restrict__ offsets,
-                                                      KeyT* __restrict__ keys_out, uint32_t* __restrict__ idx_out,
-                                                      const uint32_t* flags) {
+__global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys, const uint32_t* __restrict__ pidx,
+                                                 const uint32_t* __restrict__ pstart, uint32_t n_parts, uint64_t cap1,
+                                                 uint32_t tiles_per_part, uint32_t tile, BucketMap bm,
+                                                 uint32_t fine_log2, uint32_t split_log2, uint64_t capf,
+                                                 uint32_t* __restrict__ fcount, KeyT* __restrict__ fkeys,
+                                                 uint32_t* __restrict__ fidx, uint32_t* flags) {
   if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
-  extern __shared__ uint32_t ctr[];
-  constexpr int NW = BLOCK / 32;
-  __shared__ uint32_t wsum[NW + 1];
-  const unsigned warp = threadIdx.x >> 5, lane = lane_id();
-  if (blockIdx.x == 0 && threadIdx.x == 0) offsets[n_buckets] = pstart[n_parts];
-  for (uint64_t p = blockIdx.x; p < n_parts; p += gridDim.x) {
-    const uint32_t base = pstart[p];
-    const uint32_t cnt = pstart[p + 1] - base;
-    const uint64_t b0 = p << part_log2;
-    const uint32_t nb = static_cast<uint32_t>(min(uint64_t(1) << part_log2, n_buckets - b0));
-    const KeyT* src = pkeys + p * cap;
-    const uint32_t* srci = pidx + p * cap;
-    for (uint32_t j = threadIdx.x; j < nb; j += BLOCK) ctr[j] = 0;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t S = 1u << split_log2;
+  uint32_t* hist = reinterpret_cast<uint32_t*>(smem_raw);
+  uint32_t* lp = hist + S;
+  uint32_t* base = lp + S;
+  uint32_t* pr = base + S;
+  KeyT* sk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(S) * 12 + size_t(tile) * 4, 16));
+  uint32_t* si = reinterpret_cast<uint32_t*>(sk + tile);
+  const uint32_t coarse_log2 = fine_log2 + split_log2;
+  bool overflow = false;
+  const uint64_t vtiles = uint64_t(n_parts) * tiles_per_part;
+  for (uint64_t vt = blockIdx.x; vt < vtiles; vt += gridDim.x) {
+    const uint64_t q = vt / tiles_per_part;
+    const uint32_t r0 = static_cast<uint32_t>(vt % tiles_per_part) * tile;
+    const uint32_t m = pstart[q + 1] - pstart[q];
+    if (r0 >= m) continue;  // uniform across the block
+    const uint32_t cnt = min(tile, m - r0);
+    const KeyT* src = pkeys + q * cap1 + r0;
+    const uint32_t* srci = pidx + q * cap1 + r0;
+    const uint64_t b0 = q << coarse_log2;
+    for (uint32_t j = threadIdx.x; j < S; j += BLOCK) hist[j] = 0u;
     __syncthreads();
-    for (uint32_t r0 = 0; r0 < cnt; r0 += BLOCK) {
-      const uint32_t r = r0 + threadIdx.x;
-      const bool ok = r < cnt;
-      const KeyT k = ok ? src[r] : KeyT(0);
-      const uint32_t lb = ok ? static_cast<uint32_t>(bm.of_key(k) - b0) : 0u;
-      warp_aggregated_count(ctr, lb, ok);
+    for (uint32_t r = threadIdx.x; r < cnt; r += BLOCK) {
+      const KeyT k = src[r];
+      const uint32_t f = static_cast<uint32_t>(bm.of_key(k) - b0) >> fine_log2;
+      const uint32_t rk = atomicAdd(&hist[f], 1u);
+      pr[r] = (f << 16) | rk;
+      sk[r] = k;  // unsorted copy; sorted below into the same tile slots via pr
     }
     __syncthreads();
-    // Segmented scan: warp w owns counters [w*seg, (w+1)*seg).
-    const uint32_t seg = ((nb + NW - 1) / NW + 31) & ~31u;
-    const uint32_t s0 = min(nb, warp * seg), s1 = min(nb, s0 + seg);
-    uint32_t part = 0;
-    for (uint32_t j = s0 + lane; j < s1; j += 32) part += ctr[j];
-    part = warp_sum(part);
-    if (lane == 0) wsum[warp] = part;
-    __syncthreads();
-    if (warp == 0) {
-      const uint32_t w = lane < NW ? wsum[lane] : 0u;
-      const uint32_t wi = warp_inclusive_scan(w);
-      if (lane < NW) wsum[lane] = wi - w;
-    }
-    __syncthreads();
-    uint32_t run = base + wsum[warp];
-    for (uint32_t j0 = s0; j0 < s1; j0 += 32) {
-      const uint32_t j = j0 + lane;
-      const uint32_t v = j < s1 ? ctr[j] : 0u;
-      const uint32_t inc = warp_inclusive_scan(v);
-      if (j < s1) {
-        const uint32_t ex = run + inc - v;
-        ctr[j] = ex;
-        offsets[b0 + j] = ex;
+    if (threadIdx.x < 32) {  // exclusive scan of S <= 1024 counts by one warp
+      uint32_t run = 0;
+      for (uint32_t j0 = 0; j0 < S; j0 += 32) {
+        const uint32_t j = j0 + threadIdx.x;
+        const uint32_t v = j < S ? hist[j] : 0u;
+        const uint32_t inc = warp_inclusive_scan(v);
+        if (j < S) lp[j] = run + inc - v;
+        run += __shfl_sync(FULL_MASK, inc, 31);
       }
-      run += __shfl_sync(FULL_MASK, inc, 31);
+    }
+    for (uint32_t f = threadIdx.x; f < S; f += BLOCK) {
+      const uint32_t h = hist[f];
+      const uint32_t b = h ? atomicAdd(fcount + (q << split_log2) + f, h) : 0u;
+      if (uint64_t(b) + h > capf) overflow = true;
+      base[f] = b;
     }
     __syncthreads();
-    for (uint32_t r0 = 0; r0 < cnt; r0 += BLOCK) {
-      const uint32_t r = r0 + threadIdx.x;
-      const bool ok = r < cnt;
-      const KeyT k = ok ? src[r] : KeyT(0);
-      const uint32_t lb = ok ? static_cast<uint32_t>(bm.of_key(k) - b0) : 0u;
-      const uint32_t pos = warp_aggregated_inc(ctr, lb, ok);
-      if (ok) {
-        keys_out[pos] = k;
-        if constexpr (WITH_IDX) idx_out[pos] = srci[r];
+    // counting sort of the tile: read the unsorted record, keep it in a
+    // register across the barrier, write it to its sorted slot
+    KeyT kk[8];
+    uint32_t ii[8], pp[8];
+    for (uint32_t r1 = 0; r1 < cnt; r1 += 8 * BLOCK) {
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const uint32_t r = r1 + u * BLOCK + threadIdx.x;
+        if (r < cnt) {
+          const uint32_t v = pr[r];
+          pp[u] = lp[v >> 16] + (v & 0xffffu);
+          kk[u] = sk[r];
+          if constexpr (WITH_IDX) ii[u] = srci[r];
+        }
       }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const uint32_t r = r1 + u * BLOCK + threadIdx.x;
+        if (r < cnt) {
+          sk[pp[u]] = kk[u];
+          if constexpr (WITH_IDX) si[pp[u]] = ii[u];
+        }
+      }
+      __syncthreads();
+    }
+    for (uint32_t s = threadIdx.x; s < cnt; s += BLOCK) {
+      const KeyT k = sk[s];
+      const uint32_t f = static_cast<uint32_t>(bm.of_key(k) - b0) >> fine_log2;
+      const uint64_t off = uint64_t(base[f]) + (s - lp[f]);
+      if (off < capf) {
+        const uint64_t at = ((q << split_log2) + f) * capf + off;
+        fkeys[at] = k;
+        if constexpr (WITH_IDX) fidx[at] = si[s];
+      } else {
+        overflow = true;
+      }
+    }
+    __syncthreads();
+  }
+  if (overflow) atomicOr(flags, FLAG_OVERFLOW);
+}
+
+// Pass 3: one CTA per fine partition of W buckets.  The partition's records
+// are staged in shared memory, counted into W shared counters, the counters
+// are scanned (coalesced offsets write) and the records scattered into the
+// partition's output slice (a few hundred KB, completed while resident in L2).
+// Dynamic smem: ctr[W] | sk[capf] | si[capf]
+template <typename KeyT, bool WITH_IDX, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ fkeys, const uint32_t* __restrict__ fidx,
+                                                      const uint32_t* __restrict__ fstart, uint64_t n_fine, uint64_t capf,
+                                                      uint32_t fine_log2, BucketMap bm, uint64_t n_buckets,
+                                                      uint32_t* __restrict__ offsets, KeyT* __restrict__ keys_out,
+                                                      uint32_t* __restrict__ idx_out, const uint32_t* flags) {
+  if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t W = 1u << fine_log2;
+  uint32_t* ctr = reinterpret_cast<uint32_t*>(smem_raw);
+  KeyT* sk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(W) * 4, 16));
+  uint32_t* si = reinterpret_cast<uint32_t*>(sk + capf);
+  __shared__ uint32_t wsum[BLOCK / 32 + 1];
+  if (blockIdx.x == 0 && threadIdx.x == 0) offsets[n_buckets] = fstart[n_fine];
+  for (uint64_t f = blockIdx.x; f < n_fine; f += gridDim.x) {
+    const uint64_t b0 = f << fine_log2;
+    if (b0 >= n_buckets) break;  // fine partitions are in bucket order
+    const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
+    const uint32_t base = fstart[f];
+    const uint32_t m = fstart[f + 1] - base;
+    const KeyT* src = fkeys + f * capf;
+    const uint32_t* srci = fidx + f * capf;
+    for (uint32_t j = threadIdx.x; j < nb; j += BLOCK) ctr[j] = 0u;
+    for (uint32_t r = threadIdx.x; r < m; r += BLOCK) {
+      sk[r] = __ldcs(src + r);
+      if constexpr (WITH_IDX) si[r] = __ldcs(srci + r);
+    }
+    __syncthreads();
+    for (uint32_t r = threadIdx.x; r < m; r += BLOCK)
+      atomicAdd(&ctr[static_cast<uint32_t>(bm.of_key(sk[r]) - b0)], 1u);
+    __syncthreads();
+    block_scan_segments<BLOCK>(ctr, nb, base, base, wsum, [&](uint32_t j, uint32_t g) { offsets[b0 + j] = g; });
+    for (uint32_t r = threadIdx.x; r < m; r += BLOCK) {
+      const KeyT k = sk[r];
+      const uint32_t pos = atomicAdd(&ctr[static_cast<uint32_t>(bm.of_key(k) - b0)], 1u);
+      keys_out[pos] = k;
+      if constexpr (WITH_IDX) idx_out[pos] = si[r];
     }
     __syncthreads();
   }
@@ -302,47 +458,6 @@ int device_sm_count() {
     cached[dev] = sms;
   }
   return cached[dev];
-}
-
-constexpr int PART_LOCAL_BLOCK = 512;
-constexpr uint32_t PART_LOG2_DEFAULT = 14;
-
-hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_index, BuildPlan* plan,
-                     int force_path) {
-  if (key_bytes != 4 && key_bytes != 8) return HG_ERR_KEY_WIDTH;
-  if (n_buckets == 0) return HG_ERR_INVALID_ARGUMENT;
-  if (n >= (1ull << 32) || n_buckets > (1ull << 32)) return HG_ERR_TOO_LARGE;
-  BuildPlan p;
-  p.n = n;
-  p.n_buckets = n_buckets;
-  p.key_bytes = key_bytes;
-  p.with_index = with_index;
-  const uint64_t rec = key_bytes + (with_index ? 4 : 0);
-  const uint64_t footprint = n * (key_bytes + rec) + 4 * n_buckets;
-  int path = force_path;
-  if (path < 0) path = (footprint <= (48ull << 20) || n_buckets <= (1ull << PART_LOG2_DEFAULT)) ? BUILD_DIRECT : BUILD_PARTITIONED;
-  p.path = path;
-  size_t off = 0;
-  p.scan_tiles = (n_buckets + SCAN_TILE - 1) / SCAN_TILE;
-  p.off_status = off;  off = align_up(off + p.scan_tiles * 8);
-  p.off_ticket = off;  off = align_up(off + 2 * sizeof(unsigned));
-  p.off_flags = off;   off = align_up(off + sizeof(uint32_t));
-  if (path == BUILD_PARTITIONED) {
-    p.part_log2 = PART_LOG2_DEFAULT;
-    p.n_parts = (n_buckets + (1ull << p.part_log2) - 1) >> p.part_log2;
-    const double mean = double(n) * double(1ull << p.part_log2) / double(n_buckets);
-    uint64_t cap = static_cast<uint64_t>(std::ceil(mean + 8.0 * std::sqrt(mean) + 64.0));
-    cap = (cap + 31) & ~31ull;
-    p.part_cap = cap;
-    p.pscan_tiles = (p.n_parts + SCAN_TILE - 1) / SCAN_TILE;
-    // the partition scan gets its own status region after the bucket-scan one
-    p.off_pcount = off;  off = align_up(off + (p.n_parts + 1) * 4 + p.pscan_tiles * 8 + 8);
-    p.off_pkeys = off;   off = align_up(off + p.n_parts * cap * key_bytes);
-    if (with_index) { p.off_pidx = off; off = align_up(off + p.n_parts * cap * 4); }
-  }
-  p.total = std::max<size_t>(off, WS_ALIGN);
-  *plan = p;
-  return HG_OK;
 }
 
 template <typename KeyT, int V>
@@ -368,13 +483,14 @@ static void launch_direct_scatter(const KeyT* keys, uint64_t n, BucketMap bm, ui
 }
 
 static void launch_scan(uint32_t* data, uint64_t count, uint64_t* status, unsigned* ticket, uint32_t* first_slot,
-                        uint32_t* total_out, const uint32_t* gate, cudaStream_t s) {
+                        uint32_t* total_out, const uint32_t* gate, cudaStream_t s, const char* name = nullptr) {
   const uint64_t tiles = (count + SCAN_TILE - 1) / SCAN_TILE;
   if (tiles == 0) return;
-  Phase ph(s, gate ? "fallback_scan" : "scan");
+  Phase ph(s, name ? name : (gate ? "fallback_scan" : "scan"));
   count_launch();
-  k_scan_u32<SCAN_BLOCK, SCAN_ITEMS><<<static_cast<unsigned>(tiles), SCAN_BLOCK, 0, s>>>(data, count, status, ticket,
-                                                                                      first_slot, total_out, gate);
+  const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(tiles, uint64_t(device_sm_count()) * 8));
+  k_scan_u32<SCAN_BLOCK, SCAN_ITEMS><<<grid, SCAN_BLOCK, 0, s>>>(data, count, status, ticket, first_slot, total_out,
+                                                                 gate);
 }
 
 template <typename KeyT, int V, bool WI>
@@ -389,12 +505,212 @@ static hg_status run_direct(const BuildPlan& p, const KeyT* keys, uint32_t* offs
     count_launch();
     k_fill_u32<<<std::max(grid, 1), 256, 0, s>>>(offsets, p.n_buckets + 1, 0u, gate);
   } else {
-    if (cudaMemsetAsync(offsets, 0, (p.n_buckets + 1) * sizeof(uint32_t), s) != cudaSuccess) return HG_ERR_CUDA;
+    HG_CUDA(cudaMemsetAsync(offsets, 0, (p.n_buckets + 1) * sizeof(uint32_t), s), "build: offsets memset");
   }
-  if (cudaMemsetAsync(ws + p.off_status, 0, p.off_flags - p.off_status, s) != cudaSuccess) return HG_ERR_CUDA;
+  HG_CUDA(cudaMemsetAsync(ws + p.off_status, 0, p.off_flags - p.off_status, s), "build: scan state memset");
   if (p.n > 0) launch_direct_count<KeyT, V>(keys, p.n, bm, offsets + 1, gate, s);
   launch_scan(offsets + 1, p.n_buckets, status, ticket, offsets, nullptr, gate, s);
   if (p.n > 0) launch_direct_scatter<KeyT, V, WI>(keys, p.n, bm, offsets + 1, keys_out, idx_out, gate, s);
+  return HG_OK;
+}
+
+uint64_t slack_capacity(double mean, uint64_t margin) {
+  const uint64_t c = static_cast<uint64_t>(std::ceil(mean + 8.0 * std::sqrt(mean) + double(margin)));
+  return (c + 31) & ~31ull;
+}
+
+static uint32_t ceil_log2_u64(uint64_t x) {
+  uint32_t l = 0;
+  while ((1ull << l) < x) l++;
+  return l;
+}
+
+bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size_t smem_rec, size_t per_bucket,
+                   size_t stream_smem, uint64_t n_buckets, bool staged_may_spill, PartGeometry* out) {
+  PartGeometry g;
+  bool found = false;
+  for (uint32_t w = 15; w >= 6 && !found; w--) {
+    const uint64_t W = 1ull << w;
+    const double frac = double(std::min<uint64_t>(W, n_buckets)) / double(n_buckets);
+    const uint64_t cap = slack_capacity(double(n_staged) * frac, 64);
+    const uint64_t qcap = stream_smem ? slack_capacity(double(n_stream) * frac, 64) : 0;
+    const size_t bytes = align_up(per_bucket * (W + 1), 16) + cap * smem_rec + qcap * stream_smem;
+    if (bytes <= FINE_SMEM_BUDGET) {
+      g.fine_log2 = w;
+      g.smem_cap = static_cast<uint32_t>(cap);
+      g.smem3 = bytes;
+      found = true;
+    }
+  }
+  if (!found) {
+    if (!staged_may_spill) return false;
+    g.fine_log2 = 6;
+    const double frac = double(std::min<uint64_t>(64, n_buckets)) / double(n_buckets);
+    const uint64_t qcap = stream_smem ? slack_capacity(double(n_stream) * frac, 64) : 0;
+    const size_t head = align_up(per_bucket * ((size_t(1) << 6) + 1), 16) + qcap * stream_smem;
+    if (head + 32 * smem_rec > FINE_SMEM_BUDGET) return false;
+    g.smem_cap = static_cast<uint32_t>((FINE_SMEM_BUDGET - head) / smem_rec) & ~31u;
+    g.smem3 = head + size_t(g.smem_cap) * smem_rec;
+  }
+  const uint64_t W = 1ull << g.fine_log2;
+  g.split_log2 = std::min<uint32_t>(SPLIT_LOG2_MAX, ceil_log2_u64((n_buckets + W - 1) / W));
+  g.coarse_log2 = g.fine_log2 + g.split_log2;
+  g.n_parts = (n_buckets + (1ull << g.coarse_log2) - 1) >> g.coarse_log2;
+  g.n_fine = g.n_parts << g.split_log2;
+  g.part_cap = slack_capacity(double(n_stream) * double(std::min<uint64_t>(1ull << g.coarse_log2, n_buckets)) /
+                                  double(n_buckets), 256);
+  g.fine_cap = slack_capacity(double(n_stream) * double(std::min<uint64_t>(W, n_buckets)) / double(n_buckets), 64);
+  // pass 1: hist/lp/start per coarse partition + a sorted tile (keys, index,
+  // 16-bit partition ids)
+  g.tile1 = PASS1_TILE;
+  g.smem1 = align_up(12 * g.n_parts, 16) + size_t(PASS1_TILE) * (stream_rec + 2);
+  g.smem2 = align_up(12 * (size_t(1) << g.split_log2) + 4 * size_t(SPLIT_TILE), 16) + size_t(SPLIT_TILE) * stream_rec;
+  g.pscan_tiles = (g.n_parts + SCAN_TILE - 1) / SCAN_TILE;
+  g.fscan_tiles = (g.n_fine + SCAN_TILE - 1) / SCAN_TILE;
+  if (g.smem1 > SMEM_BUDGET || g.n_parts >= 65536 || g.part_cap >= (1ull << 32) || g.fine_cap >= (1ull << 32))
+    return false;
+  *out = g;
+  return true;
+}
+
+hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_index, BuildPlan* plan, int force_path) {
+  if (key_bytes != 4 && key_bytes != 8) return HG_ERR_KEY_WIDTH;
+  if (n_buckets == 0) return HG_ERR_INVALID_ARGUMENT;
+  if (n >= (1ull << 32) || n_buckets > (1ull << 32)) return HG_ERR_TOO_LARGE;
+  BuildPlan p;
+  p.n = n;
+  p.n_buckets = n_buckets;
+  p.key_bytes = key_bytes;
+  p.with_index = with_index;
+  const size_t rec = key_bytes + (with_index ? 4 : 0);
+  const bool part_ok = plan_geometry(n, rec, n, rec, 4, 0, n_buckets, false, &p.g);
+  const uint64_t footprint = n * (key_bytes + rec) + 4 * n_buckets;
+  int path = force_path;
+  if (path < 0) path = (part_ok && footprint > (48ull << 20)) ? BUILD_PARTITIONED : BUILD_DIRECT;
+  // A table too dense to stage a fine partition in shared memory (a few
+  // buckets holding everything) takes the direct path even when asked for
+  // the partitioned one.
+  if (path == BUILD_PARTITIONED && !part_ok) path = BUILD_DIRECT;
+  p.path = path;
+  size_t off = 0;
+  p.scan_tiles = (n_buckets + SCAN_TILE - 1) / SCAN_TILE;
+  p.off_status = off;  off = align_up(off + p.scan_tiles * 8);
+  p.off_ticket = off;  off = align_up(off + 4 * sizeof(unsigned));
+  p.off_flags = off;   off = align_up(off + sizeof(uint32_t));
+  if (path == BUILD_PARTITIONED) {
+    const PartGeometry& g = p.g;
+    p.off_pcount = off;  off = align_up(off + (g.n_parts + 1) * 4);
+    p.off_pstatus = off; off = align_up(off + g.pscan_tiles * 8);
+    p.off_fcount = off;  off = align_up(off + (g.n_fine + 1) * 4);
+    p.off_fstatus = off; off = align_up(off + g.fscan_tiles * 8);
+    p.off_pkeys = off;   off = align_up(off + g.n_parts * g.part_cap * key_bytes);
+    if (with_index) { p.off_pidx = off; off = align_up(off + g.n_parts * g.part_cap * 4); }
+    p.off_fkeys = off;   off = align_up(off + g.n_fine * g.fine_cap * key_bytes);
+    if (with_index) { p.off_fidx = off; off = align_up(off + g.n_fine * g.fine_cap * 4); }
+  } else {
+    p.off_pcount = p.off_pstatus = p.off_fcount = p.off_fstatus = off;
+    p.off_pkeys = p.off_pidx = p.off_fkeys = p.off_fidx = off;
+  }
+  p.total = std::max<size_t>(off, WS_ALIGN);
+  *plan = p;
+  return HG_OK;
+}
+
+// Cluster size for pass 1: 16 CTAs (twice the keys per reservation) when the
+// device runs 16-CTA clusters of this shape on at least as many SMs as 8-CTA
+// ones, else 8.
+template <typename Kern>
+static unsigned pick_cluster(Kern kern, unsigned block, size_t smem, int* nclusters) {
+  const int c16 = cluster_capacity(kern, block, smem, 16);
+  const int c8 = cluster_capacity(kern, block, smem, 8);
+  if (c16 > 0 && c16 * 16 >= c8 * 8) {
+    *nclusters = c16;
+    return 16;
+  }
+  *nclusters = c8;
+  return 8;
+}
+
+// Raises a kernel's dynamic shared-memory limit to the device maximum (minus
+// its static shared memory) once, and returns co-resident CTAs per SM for
+// `smem` bytes (0 if it cannot run).
+template <typename Kern>
+static int blocks_per_sm(Kern kern, unsigned block, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, size_t, unsigned, int>, int> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(reinterpret_cast<const void*>(kern), smem, block, dev);
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa = {};
+  cudaFuncGetAttributes(&fa, kern);
+  const int max_dyn = optin - static_cast<int>(fa.sharedSizeBytes);
+  int n = 0;
+  if (max_dyn >= 0 && size_t(max_dyn) >= smem &&
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn) == cudaSuccess)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, static_cast<int>(block), smem);
+  cudaGetLastError();
+  std::lock_guard<std::mutex> g(mu);
+  cache[key] = n;
+  return n;
+}
+
+// Passes 1 and 2 of a partitioned path over `n` streamed keys (with their
+// input positions when WI): cluster multisplit into coarse partitions, scan,
+// split into fine partitions, scan.  Shared by the build and the probe.
+template <typename KeyT, int V, bool WI>
+static hg_status run_partition_passes(const PartGeometry& g, uint64_t n, const KeyT* keys, const uint32_t* key_idx,
+                                      BucketMap bm, char* ws, size_t off_flags, size_t off_ticket, size_t off_pcount,
+                                      size_t off_pstatus, size_t off_fcount, size_t off_fstatus, size_t off_pkeys,
+                                      size_t off_pidx, size_t off_fkeys, size_t off_fidx, const char* who,
+                                      cudaStream_t s) {
+  uint32_t* flags = reinterpret_cast<uint32_t*>(ws + off_flags);
+  unsigned* ticket = reinterpret_cast<unsigned*>(ws + off_ticket);
+  uint32_t* pcount = reinterpret_cast<uint32_t*>(ws + off_pcount);
+  uint64_t* pstatus = reinterpret_cast<uint64_t*>(ws + off_pstatus);
+  uint32_t* fcount = reinterpret_cast<uint32_t*>(ws + off_fcount);
+  uint64_t* fstatus = reinterpret_cast<uint64_t*>(ws + off_fstatus);
+  KeyT* pkeys = reinterpret_cast<KeyT*>(ws + off_pkeys);
+  uint32_t* pidx = WI ? reinterpret_cast<uint32_t*>(ws + off_pidx) : nullptr;
+  KeyT* fkeys = reinterpret_cast<KeyT*>(ws + off_fkeys);
+  uint32_t* fidx = WI ? reinterpret_cast<uint32_t*>(ws + off_fidx) : nullptr;
+  if (n > 0) {
+    auto kern = k_multisplit<KeyT, WI, PASS1_BLOCK, PASS1_KPT>;
+    int ncl = 0;
+    const unsigned cl = pick_cluster(kern, PASS1_BLOCK, g.smem1, &ncl);
+    if (ncl <= 0) return lib_fail(HG_ERR_CUDA, "no co-resident cluster for the multisplit kernel");
+    const uint64_t ntiles = (n + uint64_t(cl) * PASS1_TILE - 1) / (uint64_t(cl) * PASS1_TILE);
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ntiles, uint64_t(ncl))) * cl;
+    Phase ph(s, who[0] == 'b' ? "multisplit" : "probe_multisplit");
+    count_launch();
+    HG_CUDA(launch_cluster(kern, grid, PASS1_BLOCK, g.smem1, cl, s, keys, key_idx, n, bm, g.coarse_log2,
+                           static_cast<uint32_t>(g.n_parts), g.part_cap, pcount, pkeys, pidx, flags),
+            "multisplit launch");
+  }
+  launch_scan(pcount, g.n_parts, pstatus, ticket + 1, nullptr, pcount + g.n_parts, nullptr, s,
+              who[0] == 'b' ? "part_scan" : "probe_part_scan");
+  {
+    auto kern = k_split<KeyT, WI, SPLIT_BLOCK>;
+    const int bps = blocks_per_sm(kern, SPLIT_BLOCK, g.smem2);
+    if (bps <= 0) return lib_fail(HG_ERR_CUDA, "split kernel cannot be resident");
+    const uint32_t tiles_per_part = static_cast<uint32_t>((g.part_cap + SPLIT_TILE - 1) / SPLIT_TILE);
+    const uint64_t vt = g.n_parts * tiles_per_part;
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(vt, uint64_t(device_sm_count()) * bps));
+    Phase ph(s, who[0] == 'b' ? "split" : "probe_split");
+    count_launch();
+    k_split<KeyT, WI, SPLIT_BLOCK><<<std::max(grid, 1u), SPLIT_BLOCK, g.smem2, s>>>(
+        pkeys, pidx, pcount, static_cast<uint32_t>(g.n_parts), g.part_cap, tiles_per_part, SPLIT_TILE, bm,
+        g.fine_log2, g.split_log2, g.fine_cap, fcount, fkeys, fidx, flags);
+    HG_CUDA(cudaPeekAtLastError(), "split launch");
+  }
+  launch_scan(fcount, g.n_fine, fstatus, ticket + 2, nullptr, fcount + g.n_fine, nullptr, s,
+              who[0] == 'b' ? "fine_scan" : "probe_fine_scan");
   return HG_OK;
 }
 
@@ -402,37 +718,30 @@ template <typename KeyT, int V, bool WI>
 static hg_status run_partitioned(const BuildPlan& p, const KeyT* keys, uint32_t* offsets, KeyT* keys_out,
                                  uint32_t* idx_out, char* ws, cudaStream_t s) {
   const BucketMap bm = BucketMap::make(p.n_buckets);
+  const PartGeometry& g = p.g;
   uint32_t* flags = reinterpret_cast<uint32_t*>(ws + p.off_flags);
-  uint32_t* pcount = reinterpret_cast<uint32_t*>(ws + p.off_pcount);
-  uint64_t* pstatus = reinterpret_cast<uint64_t*>(ws + p.off_pcount + align_up((p.n_parts + 1) * 4, 8));
-  unsigned* ticket = reinterpret_cast<unsigned*>(ws + p.off_ticket);
-  KeyT* pkeys = reinterpret_cast<KeyT*>(ws + p.off_pkeys);
-  uint32_t* pidx = WI ? reinterpret_cast<uint32_t*>(ws + p.off_pidx) : nullptr;
-  // status words, tickets, flags, partition counts and their scan status
-  if (cudaMemsetAsync(ws + p.off_status, 0, p.off_pkeys - p.off_status, s) != cudaSuccess) return HG_ERR_CUDA;
-  if (p.n > 0) {
-    const uint64_t chunks = (p.n + 32ull * V - 1) / (32ull * V);
-    const uint64_t want = (chunks + 7) / 8;
-    const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(want, uint64_t(device_sm_count()) * 8)));
-    Phase ph(s, "part_scatter");
-    count_launch();
-    k_part_scatter<KeyT, V, WI><<<grid, 256, 0, s>>>(keys, p.n, bm, p.part_log2, p.part_cap, pcount, pkeys, pidx,
-                                                     flags);
-  }
-  // partition starts: exclusive scan of pcount[0..P), total into pcount[P]
-  launch_scan(pcount, p.n_parts, pstatus, ticket + 1, nullptr, pcount + p.n_parts, nullptr, s);
+  // status words, tickets, flags, partition counts and their scan states
+  HG_CUDA(cudaMemsetAsync(ws + p.off_status, 0, p.off_pkeys - p.off_status, s), "build: workspace memset");
+  hg_status st = run_partition_passes<KeyT, V, WI>(g, p.n, keys, nullptr, bm, ws, p.off_flags, p.off_ticket,
+                                                   p.off_pcount, p.off_pstatus, p.off_fcount, p.off_fstatus,
+                                                   p.off_pkeys, p.off_pidx, p.off_fkeys, p.off_fidx, "build", s);
+  if (st != HG_OK) return st;
   {
-    const size_t smem = (size_t(1) << p.part_log2) * sizeof(uint32_t);
-    auto kern = k_part_local<KeyT, WI, PART_LOCAL_BLOCK>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess)
-      return HG_ERR_CUDA;
-    const int grid = static_cast<int>(std::min<uint64_t>(p.n_parts, uint64_t(device_sm_count()) * 4));
-    Phase ph(s, "part_local");
+    auto kern = k_fine_build<KeyT, WI, FINE_BLOCK>;
+    const int bps = blocks_per_sm(kern, FINE_BLOCK, g.smem3);
+    if (bps <= 0) return lib_fail(HG_ERR_CUDA, "fine-build kernel cannot be resident");
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(g.n_fine, uint64_t(device_sm_count()) * bps));
+    Phase ph(s, "fine_build");
     count_launch();
-    kern<<<std::max(grid, 1), PART_LOCAL_BLOCK, smem, s>>>(pkeys, pidx, pcount, p.n_parts, p.part_cap, p.part_log2,
-                                                            bm, p.n_buckets, offsets, keys_out, idx_out, flags);
+    kern<<<std::max(grid, 1u), FINE_BLOCK, g.smem3, s>>>(
+        reinterpret_cast<const KeyT*>(ws + p.off_fkeys),
+        WI ? reinterpret_cast<const uint32_t*>(ws + p.off_fidx) : nullptr,
+        reinterpret_cast<const uint32_t*>(ws + p.off_fcount), g.n_fine, g.fine_cap, g.fine_log2, bm, p.n_buckets,
+        offsets, keys_out, idx_out, flags);
+    HG_CUDA(cudaPeekAtLastError(), "fine-build launch");
   }
-  // Fallback for overflowed partitions: the direct build, gated on the flag.
+  // Fallback for an overflowed partition (heavy duplicates): the direct build,
+  // gated on the flag.
   return run_direct<KeyT, V, WI>(p, keys, offsets, keys_out, idx_out, ws, flags, s);
 }
 
@@ -462,7 +771,8 @@ hg_status launch_build(const BuildPlan& p, const void* d_keys, uint32_t* d_offse
     st = p.with_index ? dispatch<uint64_t, true>(p, d_keys, d_offsets, d_keys_out, d_idx_out, ws, s)
                       : dispatch<uint64_t, false>(p, d_keys, d_offsets, d_keys_out, d_idx_out, ws, s);
   if (st != HG_OK) return st;
-  return cudaPeekAtLastError() == cudaSuccess ? HG_OK : HG_ERR_CUDA;
+  HG_CUDA(cudaPeekAtLastError(), "build: kernel launch");
+  return HG_OK;
 }
 
 }  // namespace hg

@@ -1,6 +1,7 @@
 // hg_device.cuh -- device primitives shared by the HashGraph kernels (sm_100a).
 #pragma once
 #include <cstdint>
+#include <cstdio>
 #include <cuda_runtime.h>
 #include <cuda/atomic>
 
@@ -73,9 +74,32 @@ struct BucketMap {
 // ---------------------------------------------------------------------------
 __device__ int32_t g_device_error = 0;
 
+// Host-side record of the last CUDA failure inside the library (per thread),
+// returned by hg_last_error().
+inline char* last_error_buffer() {
+  static thread_local char buf[320] = {0};
+  return buf;
+}
+inline hg_status cuda_fail(cudaError_t e, const char* where) {
+  std::snprintf(last_error_buffer(), 320, "%s: %s (%d)", where, cudaGetErrorString(e), static_cast<int>(e));
+  return e == cudaErrorMemoryAllocation ? HG_ERR_OUT_OF_MEMORY : HG_ERR_CUDA;
+}
+inline hg_status lib_fail(hg_status st, const char* what) {
+  std::snprintf(last_error_buffer(), 320, "%s", what);
+  return st;
+}
+#define HG_CUDA(expr, where)                        \
+  do {                                              \
+    const cudaError_t hg_e_ = (expr);               \
+    if (hg_e_ != cudaSuccess) return ::hg::cuda_fail(hg_e_, where); \
+  } while (0)
+
 __device__ __forceinline__ void record_error(int32_t code) {
   atomicCAS(reinterpret_cast<int*>(&g_device_error), 0, code);
 }
+
+__host__ __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+__host__ __device__ constexpr size_t align_up_dev(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ unsigned lanemask_lt() {

@@ -18,21 +18,42 @@ constexpr uint64_t SCAN_TILE = uint64_t(SCAN_BLOCK) * SCAN_ITEMS;
 
 enum BuildPath : int { BUILD_DIRECT = 0, BUILD_PARTITIONED = 1 };
 
+constexpr size_t SMEM_BUDGET = 220 * 1024;  // dynamic shared memory per CTA (B200 opt-in max 227 KB)
+constexpr size_t FINE_SMEM_BUDGET = 72 * 1024;  // pass-3 CTAs: three per SM
+constexpr int PASS1_BLOCK = 512;
+constexpr int PASS1_KPT = 8;                     // pass-1 keys per thread per tile (registers)
+constexpr int PASS1_TILE = PASS1_BLOCK * PASS1_KPT;
+constexpr int SPLIT_BLOCK = 512;
+constexpr int SPLIT_TILE = 8 * SPLIT_BLOCK;     // k_split sorts a tile in registers: 8 records per thread
+constexpr int FINE_BLOCK = 512;
+constexpr uint32_t SPLIT_LOG2_MAX = 6;          // pass 2 splits a coarse partition up to 64 ways
+
+// Geometry of the partitioned (three-pass) paths, shared by build and probe:
+// pass 1 splits the keys into n_parts coarse partitions of 2^coarse_log2
+// buckets (cluster multisplit), pass 2 splits each coarse partition into
+// 2^split_log2 fine partitions of 2^fine_log2 buckets, pass 3 works on one
+// fine partition per CTA in shared memory.
+struct PartGeometry {
+  uint32_t fine_log2 = 0, split_log2 = 0, coarse_log2 = 0;
+  uint64_t n_parts = 0, part_cap = 0;   // coarse partitions and their record slots
+  uint64_t n_fine = 0, fine_cap = 0;    // fine partitions and their record slots
+  uint32_t smem_cap = 0;                // records pass 3 stages in shared memory
+  uint32_t tile1 = 0;                   // pass-1 keys per CTA per tile
+  size_t smem1 = 0, smem2 = 0, smem3 = 0;
+  uint64_t pscan_tiles = 0, fscan_tiles = 0;
+};
+
 struct BuildPlan {
   int path = BUILD_DIRECT;
   uint64_t n = 0, n_buckets = 0;
   int key_bytes = 8;
   bool with_index = false;
-  // direct path: in-place scan over offsets[1..B]
-  uint64_t scan_tiles = 0;
-  // partitioned path
-  uint32_t part_log2 = 0;     // buckets per partition = 2^part_log2
-  uint64_t n_parts = 0;
-  uint64_t part_cap = 0;      // record slots per partition
-  uint64_t pscan_tiles = 0;   // tiles of the partition-count scan
+  uint64_t scan_tiles = 0;  // direct path: in-place scan over offsets[1..B]
+  PartGeometry g;           // partitioned path
   // workspace byte offsets
   size_t off_status = 0, off_ticket = 0, off_flags = 0;
-  size_t off_pcount = 0, off_pkeys = 0, off_pidx = 0;
+  size_t off_pcount = 0, off_pstatus = 0, off_fcount = 0, off_fstatus = 0;
+  size_t off_pkeys = 0, off_pidx = 0, off_fkeys = 0, off_fidx = 0;
   size_t total = 0;
 };
 
@@ -41,17 +62,35 @@ struct BuildPlan {
 hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_index,
                      BuildPlan* plan, int force_path = -1);
 
+enum ProbePath : int { PROBE_DIRECT = 0, PROBE_PARTITIONED = 1 };
+
 struct ProbePlan {
-  int path = 0;               // 0 direct
-  uint64_t nq = 0, n_buckets = 0;
+  int path = PROBE_DIRECT;
+  uint64_t n_a = 0, nq = 0, n_buckets = 0;
   int key_bytes = 8;
+  bool a_idx = false;
   bool emit = false;
-  uint64_t tiles = 0;
-  size_t off_status = 0, off_ticket = 0;
+  uint64_t tiles = 0;  // direct path: tiles of queries
+  PartGeometry g;      // partitioned path (pass 3 stages A's slice)
+  size_t off_status = 0, off_ticket = 0, off_flags = 0;
+  size_t off_pcount = 0, off_pstatus = 0, off_fcount = 0, off_fstatus = 0;
+  size_t off_pkeys = 0, off_pidx = 0, off_fkeys = 0, off_fidx = 0;
   size_t total = 0;
 };
 
-hg_status plan_probe(uint64_t n_buckets, uint64_t nq, int key_bytes, bool emit, ProbePlan* plan);
+hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, int key_bytes, bool emit,
+                     ProbePlan* plan, int force_path = -1);
+
+// Partition geometry for `n_stream` streamed records of stream_rec bytes
+// (pass 1/2) over n_buckets buckets, with pass 3 staging per fine partition
+// `per_bucket` bytes per bucket plus up to smem_cap records of smem_rec bytes
+// sized for n_staged records in the table.  Returns false if infeasible.
+// With staged_may_spill, a table too dense to stage still gets the narrowest
+// fine width and as many staged records as fit (the rest is read in place).
+// Pass 3 also keeps stream_smem bytes per streamed record of a fine partition.
+bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size_t smem_rec, size_t per_bucket,
+                   size_t stream_smem, uint64_t n_buckets, bool staged_may_spill, PartGeometry* g);
+uint64_t slack_capacity(double mean, uint64_t margin);
 
 // Kernel launchers (hg_build.cu / hg_probe.cu).  Workspace pointers are
 // already carved by the caller; all launches go to `stream`.

@@ -58,6 +58,10 @@ const char* hg_status_str(hg_status status);
 /* Library version, e.g. "hashgraph_b200 0.1 sm_100a". */
 const char* hg_version(void);
 
+/* Description of the last failure inside the library on this host thread
+ * (the call site and the CUDA error string), or "" (thread-local storage). */
+const char* hg_last_error(void);
+
 /* Host form of the bucket hash: murmur3_x86_32 of the low 32 bits of `key`,
  * seed 0.  Replaces the __host__ side of hash_murmur
  * (include/SingleHashGraphOperators.cuh:31-69). */
@@ -93,7 +97,9 @@ hg_status hg_build_into(const void* d_keys, uint64_t n, int key_bytes, uint64_t 
  * src/SingleHashGraph.cu:187-213), 1 = partitioned (bucket-range partition
  * pass, then one shared-memory build per partition: the role of the
  * reference's LRB build, src/SingleHashGraph.cu:129-181, chosen there by
- * #define LRB_BUILD, :64), -1 = planner's choice. */
+ * #define LRB_BUILD, :64), -1 = planner's choice.  A table too dense for the
+ * partitioned path's shared-memory staging (nearly all keys in a few buckets)
+ * is built by the direct path even when path 1 is asked for. */
 hg_status hg_build_workspace_size_path(uint64_t n, int key_bytes, uint64_t n_buckets, int with_index,
                                        int path, size_t* bytes);
 hg_status hg_build_into_path(const void* d_keys, uint64_t n, int key_bytes, uint64_t n_buckets,
@@ -140,9 +146,10 @@ void hg_table_free(hg_table* table);
  * word records HG_ERR_PAIR_CAPACITY.  d_pairs == NULL counts only.
  * ---------------------------------------------------------------------- */
 
-/* Device scratch bytes for hg_intersect_into. */
-hg_status hg_intersect_workspace_size(uint64_t n_buckets, uint64_t nq, int key_bytes,
-                                      int emit_pairs, size_t* bytes);
+/* Device scratch bytes for hg_intersect_into against a table of n_a keys
+ * (with or without an index). */
+hg_status hg_intersect_workspace_size(uint64_t n_a, int a_has_index, uint64_t n_buckets, uint64_t nq,
+                                      int key_bytes, int emit_pairs, size_t* bytes);
 
 /* Probes nq query keys (same key width as A) against table A. */
 hg_status hg_intersect_into(const uint32_t* d_a_offsets, const void* d_a_keys,
@@ -151,6 +158,21 @@ hg_status hg_intersect_into(const uint32_t* d_a_offsets, const void* d_a_keys,
                             const uint32_t* d_query_idx, uint32_t* d_pairs, uint64_t pair_cap,
                             unsigned long long* d_count, void* d_workspace,
                             size_t workspace_bytes, hg_stream_t stream);
+
+/* Same with the probe path fixed: 0 = direct (every query reads its bucket
+ * from A in HBM), 1 = partitioned (queries are split by bucket range, A's
+ * slice of each range is staged in shared memory), -1 = planner's choice.
+ * As for the build, path 1 falls back to the direct probe when the buckets
+ * are too few to split the queries. */
+hg_status hg_intersect_workspace_size_path(uint64_t n_a, int a_has_index, uint64_t n_buckets,
+                                           uint64_t nq, int key_bytes, int emit_pairs, int path,
+                                           size_t* bytes);
+hg_status hg_intersect_into_path(const uint32_t* d_a_offsets, const void* d_a_keys,
+                                 const uint32_t* d_a_idx, uint64_t n_a, uint64_t n_buckets,
+                                 int key_bytes, const void* d_query, uint64_t nq,
+                                 const uint32_t* d_query_idx, uint32_t* d_pairs, uint64_t pair_cap,
+                                 unsigned long long* d_count, void* d_workspace,
+                                 size_t workspace_bytes, int path, hg_stream_t stream);
 
 /* Same, on an hg_table; allocates its scratch per call (stream-ordered). */
 hg_status hg_intersect(const hg_table* a, const void* d_query, uint64_t nq,

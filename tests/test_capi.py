@@ -61,7 +61,7 @@ def test_argument_checks_without_device(capi):
     assert L.hg_build_workspace_size(1 << 32, 4, 1000, 0, ctypes.byref(out)) == -6
     assert L.hg_build_workspace_size(1000, 4, (1 << 32) + 1, 0, ctypes.byref(out)) == -6
     assert L.hg_build_workspace_size(1000, 4, 1000, 0, None) == -1
-    assert L.hg_intersect_workspace_size(1000, 10, 5, 1, ctypes.byref(out)) == -8
+    assert L.hg_intersect_workspace_size(1000, 0, 1000, 10, 5, 1, ctypes.byref(out)) == -8
     assert L.hg_build_into(None, 10, 8, 10, None, None, None, None, 0, None) == -1
     assert L.hg_table_create(10, 8, 10, 0, None) == -1
     assert L.hg_zipf_cdf(None, 10, 1.1) == -1
@@ -74,13 +74,26 @@ def test_workspace_plans(capi):
     assert L.hg_build_workspace_size_path(1 << 20, 4, 1 << 20, 0, 0, ctypes.byref(out)) == 0
     direct = out.value
     assert direct < (1 << 20)
-    # partitioned path: partition buffers hold every key (+ index) with slack
+    # partitioned path: coarse and fine partition buffers each hold every key
+    # (+ index) with a few percent of slack
     assert L.hg_build_workspace_size_path(1 << 20, 4, 1 << 20, 1, 1, ctypes.byref(out)) == 0
     part = out.value
-    assert (1 << 20) * 8 <= part < (1 << 20) * 8 * 1.5
+    assert 2 * (1 << 20) * 8 <= part < (1 << 20) * 8 * 2.5
     # the planner picks the partitioned path for a 2^28 x u64 table
     assert L.hg_build_workspace_size(1 << 28, 8, 1 << 28, 0, ctypes.byref(out)) == 0
     assert out.value >= (1 << 28) * 8
+    # and for probing 2^28 queries against it (queries + their index staged)
+    assert L.hg_intersect_workspace_size(1 << 28, 0, 1 << 28, 1 << 28, 8, 1, ctypes.byref(out)) == 0
+    assert out.value >= 2 * (1 << 28) * 12
+    # a single bucket cannot be split finely: asking for the partitioned
+    # probe (or build) plans the direct one
+    assert L.hg_intersect_workspace_size_path(1 << 15, 0, 1, 1 << 15, 4, 1, 1, ctypes.byref(out)) == 0
+    assert out.value < (1 << 16)
+    assert L.hg_build_workspace_size_path(1 << 15, 4, 1, 0, 1, ctypes.byref(out)) == 0
+    assert out.value < (1 << 16)
+    # a small probe stays direct: only tile status words
+    assert L.hg_intersect_workspace_size(1 << 16, 0, 1 << 16, 1 << 16, 8, 1, ctypes.byref(out)) == 0
+    assert out.value < (1 << 16)
 
 
 def test_zipf_cdf_matches_oracle(capi):

@@ -23,20 +23,39 @@ def _oracle_pairs(a_keys_np, B, with_index, q_np):
     return c, pairs
 
 
+@pytest.mark.parametrize("probe_path", [0, 1])
 @pytest.mark.parametrize("path", [0, 1])
 @pytest.mark.parametrize("kb", [4, 8])
 @pytest.mark.parametrize("na,nq,B,frac", [(1 << 16, 1 << 16, 1 << 16, 0.5), (70_001, 30_000, 12_345, 0.25),
-                                          (5000, 90_000, 1 << 14, 1.0), (1 << 15, 1 << 15, 1, 0.1)])
-def test_intersect_pairs_with_index(hg, path, kb, na, nq, B, frac):
+                                          (5000, 90_000, 1 << 14, 1.0), (1 << 15, 1 << 15, 1, 0.1),
+                                          (300_000, 200_000, 1 << 20, 0.5)])
+def test_intersect_pairs_with_index(hg, probe_path, path, kb, na, nq, B, frac):
     a = oracle.gen_uniform(na, kb, 31 + na)
     q = oracle.gen_overlap(nq, a, frac, 37 + nq)
     t = hg.Table.build(from_np_u(a), B, with_index=True, path=path)
-    count, pairs = t.intersect(from_np_u(q), pair_cap=nq * 2)
+    count, pairs = t.intersect(from_np_u(q), pair_cap=nq * 2, path=probe_path)
     c = int(count.item())
     oc, op = _oracle_pairs(a, B, True, q)
     assert c == oc
     np.testing.assert_array_equal(_sorted_pairs(to_np_u(pairs[:c], 4)), _sorted_pairs(op))
+    count2, _ = t.intersect(from_np_u(q), emit=False, path=probe_path)
+    assert int(count2.item()) == oc
     assert hg.device_error() == 0
+
+
+@pytest.mark.parametrize("probe_path", [0, 1])
+def test_intersect_without_index_table(hg, probe_path):
+    a = oracle.gen_uniform(200_000, 8, 41)
+    q = oracle.gen_overlap(150_000, a, 0.3, 42)
+    t = hg.Table.build(from_np_u(a), 1 << 17, with_index=False, path=1)
+    count, pairs = t.intersect(from_np_u(q), path=probe_path)
+    c = int(count.item())
+    p = to_np_u(pairs[:c], 4)
+    csr_keys = to_np_u(t.view_keys(), 8)
+    assert np.all(csr_keys[p[:, 0]] == q[p[:, 1]])
+    oc, op = _oracle_pairs(a, 1 << 17, True, q)
+    assert c == oc
+    np.testing.assert_array_equal(np.sort(p[:, 1]), np.sort(op[:, 1]))
 
 
 @pytest.mark.parametrize("kb", [4, 8])
@@ -55,30 +74,33 @@ def test_intersect_without_index_refers_to_csr_positions(hg, kb):
     np.testing.assert_array_equal(np.sort(q[p[:, 1]]), np.sort(q[op[:, 1]]))
 
 
-def test_intersect_duplicates_multiply(hg):
-    """Multiset join: k copies in A and m in the queries give k*m matches."""
+@pytest.mark.parametrize("probe_path", [0, 1])
+def test_intersect_duplicates_multiply(hg, probe_path):
+    """Multiset join: k copies in A and m in the queries give k*m matches.
+    The partitioned probe overflows its query partitions / spills owners here."""
     a = (oracle.gen_uniform(30_000, 8, 8) % np.uint64(200)).astype(np.uint64)
     q = (oracle.gen_uniform(20_000, 8, 9) % np.uint64(300)).astype(np.uint64)
     t = hg.Table.build(from_np_u(a), 4096, with_index=True)
     expect = oracle.join_count(a, q)
-    count, _ = t.intersect(from_np_u(q), emit=False)
+    count, _ = t.intersect(from_np_u(q), emit=False, path=probe_path)
     assert int(count.item()) == expect
-    count, pairs = t.intersect(from_np_u(q), pair_cap=expect)
+    count, pairs = t.intersect(from_np_u(q), pair_cap=expect, path=probe_path)
     assert int(count.item()) == expect
     oc, op = _oracle_pairs(a, 4096, True, q)
     np.testing.assert_array_equal(_sorted_pairs(to_np_u(pairs, 4)), _sorted_pairs(op))
 
 
-def test_intersect_pair_capacity(hg):
+@pytest.mark.parametrize("probe_path", [0, 1])
+def test_intersect_pair_capacity(hg, probe_path):
     """Too small a pair buffer: exact count, pairs truncated, error recorded."""
     a = oracle.gen_uniform(1 << 15, 4, 10)
     q = oracle.gen_overlap(1 << 15, a, 0.75, 11)
     t = hg.Table.build(from_np_u(a), 1 << 15, with_index=True)
-    full, _ = t.intersect(from_np_u(q), emit=False)
+    full, _ = t.intersect(from_np_u(q), emit=False, path=probe_path)
     c = int(full.item())
     assert hg.device_error() == 0
     cap = c // 3
-    count, pairs = t.intersect(from_np_u(q), pair_cap=cap)
+    count, pairs = t.intersect(from_np_u(q), pair_cap=cap, path=probe_path)
     assert int(count.item()) == c
     assert hg.device_error() == hg.ERR_PAIR_CAPACITY
     p = to_np_u(pairs[:cap], 4)

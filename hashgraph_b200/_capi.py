@@ -48,6 +48,7 @@ SIGNATURES = {
     "hg_build_into": (_i32, [_p, _u64, _int, _u64, _p, _p, _p, _p, _sz, _p]),
     "hg_build_workspace_size_path": (_i32, [_u64, _int, _u64, _int, _int, ctypes.POINTER(_sz)]),
     "hg_build_into_path": (_i32, [_p, _u64, _int, _u64, _p, _p, _p, _p, _sz, _int, _p]),
+    "hg_build_into_noalloc": (_i32, [_p, _u64, _int, _u64, _p, _p, _p, _p]),
     "hg_table_create": (_i32, [_u64, _int, _u64, _int, _pp]),
     "hg_table_build": (_i32, [_p, _p, _u64, _p]),
     "hg_build": (_i32, [_p, _u64, _int, _u64, _int, _pp, _p]),

@@ -5,3 +5,4 @@
 #include "hg_probe.cu"
 #include "hg_gen.cu"
 #include "hg_api.cu"
+#include "hg_noalloc.cu"

@@ -106,6 +106,21 @@ hg_status hg_build_into_path(const void* d_keys, uint64_t n, int key_bytes, uint
                              uint32_t* d_offsets, void* d_keys_out, uint32_t* d_idx_out,
                              void* d_workspace, size_t workspace_bytes, int path, hg_stream_t stream);
 
+/* Allocation-free build (no counterpart in the reference).  For callers that
+ * must not allocate device memory when they build a table: a process whose
+ * HBM is handed out by its own pool allocator, code running inside another
+ * allocator's callback, or a loop that forbids cudaMalloc after start-up.
+ * Same arguments and result as hg_build_into on the direct path, but the
+ * scratch is a fixed 64 KiB array inside this library (held on every GPU
+ * that loads it), so n_buckets is limited to 2^25 = 33554432; larger values
+ * return HG_ERR_TOO_LARGE.  The caller provides keys and outputs.  The first
+ * call on a device looks up the array's device address; make it before any
+ * stream capture.  All calls share the array: calls whose work overlaps on
+ * the GPU race and must be serialised by the caller. */
+hg_status hg_build_into_noalloc(const void* d_keys, uint64_t n, int key_bytes, uint64_t n_buckets,
+                                uint32_t* d_offsets, void* d_keys_out, uint32_t* d_idx_out,
+                                hg_stream_t stream);
+
 /* ------------------------------------------------------------------------
  * Library-owned tables.
  * ---------------------------------------------------------------------- */

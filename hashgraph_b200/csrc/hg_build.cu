@@ -35,6 +35,7 @@
 #include <tuple>
 
 #include "hg_device.cuh"
+#include "hg_bulk.cuh"
 #include "hg_cluster.cuh"
 #include "hg_plan.h"
 #include "hg_prof.cuh"
@@ -193,20 +194,21 @@ __global__ void k_fill_u32(uint32_t* p, uint64_t count, uint32_t value, const ui
 // ---------------------------------------------------------------------------
 
 // Pass 1: cluster multisplit.  A cluster of CL CTAs takes a tile of
-// CL*TILE consecutive keys (TILE = BLOCK*KPT, held in registers); every CTA
-// ranks its keys per coarse partition with shared-memory atomics, the cluster
-// sums the per-CTA histograms over DSMEM (CTA c owns partitions
-// [c*P/CL, (c+1)*P/CL)), each owner reserves the cluster's run in partition
-// p with ONE global atomic and hands every CTA its start, and each CTA writes
-// its keys partition-sorted (shared-memory counting sort) so the runs leave
-// as coalesced stores.
-// Dynamic smem: hist[P] | lp[P] | start[P] | sk[TILE] | si[TILE] | sp[TILE] (u16)
-template <typename KeyT, bool WITH_IDX, int BLOCK, int KPT>
+// CL*TILE consecutive keys (TILE = BLOCK*KPT per CTA); every CTA ranks its
+// keys per coarse partition with shared-memory atomics, the cluster sums the
+// per-CTA histograms over DSMEM (CTA c owns partitions [c*P/CL, (c+1)*P/CL)),
+// each owner reserves the cluster's run in partition p with ONE global atomic
+// and hands every CTA its start, and each CTA writes its keys
+// partition-sorted (shared-memory counting sort) so the runs leave as
+// coalesced stores.  With BULK, the CTA's next tile is prefetched into shared
+// memory by a bulk copy (TMA) while the current one is processed.
+// Dynamic smem: hist[P] | lp[P] | start[P] | raw[2][TILE] | si[TILE] | sp[TILE] (u16)
+template <typename KeyT, bool WITH_IDX, int BLOCK, int KPT, bool BULK>
 __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict__ keys, const uint32_t* __restrict__ key_idx,
-                                                      uint64_t n, BucketMap bm, uint32_t coarse_log2, uint32_t n_parts,
-                                                      uint64_t cap, uint32_t* __restrict__ pcount,
-                                                      KeyT* __restrict__ pkeys, uint32_t* __restrict__ pidx,
-                                                      uint32_t* flags) {
+                                                         uint64_t n, BucketMap bm, uint32_t coarse_log2, uint32_t n_parts,
+                                                         uint64_t cap, uint32_t* __restrict__ pcount,
+                                                         KeyT* __restrict__ pkeys, uint32_t* __restrict__ pidx,
+                                                         uint32_t* flags) {
   constexpr uint32_t TILE = BLOCK * KPT;
   cg::cluster_group cluster = cg::this_cluster();
   const unsigned CL = cluster.num_blocks();
@@ -215,27 +217,65 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict_
   uint32_t* hist = reinterpret_cast<uint32_t*>(smem_raw);
   uint32_t* lp = hist + n_parts;
   uint32_t* start = lp + n_parts;
-  KeyT* sk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(n_parts) * 12, 16));
-  uint32_t* si = reinterpret_cast<uint32_t*>(sk + TILE);
-  uint16_t* sp = reinterpret_cast<uint16_t*>(WITH_IDX ? reinterpret_cast<unsigned char*>(si + TILE)
-                                                      : reinterpret_cast<unsigned char*>(si));
+  KeyT* raw = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(n_parts) * 12, 16));
+  uint32_t* si = reinterpret_cast<uint32_t*>(raw + 2 * TILE);
+  uint16_t* sp = reinterpret_cast<uint16_t*>(si + TILE);
   __shared__ uint32_t wsum[BLOCK / 32 + 1];
+  __shared__ uint64_t bar[2];
   const uint64_t cluster_id = blockIdx.x / CL, nclusters = gridDim.x / CL;
   const uint64_t ctile = uint64_t(CL) * TILE;
   const uint64_t ntiles = (n + ctile - 1) / ctile;
   const uint32_t per = (n_parts + CL - 1) / CL;
   const uint32_t p0 = min(n_parts, rank * per), p1 = min(n_parts, p0 + per);
+  auto tile_base = [&](uint64_t ct) { return ct * ctile + uint64_t(rank) * TILE; };
+  auto tile_cnt = [&](uint64_t ct) -> uint32_t {
+    const uint64_t b = tile_base(ct);
+    return b < n ? static_cast<uint32_t>(umin64(TILE, n - b)) : 0u;
+  };
+  // bulk part of a tile: whole 16-byte units; the ragged tail is read with plain loads
+  auto bulk_bytes = [&](uint32_t cnt) -> uint32_t { return (cnt * uint32_t(sizeof(KeyT))) & ~15u; };
+  if constexpr (BULK) {
+    if (threadIdx.x == 0) {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+      fence_mbar_init();
+      if (cluster_id < ntiles) bulk_load(raw, keys + tile_base(cluster_id), bulk_bytes(tile_cnt(cluster_id)), &bar[0]);
+    }
+    __syncthreads();
+  }
   bool overflow = false;
-  for (uint64_t ct = cluster_id; ct < ntiles; ct += nclusters) {
-    const uint64_t base = ct * ctile + uint64_t(rank) * TILE;
-    const uint32_t cnt = base < n ? static_cast<uint32_t>(umin64(TILE, n - base)) : 0u;
+  bool timed_out = false;
+  uint32_t it = 0;
+  for (uint64_t ct = cluster_id; ct < ntiles; ct += nclusters, it++) {
+    const uint64_t base = tile_base(ct);
+    const uint32_t cnt = tile_cnt(ct);
+    KeyT* cur = raw + (it & 1) * TILE;
+    if constexpr (BULK) {
+      // prefetch the next tile into the other buffer (its readers finished at
+      // the __syncthreads that closed the previous iteration)
+      if (threadIdx.x == 0 && ct + nclusters < ntiles) {
+        fence_proxy_async_smem();
+        const uint64_t nx = ct + nclusters;
+        bulk_load(raw + ((it + 1) & 1) * TILE, keys + tile_base(nx), bulk_bytes(tile_cnt(nx)), &bar[(it + 1) & 1]);
+      }
+    }
     for (uint32_t j = threadIdx.x; j < n_parts; j += BLOCK) hist[j] = 0u;
     KeyT k[KPT];
     uint32_t pr[KPT];
+    if constexpr (BULK) {
+      if (!mbar_wait(&bar[it & 1], (it >> 1) & 1)) timed_out = true;
+      const uint32_t nb = bulk_bytes(cnt) / uint32_t(sizeof(KeyT));
 #pragma unroll
-    for (int u = 0; u < KPT; u++) {
-      const uint32_t r = u * BLOCK + threadIdx.x;
-      k[u] = r < cnt ? __ldcs(keys + base + r) : KeyT(0);
+      for (int u = 0; u < KPT; u++) {
+        const uint32_t r = u * BLOCK + threadIdx.x;
+        k[u] = r < nb ? cur[r] : (r < cnt ? keys[base + r] : KeyT(0));
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < KPT; u++) {
+        const uint32_t r = u * BLOCK + threadIdx.x;
+        k[u] = r < cnt ? __ldcs(keys + base + r) : KeyT(0);
+      }
     }
     __syncthreads();
 #pragma unroll
@@ -247,10 +287,12 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict_
       }
     }
     __syncthreads();
+    // the histogram is complete: let the owners start while this CTA scans it
+    cluster.barrier_arrive();
     for (uint32_t j = threadIdx.x; j < n_parts; j += BLOCK) lp[j] = hist[j];
     __syncthreads();
     block_scan_segments<BLOCK>(lp, n_parts, 0u, 0u, wsum, [](uint32_t, uint32_t) {});
-    cluster.sync();
+    cluster.barrier_wait();
     // owners: sum the cluster's histograms for their partitions and reserve
     for (uint32_t p = p0 + threadIdx.x; p < p1; p += BLOCK) {
       uint32_t h[16];
@@ -266,24 +308,27 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict_
         run += h[c];
       }
     }
-    cluster.sync();
+    // the starts are written; the local counting sort needs only lp, so it
+    // runs while the cluster barrier completes
+    cluster.barrier_arrive();
 #pragma unroll
     for (int u = 0; u < KPT; u++) {
       const uint32_t r = u * BLOCK + threadIdx.x;
       if (r < cnt) {
         const uint32_t p = pr[u] >> 16;
         const uint32_t pos = lp[p] + (pr[u] & 0xffffu);
-        sk[pos] = k[u];
+        cur[pos] = k[u];
         sp[pos] = static_cast<uint16_t>(p);
         if constexpr (WITH_IDX) si[pos] = key_idx ? key_idx[base + r] : static_cast<uint32_t>(base + r);
       }
     }
     __syncthreads();
+    cluster.barrier_wait();
     for (uint32_t s = threadIdx.x; s < cnt; s += BLOCK) {
       const uint32_t p = sp[s];
       const uint64_t off = uint64_t(start[p]) + (s - lp[p]);
       if (off < cap) {
-        pkeys[uint64_t(p) * cap + off] = sk[s];
+        pkeys[uint64_t(p) * cap + off] = cur[s];
         if constexpr (WITH_IDX) pidx[uint64_t(p) * cap + off] = si[s];
       } else {
         overflow = true;
@@ -291,50 +336,112 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict_
     }
     __syncthreads();
   }
+  if constexpr (BULK) {
+    // no copy is left in flight: the last iteration issued none
+    (void)timed_out;
+  }
   if (overflow) atomicOr(flags, FLAG_OVERFLOW);
 }
 
 // Pass 2: split every coarse partition S ways into fine partitions of W
-// buckets.  One CTA per tile of a coarse partition's records: a
-// shared-memory counting sort by fine partition, one global atomic per
-// (tile, fine partition) to reserve the run, coalesced run writes.
-// Dynamic smem: hist[S] | lp[S] | base[S] | pr[tile] | sk[tile] | si[tile]
+// buckets.  One CTA per tile of a coarse partition's records (bulk-copied,
+// the next tile prefetched while this one is sorted): a shared-memory
+// counting sort by fine partition, one global atomic per (tile, fine
+// partition) to reserve the run, coalesced run writes.
+// Dynamic smem: hist[S] | lp[S] | base[S] | rk[2][TILE] | ri[2][TILE] | sp[TILE] (u16)
 template <typename KeyT, bool WITH_IDX, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys, const uint32_t* __restrict__ pidx,
                                                  const uint32_t* __restrict__ pstart, uint32_t n_parts, uint64_t cap1,
-                                                 uint32_t tiles_per_part, uint32_t tile, BucketMap bm,
-                                                 uint32_t fine_log2, uint32_t split_log2, uint64_t capf,
-                                                 uint32_t* __restrict__ fcount, KeyT* __restrict__ fkeys,
-                                                 uint32_t* __restrict__ fidx, uint32_t* flags) {
+                                                 uint32_t tiles_per_part, BucketMap bm, uint32_t fine_log2,
+                                                 uint32_t split_log2, uint64_t capf, uint32_t* __restrict__ fcount,
+                                                 KeyT* __restrict__ fkeys, uint32_t* __restrict__ fidx,
+                                                 uint32_t* flags) {
+  constexpr uint32_t KPT = 8;
+  constexpr uint32_t TILE = BLOCK * KPT;
   if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t S = 1u << split_log2;
   uint32_t* hist = reinterpret_cast<uint32_t*>(smem_raw);
   uint32_t* lp = hist + S;
   uint32_t* base = lp + S;
-  uint32_t* pr = base + S;
-  KeyT* sk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(S) * 12 + size_t(tile) * 4, 16));
-  uint32_t* si = reinterpret_cast<uint32_t*>(sk + tile);
+  KeyT* rk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(S) * 12, 16));
+  uint32_t* ri = reinterpret_cast<uint32_t*>(rk + 2 * TILE);
+  uint16_t* sp = reinterpret_cast<uint16_t*>(ri + (WITH_IDX ? 2 * TILE : 0));
+  __shared__ uint64_t bar[2];
+  __shared__ uint64_t s_next;
+  __shared__ uint32_t s_next_cnt;
   const uint32_t coarse_log2 = fine_log2 + split_log2;
-  bool overflow = false;
   const uint64_t vtiles = uint64_t(n_parts) * tiles_per_part;
-  for (uint64_t vt = blockIdx.x; vt < vtiles; vt += gridDim.x) {
+  // first valid virtual tile at or after vt (stepping by the grid); vtiles if none
+  auto next_valid = [&](uint64_t vt, uint32_t* cnt) -> uint64_t {
+    for (; vt < vtiles; vt += gridDim.x) {
+      const uint64_t q = vt / tiles_per_part;
+      const uint32_t r0 = static_cast<uint32_t>(vt % tiles_per_part) * TILE;
+      const uint32_t m = pstart[q + 1] - pstart[q];
+      if (r0 < m) {
+        *cnt = min(TILE, m - r0);
+        return vt;
+      }
+    }
+    *cnt = 0;
+    return vtiles;
+  };
+  auto issue = [&](uint64_t vt, uint32_t cnt, uint32_t buf) {
     const uint64_t q = vt / tiles_per_part;
-    const uint32_t r0 = static_cast<uint32_t>(vt % tiles_per_part) * tile;
-    const uint32_t m = pstart[q + 1] - pstart[q];
-    if (r0 >= m) continue;  // uniform across the block
-    const uint32_t cnt = min(tile, m - r0);
-    const KeyT* src = pkeys + q * cap1 + r0;
-    const uint32_t* srci = pidx + q * cap1 + r0;
+    const uint64_t r0 = (vt % tiles_per_part) * TILE;
+    const uint32_t bk = (cnt * uint32_t(sizeof(KeyT)) + 15u) & ~15u;  // stays inside the partition's slots
+    const uint32_t bi = WITH_IDX ? ((cnt * 4u + 15u) & ~15u) : 0u;
+    mbar_arrive_expect_tx(&bar[buf], bk + bi);
+    bulk_g2s(rk + buf * TILE, pkeys + q * cap1 + r0, bk, &bar[buf]);
+    if constexpr (WITH_IDX) bulk_g2s(ri + buf * TILE, pidx + q * cap1 + r0, bi, &bar[buf]);
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+    uint32_t c0;
+    const uint64_t v0 = next_valid(blockIdx.x, &c0);
+    if (v0 < vtiles) issue(v0, c0, 0);
+    s_next = v0;
+    s_next_cnt = c0;
+  }
+  __syncthreads();
+  bool overflow = false;
+  uint32_t it = 0;
+  while (true) {
+    const uint64_t vt = s_next;
+    const uint32_t cnt = s_next_cnt;
+    if (vt >= vtiles) break;
+    const uint32_t buf = it & 1;
+    __syncthreads();  // everyone has read s_next before thread 0 moves it
+    if (threadIdx.x == 0) {
+      uint32_t cn;
+      const uint64_t nx = next_valid(vt + gridDim.x, &cn);
+      if (nx < vtiles) {
+        fence_proxy_async_smem();
+        issue(nx, cn, buf ^ 1u);
+      }
+      s_next = nx;
+      s_next_cnt = cn;
+    }
+    const uint64_t q = vt / tiles_per_part;
     const uint64_t b0 = q << coarse_log2;
+    KeyT* ck = rk + buf * TILE;
+    uint32_t* ci = ri + buf * TILE;
     for (uint32_t j = threadIdx.x; j < S; j += BLOCK) hist[j] = 0u;
+    mbar_wait(&bar[buf], (it >> 1) & 1);
     __syncthreads();
-    for (uint32_t r = threadIdx.x; r < cnt; r += BLOCK) {
-      const KeyT k = src[r];
-      const uint32_t f = static_cast<uint32_t>(bm.of_key(k) - b0) >> fine_log2;
-      const uint32_t rk = atomicAdd(&hist[f], 1u);
-      pr[r] = (f << 16) | rk;
-      sk[r] = k;  // unsorted copy; sorted below into the same tile slots via pr
+    KeyT kk[KPT];
+    uint32_t ii[KPT], pp[KPT];
+#pragma unroll
+    for (int u = 0; u < KPT; u++) {
+      const uint32_t r = u * BLOCK + threadIdx.x;
+      if (r < cnt) {
+        kk[u] = ck[r];
+        if constexpr (WITH_IDX) ii[u] = ci[r];
+        const uint32_t f = static_cast<uint32_t>(bm.of_key(kk[u]) - b0) >> fine_log2;
+        pp[u] = (f << 16) | atomicAdd(&hist[f], 1u);
+      }
     }
     __syncthreads();
     if (threadIdx.x < 32) {  // exclusive scan of S <= 1024 counts by one warp
@@ -354,54 +461,41 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
       base[f] = b;
     }
     __syncthreads();
-    // counting sort of the tile: read the unsorted record, keep it in a
-    // register across the barrier, write it to its sorted slot
-    KeyT kk[8];
-    uint32_t ii[8], pp[8];
-    for (uint32_t r1 = 0; r1 < cnt; r1 += 8 * BLOCK) {
 #pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const uint32_t r = r1 + u * BLOCK + threadIdx.x;
-        if (r < cnt) {
-          const uint32_t v = pr[r];
-          pp[u] = lp[v >> 16] + (v & 0xffffu);
-          kk[u] = sk[r];
-          if constexpr (WITH_IDX) ii[u] = srci[r];
-        }
+    for (int u = 0; u < KPT; u++) {
+      const uint32_t r = u * BLOCK + threadIdx.x;
+      if (r < cnt) {
+        const uint32_t f = pp[u] >> 16;
+        const uint32_t pos = lp[f] + (pp[u] & 0xffffu);
+        ck[pos] = kk[u];
+        sp[pos] = static_cast<uint16_t>(f);
+        if constexpr (WITH_IDX) ci[pos] = ii[u];
       }
-      __syncthreads();
-#pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const uint32_t r = r1 + u * BLOCK + threadIdx.x;
-        if (r < cnt) {
-          sk[pp[u]] = kk[u];
-          if constexpr (WITH_IDX) si[pp[u]] = ii[u];
-        }
-      }
-      __syncthreads();
     }
+    __syncthreads();
     for (uint32_t s = threadIdx.x; s < cnt; s += BLOCK) {
-      const KeyT k = sk[s];
-      const uint32_t f = static_cast<uint32_t>(bm.of_key(k) - b0) >> fine_log2;
+      const uint32_t f = sp[s];
       const uint64_t off = uint64_t(base[f]) + (s - lp[f]);
       if (off < capf) {
         const uint64_t at = ((q << split_log2) + f) * capf + off;
-        fkeys[at] = k;
-        if constexpr (WITH_IDX) fidx[at] = si[s];
+        fkeys[at] = ck[s];
+        if constexpr (WITH_IDX) fidx[at] = ci[s];
       } else {
         overflow = true;
       }
     }
     __syncthreads();
+    it++;
   }
   if (overflow) atomicOr(flags, FLAG_OVERFLOW);
 }
 
 // Pass 3: one CTA per fine partition of W buckets.  The partition's records
-// are staged in shared memory, counted into W shared counters, the counters
-// are scanned (coalesced offsets write) and the records scattered into the
-// partition's output slice (a few hundred KB, completed while resident in L2).
-// Dynamic smem: ctr[W] | sk[capf] | si[capf]
+// are bulk-copied into shared memory (the next partition's copy is in flight
+// meanwhile), counted into W shared counters, the counters are scanned
+// (coalesced offsets write) and the records scattered into the partition's
+// output slice (a few tens of KB, completed while resident in L2).
+// Dynamic smem: ctr[W] | sk[2][capf] | si[2][capf]
 template <typename KeyT, bool WITH_IDX, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ fkeys, const uint32_t* __restrict__ fidx,
                                                       const uint32_t* __restrict__ fstart, uint64_t n_fine, uint64_t capf,
@@ -413,32 +507,51 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ f
   const uint32_t W = 1u << fine_log2;
   uint32_t* ctr = reinterpret_cast<uint32_t*>(smem_raw);
   KeyT* sk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(W) * 4, 16));
-  uint32_t* si = reinterpret_cast<uint32_t*>(sk + capf);
+  uint32_t* si = reinterpret_cast<uint32_t*>(sk + 2 * capf);
   __shared__ uint32_t wsum[BLOCK / 32 + 1];
+  __shared__ uint64_t bar[2];
   if (blockIdx.x == 0 && threadIdx.x == 0) offsets[n_buckets] = fstart[n_fine];
-  for (uint64_t f = blockIdx.x; f < n_fine; f += gridDim.x) {
+  const uint64_t n_live = umin64(n_fine, (n_buckets + W - 1) >> fine_log2);  // partitions holding buckets
+  auto issue = [&](uint64_t f, uint32_t buf) {
+    const uint32_t m = fstart[f + 1] - fstart[f];
+    const uint32_t bk = (m * uint32_t(sizeof(KeyT)) + 15u) & ~15u;
+    const uint32_t bi = WITH_IDX ? ((m * 4u + 15u) & ~15u) : 0u;
+    mbar_arrive_expect_tx(&bar[buf], bk + bi);
+    bulk_g2s(sk + buf * capf, fkeys + f * capf, bk, &bar[buf]);
+    if constexpr (WITH_IDX) bulk_g2s(si + buf * capf, fidx + f * capf, bi, &bar[buf]);
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+    if (blockIdx.x < n_live) issue(blockIdx.x, 0);
+  }
+  __syncthreads();
+  uint32_t it = 0;
+  for (uint64_t f = blockIdx.x; f < n_live; f += gridDim.x, it++) {
+    const uint32_t buf = it & 1;
+    if (threadIdx.x == 0 && f + gridDim.x < n_live) {
+      fence_proxy_async_smem();
+      issue(f + gridDim.x, buf ^ 1u);
+    }
     const uint64_t b0 = f << fine_log2;
-    if (b0 >= n_buckets) break;  // fine partitions are in bucket order
     const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
     const uint32_t base = fstart[f];
     const uint32_t m = fstart[f + 1] - base;
-    const KeyT* src = fkeys + f * capf;
-    const uint32_t* srci = fidx + f * capf;
+    const KeyT* ck = sk + buf * capf;
+    const uint32_t* ci = si + buf * capf;
     for (uint32_t j = threadIdx.x; j < nb; j += BLOCK) ctr[j] = 0u;
-    for (uint32_t r = threadIdx.x; r < m; r += BLOCK) {
-      sk[r] = __ldcs(src + r);
-      if constexpr (WITH_IDX) si[r] = __ldcs(srci + r);
-    }
+    mbar_wait(&bar[buf], (it >> 1) & 1);
     __syncthreads();
     for (uint32_t r = threadIdx.x; r < m; r += BLOCK)
-      atomicAdd(&ctr[static_cast<uint32_t>(bm.of_key(sk[r]) - b0)], 1u);
+      atomicAdd(&ctr[static_cast<uint32_t>(bm.of_key(ck[r]) - b0)], 1u);
     __syncthreads();
     block_scan_segments<BLOCK>(ctr, nb, base, base, wsum, [&](uint32_t j, uint32_t g) { offsets[b0 + j] = g; });
     for (uint32_t r = threadIdx.x; r < m; r += BLOCK) {
-      const KeyT k = sk[r];
+      const KeyT k = ck[r];
       const uint32_t pos = atomicAdd(&ctr[static_cast<uint32_t>(bm.of_key(k) - b0)], 1u);
       keys_out[pos] = k;
-      if constexpr (WITH_IDX) idx_out[pos] = si[r];
+      if constexpr (WITH_IDX) idx_out[pos] = ci[r];
     }
     __syncthreads();
   }
@@ -525,10 +638,21 @@ static uint32_t ceil_log2_u64(uint64_t x) {
   return l;
 }
 
+size_t pass1_smem(uint64_t n_parts, int key_bytes) {
+  return align_up(12 * n_parts, 16) + size_t(PASS1_TILE) * (2 * key_bytes + 6);
+}
+
+size_t split_smem(uint32_t split_log2, int key_bytes, bool with_index) {
+  return align_up(12 * (size_t(1) << split_log2), 16) +
+         size_t(SPLIT_TILE) * (2 * key_bytes + (with_index ? 8 : 0) + 2);
+}
+
 bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size_t smem_rec, size_t per_bucket,
-                   size_t stream_smem, uint64_t n_buckets, bool staged_may_spill, PartGeometry* out) {
+                   size_t stream_smem, uint64_t n_buckets, bool staged_may_spill, PartGeometry* out,
+                   size_t fine_budget) {
   PartGeometry g;
   bool found = false;
+  const size_t FINE_SMEM_BUDGET = fine_budget;
   for (uint32_t w = 15; w >= 6 && !found; w--) {
     const uint64_t W = 1ull << w;
     const double frac = double(std::min<uint64_t>(W, n_buckets)) / double(n_buckets);
@@ -563,12 +687,14 @@ bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size
   // pass 1: hist/lp/start per coarse partition + a sorted tile (keys, index,
   // 16-bit partition ids)
   g.tile1 = PASS1_TILE;
-  g.smem1 = align_up(12 * g.n_parts, 16) + size_t(PASS1_TILE) * (stream_rec + 2);
-  g.smem2 = align_up(12 * (size_t(1) << g.split_log2) + 4 * size_t(SPLIT_TILE), 16) + size_t(SPLIT_TILE) * stream_rec;
+  // pass 1: hist/lp/start, two raw key tiles, the index and the 16-bit
+  // partition id of the sorted tile (sizes set by the caller, which knows the
+  // key width: pass1_smem / split_smem)
+  g.smem1 = 0;
+  g.smem2 = 0;
   g.pscan_tiles = (g.n_parts + SCAN_TILE - 1) / SCAN_TILE;
   g.fscan_tiles = (g.n_fine + SCAN_TILE - 1) / SCAN_TILE;
-  if (g.smem1 > SMEM_BUDGET || g.n_parts >= 65536 || g.part_cap >= (1ull << 32) || g.fine_cap >= (1ull << 32))
-    return false;
+  if (g.n_parts >= 65536 || g.part_cap >= (1ull << 32) || g.fine_cap >= (1ull << 32)) return false;
   *out = g;
   return true;
 }
@@ -583,7 +709,13 @@ hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_in
   p.key_bytes = key_bytes;
   p.with_index = with_index;
   const size_t rec = key_bytes + (with_index ? 4 : 0);
-  const bool part_ok = plan_geometry(n, rec, n, rec, 4, 0, n_buckets, false, &p.g);
+  // pass 3 double-buffers its partition's records: 2 * rec per staged record
+  bool part_ok = plan_geometry(n, rec, n, 2 * rec, 4, 0, n_buckets, false, &p.g);
+  if (part_ok) {
+    p.g.smem1 = pass1_smem(p.g.n_parts, key_bytes);
+    p.g.smem2 = split_smem(p.g.split_log2, key_bytes, with_index);
+    part_ok = p.g.smem1 <= SMEM_BUDGET && p.g.smem2 <= SMEM_BUDGET;
+  }
   const uint64_t footprint = n * (key_bytes + rec) + 4 * n_buckets;
   int path = force_path;
   if (path < 0) path = (part_ok && footprint > (48ull << 20)) ? BUILD_PARTITIONED : BUILD_DIRECT;
@@ -681,7 +813,7 @@ static hg_status run_partition_passes(const PartGeometry& g, uint64_t n, const K
   KeyT* fkeys = reinterpret_cast<KeyT*>(ws + off_fkeys);
   uint32_t* fidx = WI ? reinterpret_cast<uint32_t*>(ws + off_fidx) : nullptr;
   if (n > 0) {
-    auto kern = k_multisplit<KeyT, WI, PASS1_BLOCK, PASS1_KPT>;
+    auto kern = k_multisplit<KeyT, WI, PASS1_BLOCK, PASS1_KPT, (V > 1)>;
     int ncl = 0;
     const unsigned cl = pick_cluster(kern, PASS1_BLOCK, g.smem1, &ncl);
     if (ncl <= 0) return lib_fail(HG_ERR_CUDA, "no co-resident cluster for the multisplit kernel");
@@ -705,8 +837,8 @@ static hg_status run_partition_passes(const PartGeometry& g, uint64_t n, const K
     Phase ph(s, who[0] == 'b' ? "split" : "probe_split");
     count_launch();
     k_split<KeyT, WI, SPLIT_BLOCK><<<std::max(grid, 1u), SPLIT_BLOCK, g.smem2, s>>>(
-        pkeys, pidx, pcount, static_cast<uint32_t>(g.n_parts), g.part_cap, tiles_per_part, SPLIT_TILE, bm,
-        g.fine_log2, g.split_log2, g.fine_cap, fcount, fkeys, fidx, flags);
+        pkeys, pidx, pcount, static_cast<uint32_t>(g.n_parts), g.part_cap, tiles_per_part, bm, g.fine_log2,
+        g.split_log2, g.fine_cap, fcount, fkeys, fidx, flags);
     HG_CUDA(cudaPeekAtLastError(), "split launch");
   }
   launch_scan(fcount, g.n_fine, fstatus, ticket + 2, nullptr, fcount + g.n_fine, nullptr, s,

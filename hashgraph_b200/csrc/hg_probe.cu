@@ -263,7 +263,12 @@ hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, 
   const size_t a_rec = key_bytes + (a_idx ? 4 : 0);
   const size_t q_rec = key_bytes + 4;  // queries travel with their position
   // pass 3 keeps a 16-bit local bucket and a 32-bit first match per query
-  const bool part_ok = plan_geometry(nq, q_rec, n_a, a_rec, 4, 6, n_buckets, true, &p.g);
+  bool part_ok = plan_geometry(nq, q_rec, n_a, a_rec, 4, 6, n_buckets, true, &p.g, FINE_PROBE_SMEM_BUDGET);
+  if (part_ok) {
+    p.g.smem1 = pass1_smem(p.g.n_parts, key_bytes);
+    p.g.smem2 = split_smem(p.g.split_log2, key_bytes, true);
+    part_ok = p.g.smem1 <= SMEM_BUDGET && p.g.smem2 <= SMEM_BUDGET;
+  }
   const uint64_t a_bytes = n_a * a_rec + 4 * n_buckets;
   int path = force_path;
   if (path < 0) path = (part_ok && a_bytes > (64ull << 20) && nq >= (1ull << 20)) ? PROBE_PARTITIONED : PROBE_DIRECT;

@@ -13,6 +13,12 @@ plus digests of the 2^20-key workload -> ref_multi_digest.json.
 
     python tests/golden/make_golden.py hash  [--out DIR]
     python tests/golden/make_golden.py multi [--out DIR]
+    python tests/golden/make_golden.py timing [--n LOG2] [--key-bytes 8|4]
+
+Part `timing` (GPU): times the reference MultiHashGraph (gpuCount = 1,
+sm_100a) on the seeded build + intersect workload -- A = 2^n uniform keys
+(seed 3), B = 2^n keys with 25% drawn from A (seed 30), tableSize = 2^n --
+with CUDA events as its own test main does, and prints its JSON timing line.
 
 The fixtures only depend on the oracle's generators (oracle/hg_oracle.c), so
 the inputs are regenerated from the parameters stored next to each result.
@@ -131,16 +137,40 @@ def part_multi(out):
     print("digest", digest)
 
 
+def part_timing(log2n, key_bytes):
+    n = 1 << log2n
+    exe = oracle.ref_binary("ref_multi" if key_bytes == 8 else "ref_multi32")
+    a = oracle.gen_uniform(n, key_bytes, 3)
+    b = oracle.gen_overlap(n, a, 0.25, 30)
+    with tempfile.TemporaryDirectory() as td:
+        fa, fb = os.path.join(td, "a.bin"), os.path.join(td, "b.bin")
+        a.astype(np.int64 if key_bytes == 8 else np.uint32).tofile(fa)
+        b.astype(np.int64 if key_bytes == 8 else np.uint32).tofile(fb)
+        del a, b
+        r = subprocess.run([exe, fa, str(n), fb, str(n), str(n), "-", "1"], check=True,
+                           capture_output=True, text=True)
+    timing = json.loads(r.stdout.strip().splitlines()[-1])
+    timing["build_keys_per_s"] = n / timing["build_a_s"]
+    timing["build_and_intersect_keys_per_s"] = n / (timing["build_a_s"] + timing["intersect_s"])
+    timing["published_composite_keys_per_s"] = n / timing["total_s"]
+    print(json.dumps(timing))
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("part", choices=["hash", "multi"])
+    ap.add_argument("part", choices=["hash", "multi", "timing"])
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--n", type=int, default=28)
+    ap.add_argument("--key-bytes", type=int, default=8)
     args = ap.parse_args()
-    os.makedirs(args.out, exist_ok=True)
     if args.part == "hash":
+        os.makedirs(args.out, exist_ok=True)
         part_hash(args.out)
-    else:
+    elif args.part == "multi":
+        os.makedirs(args.out, exist_ok=True)
         part_multi(args.out)
+    else:
+        part_timing(args.n, args.key_bytes)
 
 
 if __name__ == "__main__":

@@ -148,24 +148,27 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(x, world):
+def _reduce(x, world, op):
     if world <= 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(x, world):
+    """Slowest rank's time: the job's step time."""
+    import torch.distributed as dist
+    return _reduce(x, world, dist.ReduceOp.MAX if world > 1 else None)
 
 
 def sum_over_ranks(x, world):
-    if world <= 1:
-        return x
-    import torch
+    """Units processed by all ranks together."""
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, world, dist.ReduceOp.SUM if world > 1 else None)
 
 
 # ---------------------------------------------------------------------------

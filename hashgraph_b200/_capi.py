@@ -69,6 +69,9 @@ SIGNATURES = {
     "hg_gen_overlap": (_i32, [_p, _u64, _int, _p, _u64, _u64, _u64, _p]),
     "hg_gen_zipf": (_i32, [_p, _u64, _int, _p, _u64, _u64, _p]),
     "hg_zipf_cdf": (_i32, [_p, _u64, ctypes.c_double]),
+    "hg_gen_bounded": (_i32, [_p, _u64, _int, _u64, _u64, _p]),
+    "hg_gather_pair_keys": (_i32, [_p, _int, _p, _u64, _int, _p, _p]),
+    "hg_export_reference_layout": (_i32, [_p, _p, _p, _u64, _u64, _int, _p, _p, _p]),
     "hg_profile_enable": (_i32, [_int]),
     "hg_profile_read": (_i32, [_int, ctypes.POINTER(_int), ctypes.POINTER(ctypes.c_char_p),
                                ctypes.POINTER(ctypes.c_float)]),

@@ -67,6 +67,20 @@ __global__ void k_gen_uniform(KeyT* out, uint64_t n, uint64_t seed) {
 }
 
 template <typename KeyT>
+__global__ void k_gen_bounded(KeyT* out, uint64_t n, uint64_t seed, uint64_t bound) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    out[i] = static_cast<KeyT>(rand64(seed, 0, i) % bound);
+}
+
+// out[i] = keys[pairs[2i + which]] widened to 64 bits.
+template <typename KeyT>
+__global__ void k_gather_pair_keys(const KeyT* keys, const uint32_t* pairs, uint64_t count, int which,
+                                   int64_t* out) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += uint64_t(gridDim.x) * blockDim.x)
+    out[i] = static_cast<int64_t>(keys[pairs[2 * i + which]]);
+}
+
+template <typename KeyT>
 __global__ void k_gen_overlap(KeyT* out, uint64_t n, const KeyT* a, uint64_t m, Perm pb, Perm pa, uint64_t seed) {
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
     const uint64_t j = pb(i);
@@ -113,6 +127,72 @@ extern "C" hg_status hg_gen_uniform(void* d_out, uint64_t n, int key_bytes, uint
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (key_bytes == 8) k_gen_uniform<uint64_t><<<gen_grid(n), 256, 0, s>>>(static_cast<uint64_t*>(d_out), n, seed);
   else k_gen_uniform<uint32_t><<<gen_grid(n), 256, 0, s>>>(static_cast<uint32_t*>(d_out), n, seed);
+  return cudaPeekAtLastError() == cudaSuccess ? HG_OK : HG_ERR_CUDA;
+}
+
+extern "C" hg_status hg_gen_bounded(void* d_out, uint64_t n, int key_bytes, uint64_t seed, uint64_t bound,
+                                    hg_stream_t stream) {
+  if (key_bytes != 4 && key_bytes != 8) return HG_ERR_KEY_WIDTH;
+  if (n == 0) return HG_OK;
+  if (!d_out || bound == 0) return HG_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  count_launch();
+  if (key_bytes == 8) k_gen_bounded<uint64_t><<<gen_grid(n), 256, 0, s>>>(static_cast<uint64_t*>(d_out), n, seed, bound);
+  else k_gen_bounded<uint32_t><<<gen_grid(n), 256, 0, s>>>(static_cast<uint32_t*>(d_out), n, seed, bound);
+  return cudaPeekAtLastError() == cudaSuccess ? HG_OK : HG_ERR_CUDA;
+}
+
+extern "C" hg_status hg_gather_pair_keys(const void* d_keys, int key_bytes, const uint32_t* d_pairs, uint64_t count,
+                                         int which, int64_t* d_out, hg_stream_t stream) {
+  if (key_bytes != 4 && key_bytes != 8) return HG_ERR_KEY_WIDTH;
+  if (count == 0) return HG_OK;
+  if (!d_keys || !d_pairs || !d_out || (which != 0 && which != 1)) return HG_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  count_launch();
+  if (key_bytes == 8)
+    k_gather_pair_keys<uint64_t><<<gen_grid(count), 256, 0, s>>>(static_cast<const uint64_t*>(d_keys), d_pairs, count,
+                                                                 which, d_out);
+  else
+    k_gather_pair_keys<uint32_t><<<gen_grid(count), 256, 0, s>>>(static_cast<const uint32_t*>(d_keys), d_pairs, count,
+                                                                 which, d_out);
+  return cudaPeekAtLastError() == cudaSuccess ? HG_OK : HG_ERR_CUDA;
+}
+
+// Reference-layout export: 16-byte {key, int64 index} records and int64 offsets.
+template <typename KeyT>
+__global__ void k_export_reference(const KeyT* keys, const uint32_t* idx, uint64_t n, const uint32_t* off,
+                                   uint64_t n_buckets, unsigned char* kv16, int64_t* off64) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += stride) {
+    unsigned char* rec = kv16 + 16 * j;
+    if (sizeof(KeyT) == 8) {
+      *reinterpret_cast<uint64_t*>(rec) = static_cast<uint64_t>(keys[j]);
+    } else {
+      *reinterpret_cast<uint32_t*>(rec) = static_cast<uint32_t>(keys[j]);
+      *reinterpret_cast<uint32_t*>(rec + 4) = 0u;
+    }
+    *reinterpret_cast<int64_t*>(rec + 8) = idx ? static_cast<int64_t>(idx[j]) : static_cast<int64_t>(j);
+  }
+  for (uint64_t b = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; b <= n_buckets; b += stride)
+    off64[b] = static_cast<int64_t>(off[b]);
+}
+
+extern "C" hg_status hg_export_reference_layout(const uint32_t* d_offsets, const void* d_keys, const uint32_t* d_idx,
+                                                uint64_t n, uint64_t n_buckets, int key_bytes, void* d_kv16,
+                                                int64_t* d_offsets64, hg_stream_t stream) {
+  if (key_bytes != 4 && key_bytes != 8) return HG_ERR_KEY_WIDTH;
+  if (!d_offsets || !d_kv16 || !d_offsets64 || (n && !d_keys)) return HG_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const uint64_t work = n > n_buckets + 1 ? n : n_buckets + 1;
+  count_launch();
+  if (key_bytes == 8)
+    k_export_reference<uint64_t><<<gen_grid(work), 256, 0, s>>>(static_cast<const uint64_t*>(d_keys), d_idx, n,
+                                                                d_offsets, n_buckets,
+                                                                static_cast<unsigned char*>(d_kv16), d_offsets64);
+  else
+    k_export_reference<uint32_t><<<gen_grid(work), 256, 0, s>>>(static_cast<const uint32_t*>(d_keys), d_idx, n,
+                                                                d_offsets, n_buckets,
+                                                                static_cast<unsigned char*>(d_kv16), d_offsets64);
   return cudaPeekAtLastError() == cudaSuccess ? HG_OK : HG_ERR_CUDA;
 }
 

@@ -224,6 +224,26 @@ hg_status hg_gen_overlap(void* d_out, uint64_t n, int key_bytes, const void* d_a
 /* Zipf draws through a u64 fixed-point CDF table (universe entries, device). */
 hg_status hg_gen_zipf(void* d_out, uint64_t n, int key_bytes, const uint64_t* d_cdf,
                       uint64_t universe, uint64_t seed, hg_stream_t stream);
+/* key[i] = splitmix-stream(seed, 0, i) mod bound: uniform keys in [0, bound),
+ * the key range of the reference's SingleHashGraph generator
+ * (src/SingleHashGraph.cu:66-77,116-119, thrust draws in [0, maxkey]). */
+hg_status hg_gen_bounded(void* d_out, uint64_t n, int key_bytes, uint64_t seed, uint64_t bound,
+                         hg_stream_t stream);
+/* d_out[i] = (int64) d_keys[d_pairs[2*i + which]] for i < count: the key side
+ * of intersect pairs, e.g. B's key per match as MultiHashGraph::intersect
+ * outputs it (keypair{right}, include/MultiHashGraph.cuh:89-93). */
+hg_status hg_gather_pair_keys(const void* d_keys, int key_bytes, const uint32_t* d_pairs,
+                              uint64_t count, int which, int64_t* d_out, hg_stream_t stream);
+/* Writes a built table in the reference's layout: n 16-byte records
+ * {key (8 bytes, or 4 + 4 padding for 32-bit keys), int64 index} into d_kv16
+ * (the index is the stored input position, or the CSR position without an
+ * index) and n_buckets+1 int64 offsets into d_offsets64 -- keyval_ind and
+ * index_t of include/MultiHashGraph.cuh:82-87,66-74, as MultiHashGraph keeps
+ * them at h_dFinalKeys + h_edgesOff / h_offsetOff (src/MultiHashGraph.cu:549-566). */
+hg_status hg_export_reference_layout(const uint32_t* d_offsets, const void* d_keys,
+                                     const uint32_t* d_idx, uint64_t n, uint64_t n_buckets,
+                                     int key_bytes, void* d_kv16, int64_t* d_offsets64,
+                                     hg_stream_t stream);
 /* Host: fills cdf[universe] for Zipf(s). */
 hg_status hg_zipf_cdf(uint64_t* cdf, uint64_t universe, double s);
 

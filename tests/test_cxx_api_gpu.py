@@ -1,0 +1,52 @@
+"""The C++ classes that keep the reference's API (SingleHashGraph,
+MultiHashGraph), exercised through the reference's own test mains rewritten
+over them (hashgraph_b200/_lib/multi-hash, sing-hash): same arguments, same
+sequential inputs, with `check` -- buildSingle() cross-checks the exported
+reference-layout table against the plain build, and the intersect output is
+compared with a CPU multiset join.  A mismatch exits non-zero."""
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "hashgraph_b200", "_lib")
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(exe, *args):
+    path = os.path.join(LIB, exe)
+    if not os.path.exists(path):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "hashgraph_b200", "csrc")], check=True)
+    r = subprocess.run([path, *map(str, args)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "error" not in r.stderr.lower(), r.stderr[:2000]
+    return r.stdout
+
+
+@pytest.mark.parametrize("n_a,n_b,table", [(100_000, 60_000, 100_000), (1 << 22, 3 << 20, 1 << 22),
+                                           (5000, 9000, 4099)])
+def test_multi_hash_intersect_check(hg, n_a, n_b, table):
+    # argv: size maxkey binCount gpuCount lrbBins check countSizeB intersect (tableSize = maxkey)
+    out = _run("multi-hash", n_a, table, 16000, 1, 16000, "check", n_b, "intersect")
+    assert "multi intersect() time:" in out
+    assert f"intersect check ok: {min(n_a, n_b)} matches" in out
+
+
+@pytest.mark.parametrize("n,table", [(1_000_000, 1_000_000), (1 << 22, 1 << 21), (777, 1)])
+def test_multi_hash_build_check(hg, n, table):
+    out = _run("multi-hash", n, table, 16000, 1, 16000, "check", 1, "build")
+    assert "multi buildTable() time:" in out
+
+
+def test_single_hash_build(hg):
+    out = _run("sing-hash", 1 << 22, 1 << 23, 16000)
+    assert "single buildTable() time:" in out
+
+
+def test_multi_hash_rejects_several_gpus(hg):
+    path = os.path.join(LIB, "multi-hash")
+    r = subprocess.run([path, "1000", "1000", "16000", "2", "16000", "nocheck", "1000", "build"],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 2 and "gpuCount" in r.stderr

@@ -224,11 +224,14 @@ def run_ours(args, rank, world, local):
         a_keys = hg.gen_uniform(n, kb, seed_a, device=dev)
         q_keys = hg.gen_overlap(n, a_keys, overlap, seed_q)
     nq = q_keys.numel()
-    table = hg.Table(B, kb, with_index, n, dev)
+    paths = {"auto": hg.PATH_AUTO, "direct": 0, "partitioned": 1}
+    build_path, probe_path = paths[args.build_path], paths[args.probe_path]
+    table = hg.Table(B, kb, with_index, n, dev, build_path)
     pair_cap = nq if emit else 0
     import ctypes
     table.n = n  # the probe plan depends on the table's size
-    ws = torch.empty(max(hg.intersect_workspace_bytes(table, nq, emit), 1), dtype=torch.uint8, device=dev)
+    ws = torch.empty(max(hg.intersect_workspace_bytes(table, nq, emit, probe_path), 1), dtype=torch.uint8,
+                     device=dev)
     count = torch.zeros(1, dtype=torch.int64, device=dev)
     pairs = torch.empty((max(pair_cap, 1), 2), dtype=torch.int32, device=dev) if emit else None
     L = hg.lib()
@@ -236,12 +239,12 @@ def run_ours(args, rank, world, local):
 
     def step(a_src, q_src):
         table.rebuild(a_src, stream)
-        hg.check(L.hg_intersect_into(
+        hg.check(L.hg_intersect_into_path(
             ctypes.c_void_p(table.offsets.data_ptr()), ctypes.c_void_p(table.keys.data_ptr()),
             ctypes.c_void_p(table.idx.data_ptr()) if table.idx is not None else None, table.n, B, kb,
             ctypes.c_void_p(q_src.data_ptr()), nq, None,
             ctypes.c_void_p(pairs.data_ptr()) if emit else None, pair_cap,
-            ctypes.c_void_p(count.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(), sptr),
+            ctypes.c_void_p(count.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(), probe_path, sptr),
             "intersect")
 
     for _ in range(args.warmup):
@@ -341,7 +344,8 @@ def run_ours(args, rank, world, local):
         "data": "synthetic (seeded splitmix64 keys generated on the device; definitions shared with the oracle)",
         "config": {"workload": describe(args.workload, kb, n, B, kind, overlap, with_index), "n": n, "nq": nq,
                    "n_buckets": B, "key_bytes": kb, "with_index": with_index, "emit_pairs": emit,
-                   "matches": n_matches, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "matches": n_matches, "build_path": args.build_path, "probe_path": args.probe_path,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (each set %d MiB vs 126 MB L2); no flush" % (n * kb >> 20)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": None,
@@ -444,6 +448,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1 << 26)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--build-path", choices=["auto", "direct", "partitioned"], default="auto")
+    ap.add_argument("--probe-path", choices=["auto", "direct", "partitioned"], default="auto")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

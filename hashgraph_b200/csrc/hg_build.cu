@@ -30,6 +30,7 @@
 //   the decision is taken on the device, so the launch sequence is fixed.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -294,19 +295,31 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict_
     block_scan_segments<BLOCK>(lp, n_parts, 0u, 0u, wsum, [](uint32_t, uint32_t) {});
     cluster.barrier_wait();
     // owners: sum the cluster's histograms for their partitions and reserve
-    for (uint32_t p = p0 + threadIdx.x; p < p1; p += BLOCK) {
-      uint32_t h[16];
-      uint32_t tot = 0;
-      for (unsigned c = 0; c < CL; c++) {
-        h[c] = cluster.map_shared_rank(hist, c)[p];
-        tot += h[c];
+    // One (partition, CTA) pair per thread: lanes in groups of CL (a power of
+    // two dividing 32) hold one partition's per-CTA counts, scan them with
+    // shuffles, and the group's last lane reserves the cluster's run with one
+    // global atomic; every lane then hands its CTA the start.
+    for (uint32_t u0 = 0; u0 < (p1 - p0) * CL; u0 += BLOCK) {
+      const uint32_t u = u0 + threadIdx.x;
+      const uint32_t p = p0 + u / CL, c = u % CL;
+      const bool valid = p < p1;
+      const uint32_t h = valid ? cluster.map_shared_rank(hist, c)[p] : 0u;
+      uint32_t inc = h;
+#pragma unroll
+      for (unsigned o = 1; o < 16; o <<= 1) {
+        if (o < CL) {
+          const uint32_t t = __shfl_up_sync(FULL_MASK, inc, o, CL);
+          if (c >= o) inc += t;
+        }
       }
-      uint32_t run = tot ? atomicAdd(pcount + p, tot) : 0u;
-      if (uint64_t(run) + tot > cap) overflow = true;
-      for (unsigned c = 0; c < CL; c++) {
-        cluster.map_shared_rank(start, c)[p] = run;
-        run += h[c];
+      const uint32_t tot = __shfl_sync(FULL_MASK, inc, CL - 1, CL);
+      uint32_t run = 0;
+      if (c == CL - 1 && tot) {
+        run = atomicAdd(pcount + p, tot);
+        if (uint64_t(run) + tot > cap) overflow = true;
       }
+      run = __shfl_sync(FULL_MASK, run, CL - 1, CL);
+      if (valid) cluster.map_shared_rank(start, c)[p] = run + inc - h;
     }
     // the starts are written; the local counting sort needs only lp, so it
     // runs while the cluster barrier completes
@@ -367,6 +380,9 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
   KeyT* rk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(S) * 12, 16));
   uint32_t* ri = reinterpret_cast<uint32_t*>(rk + 2 * TILE);
   uint16_t* sp = reinterpret_cast<uint16_t*>(ri + (WITH_IDX ? 2 * TILE : 0));
+  uint32_t* sps = reinterpret_cast<uint32_t*>(sp + TILE);  // partition starts (n_parts + 1)
+  for (uint32_t j = threadIdx.x; j <= n_parts; j += BLOCK) sps[j] = pstart[j];
+  __syncthreads();
   __shared__ uint64_t bar[2];
   __shared__ uint64_t s_next;
   __shared__ uint32_t s_next_cnt;
@@ -377,7 +393,7 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
     for (; vt < vtiles; vt += gridDim.x) {
       const uint64_t q = vt / tiles_per_part;
       const uint32_t r0 = static_cast<uint32_t>(vt % tiles_per_part) * TILE;
-      const uint32_t m = pstart[q + 1] - pstart[q];
+      const uint32_t m = sps[q + 1] - sps[q];
       if (r0 < m) {
         *cnt = min(TILE, m - r0);
         return vt;
@@ -510,21 +526,32 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ f
   uint32_t* si = reinterpret_cast<uint32_t*>(sk + 2 * capf);
   __shared__ uint32_t wsum[BLOCK / 32 + 1];
   __shared__ uint64_t bar[2];
+  __shared__ uint32_t s_base[2], s_m[2];
   if (blockIdx.x == 0 && threadIdx.x == 0) offsets[n_buckets] = fstart[n_fine];
   const uint64_t n_live = umin64(n_fine, (n_buckets + W - 1) >> fine_log2);  // partitions holding buckets
-  auto issue = [&](uint64_t f, uint32_t buf) {
-    const uint32_t m = fstart[f + 1] - fstart[f];
-    const uint32_t bk = (m * uint32_t(sizeof(KeyT)) + 15u) & ~15u;
+  // thread 0 loads a partition's start and size one iteration before it issues its copy
+  auto load_meta = [&](uint64_t f) -> uint2 {
+    return f < n_live ? make_uint2(fstart[f], fstart[f + 1]) : make_uint2(0u, 0u);
+  };
+  auto issue = [&](uint64_t f, uint32_t buf, uint2 mt) {
+    const uint32_t m = mt.y - mt.x;
+    s_base[buf] = mt.x;
+    s_m[buf] = m;
+    const uint32_t bk = (m * uint32_t(sizeof(KeyT)) + 15u) & ~15u;  // stays inside the partition's slots
     const uint32_t bi = WITH_IDX ? ((m * 4u + 15u) & ~15u) : 0u;
     mbar_arrive_expect_tx(&bar[buf], bk + bi);
-    bulk_g2s(sk + buf * capf, fkeys + f * capf, bk, &bar[buf]);
-    if constexpr (WITH_IDX) bulk_g2s(si + buf * capf, fidx + f * capf, bi, &bar[buf]);
+    if (bk) bulk_g2s(sk + buf * capf, fkeys + f * capf, bk, &bar[buf]);
+    if constexpr (WITH_IDX) {
+      if (bi) bulk_g2s(si + buf * capf, fidx + f * capf, bi, &bar[buf]);
+    }
   };
+  uint2 next_meta = make_uint2(0u, 0u);
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     fence_mbar_init();
-    if (blockIdx.x < n_live) issue(blockIdx.x, 0);
+    if (blockIdx.x < n_live) issue(blockIdx.x, 0, load_meta(blockIdx.x));
+    next_meta = load_meta(blockIdx.x + gridDim.x);
   }
   __syncthreads();
   uint32_t it = 0;
@@ -532,17 +559,18 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ f
     const uint32_t buf = it & 1;
     if (threadIdx.x == 0 && f + gridDim.x < n_live) {
       fence_proxy_async_smem();
-      issue(f + gridDim.x, buf ^ 1u);
+      issue(f + gridDim.x, buf ^ 1u, next_meta);
+      next_meta = load_meta(f + 2 * uint64_t(gridDim.x));  // consumed next iteration
     }
     const uint64_t b0 = f << fine_log2;
     const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
-    const uint32_t base = fstart[f];
-    const uint32_t m = fstart[f + 1] - base;
     const KeyT* ck = sk + buf * capf;
     const uint32_t* ci = si + buf * capf;
     for (uint32_t j = threadIdx.x; j < nb; j += BLOCK) ctr[j] = 0u;
     mbar_wait(&bar[buf], (it >> 1) & 1);
     __syncthreads();
+    const uint32_t base = s_base[buf];
+    const uint32_t m = s_m[buf];
     for (uint32_t r = threadIdx.x; r < m; r += BLOCK)
       atomicAdd(&ctr[static_cast<uint32_t>(bm.of_key(ck[r]) - b0)], 1u);
     __syncthreads();
@@ -627,8 +655,8 @@ static hg_status run_direct(const BuildPlan& p, const KeyT* keys, uint32_t* offs
   return HG_OK;
 }
 
-uint64_t slack_capacity(double mean, uint64_t margin) {
-  const uint64_t c = static_cast<uint64_t>(std::ceil(mean + 8.0 * std::sqrt(mean) + double(margin)));
+uint64_t slack_capacity(double mean, uint64_t margin, double sigmas) {
+  const uint64_t c = static_cast<uint64_t>(std::ceil(mean + sigmas * std::sqrt(mean) + double(margin)));
   return (c + 31) & ~31ull;
 }
 
@@ -642,9 +670,9 @@ size_t pass1_smem(uint64_t n_parts, int key_bytes) {
   return align_up(12 * n_parts, 16) + size_t(PASS1_TILE) * (2 * key_bytes + 6);
 }
 
-size_t split_smem(uint32_t split_log2, int key_bytes, bool with_index) {
+size_t split_smem(uint32_t split_log2, int key_bytes, bool with_index, uint64_t n_parts) {
   return align_up(12 * (size_t(1) << split_log2), 16) +
-         size_t(SPLIT_TILE) * (2 * key_bytes + (with_index ? 8 : 0) + 2);
+         size_t(SPLIT_TILE) * (2 * key_bytes + (with_index ? 8 : 0) + 2) + (n_parts + 1) * 4;
 }
 
 bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size_t smem_rec, size_t per_bucket,
@@ -653,10 +681,16 @@ bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size
   PartGeometry g;
   bool found = false;
   const size_t FINE_SMEM_BUDGET = fine_budget;
-  for (uint32_t w = 15; w >= 6 && !found; w--) {
+  // tuning overrides: HG_FINE_LOG2 caps the fine width (W = 2^value buckets),
+  // HG_SPLIT_LOG2 caps the pass-2 split factor
+  uint32_t w_max = 15, s_max = SPLIT_LOG2_MAX;
+  if (const char* e = std::getenv("HG_FINE_LOG2")) w_max = std::max(6, std::min(15, std::atoi(e)));
+  if (const char* e = std::getenv("HG_SPLIT_LOG2")) s_max = std::max(0, std::min(10, std::atoi(e)));
+  for (uint32_t w = w_max; w >= 6 && !found; w--) {
     const uint64_t W = 1ull << w;
     const double frac = double(std::min<uint64_t>(W, n_buckets)) / double(n_buckets);
-    const uint64_t cap = slack_capacity(double(n_staged) * frac, 64);
+    // a probe's staged slice may spill (read in place), so it takes less slack
+    const uint64_t cap = slack_capacity(double(n_staged) * frac, 64, staged_may_spill ? 4.0 : 8.0);
     const uint64_t qcap = stream_smem ? slack_capacity(double(n_stream) * frac, 64) : 0;
     const size_t bytes = align_up(per_bucket * (W + 1), 16) + cap * smem_rec + qcap * stream_smem;
     if (bytes <= FINE_SMEM_BUDGET) {
@@ -677,7 +711,7 @@ bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size
     g.smem3 = head + size_t(g.smem_cap) * smem_rec;
   }
   const uint64_t W = 1ull << g.fine_log2;
-  g.split_log2 = std::min<uint32_t>(SPLIT_LOG2_MAX, ceil_log2_u64((n_buckets + W - 1) / W));
+  g.split_log2 = std::min<uint32_t>(s_max, ceil_log2_u64((n_buckets + W - 1) / W));
   g.coarse_log2 = g.fine_log2 + g.split_log2;
   g.n_parts = (n_buckets + (1ull << g.coarse_log2) - 1) >> g.coarse_log2;
   g.n_fine = g.n_parts << g.split_log2;
@@ -713,7 +747,7 @@ hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_in
   bool part_ok = plan_geometry(n, rec, n, 2 * rec, 4, 0, n_buckets, false, &p.g);
   if (part_ok) {
     p.g.smem1 = pass1_smem(p.g.n_parts, key_bytes);
-    p.g.smem2 = split_smem(p.g.split_log2, key_bytes, with_index);
+    p.g.smem2 = split_smem(p.g.split_log2, key_bytes, with_index, p.g.n_parts);
     part_ok = p.g.smem1 <= SMEM_BUDGET && p.g.smem2 <= SMEM_BUDGET;
   }
   const uint64_t footprint = n * (key_bytes + rec) + 4 * n_buckets;

@@ -20,14 +20,14 @@ enum BuildPath : int { BUILD_DIRECT = 0, BUILD_PARTITIONED = 1 };
 
 constexpr size_t SMEM_BUDGET = 220 * 1024;  // dynamic shared memory per CTA (B200 opt-in max 227 KB)
 constexpr size_t FINE_SMEM_BUDGET = 100 * 1024;        // pass-3 build CTAs: two per SM (double-buffered)
-constexpr size_t FINE_PROBE_SMEM_BUDGET = 72 * 1024;   // pass-3 probe CTAs: three per SM
+constexpr size_t FINE_PROBE_SMEM_BUDGET = 113 * 1024;  // pass-3 probe CTAs: two per SM (double-buffered)
 constexpr int PASS1_BLOCK = 512;
 constexpr int PASS1_KPT = 8;                     // pass-1 keys per thread per tile (registers)
 constexpr int PASS1_TILE = PASS1_BLOCK * PASS1_KPT;
 constexpr int SPLIT_BLOCK = 512;
 constexpr int SPLIT_TILE = 8 * SPLIT_BLOCK;     // k_split sorts a tile in registers: 8 records per thread
 constexpr int FINE_BLOCK = 512;
-constexpr uint32_t SPLIT_LOG2_MAX = 6;          // pass 2 splits a coarse partition up to 64 ways
+constexpr uint32_t SPLIT_LOG2_MAX = 8;          // pass 2 splits a coarse partition up to 256 ways
 
 // Geometry of the partitioned (three-pass) paths, shared by build and probe:
 // pass 1 splits the keys into n_parts coarse partitions of 2^coarse_log2
@@ -92,9 +92,9 @@ hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, 
 bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size_t smem_rec, size_t per_bucket,
                    size_t stream_smem, uint64_t n_buckets, bool staged_may_spill, PartGeometry* g,
                    size_t fine_budget = FINE_SMEM_BUDGET);
-uint64_t slack_capacity(double mean, uint64_t margin);
+uint64_t slack_capacity(double mean, uint64_t margin, double sigmas = 8.0);
 size_t pass1_smem(uint64_t n_parts, int key_bytes);
-size_t split_smem(uint32_t split_log2, int key_bytes, bool with_index);
+size_t split_smem(uint32_t split_log2, int key_bytes, bool with_index, uint64_t n_parts);
 
 // Kernel launchers (hg_build.cu / hg_probe.cu).  Workspace pointers are
 // already carved by the caller; all launches go to `stream`.

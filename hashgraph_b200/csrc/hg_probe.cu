@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "hg_bulk.cuh"
 #include "hg_cluster.cuh"
 #include "hg_device.cuh"
 #include "hg_plan.h"
@@ -107,144 +108,262 @@ __global__ void __launch_bounds__(PROBE_BLOCK)
 }
 
 // Pass 3 of the partitioned probe: one CTA per fine partition of W buckets.
-// The CTA stages table A's offsets for its W buckets and, when they fit, A's
-// keys (and index) for those buckets in shared memory with coalesced loads;
-// the fine partition's queries then probe shared memory only.  A partition
-// whose keys do not fit ("spill", heavy duplicates) reads A from global
-// memory instead.  Every query is hashed once: its local bucket is kept in
-// shared memory between the counting pass and the emitting pass.  Emission:
-// the CTA reserves its partition's output range with one atomic on the running
-// pair count, then writes pairs chunk by chunk (block scan per chunk); a
-// query with exactly one match writes it from the first pass's result.
-// Dynamic smem: soff[W+1] | sak[capa] | sai[capa] | slb[capq] (u16) | sx[capq] (u32, EMIT)
+// Both sides of the partition are staged in shared memory by bulk copies --
+// A's offsets, keys (and index) for the W buckets, and the partition's
+// queries with their positions -- and the next partition's copies are in
+// flight while this one is probed.  A's ragged ends that are not 16-byte
+// aligned are read with plain loads, so no copy touches memory outside A's
+// arrays; an A slice that does not fit ("spill", heavy duplicates) is read
+// from global memory instead.
+//
+// Each thread takes queries r = r0 + j*BLOCK + tid (j < FPROBE_QCH) and keeps,
+// per query, its match count and the first match's reference in registers.
+// One block scan of the thread totals and ONE atomic on the running pair
+// count reserve the round's output range, then every thread writes its pairs
+// straight from the registers (a query with several matches rescans its
+// bucket).  A round covers FPROBE_QCH*BLOCK queries, so a partition normally
+// takes one.
+// Dynamic smem: [2] x { off[W+4] | keys[capa + 2*EPK] | idx[capa + 8] | qkeys[capq] | qidx[capq] }
+constexpr int FPROBE_QCH = 8;
+
+__host__ __device__ inline size_t fine_probe_buf_bytes(uint32_t fine_log2, uint32_t capa, uint64_t capq,
+                                                       int key_bytes, bool a_idx, bool emit) {
+  const size_t epk = 16 / key_bytes;
+  auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
+  return a16(((size_t(1) << fine_log2) + 4) * 4) + a16((capa + 2 * epk) * key_bytes) +
+         (a_idx ? a16((size_t(capa) + 8) * 4) : 0) + a16(capq * key_bytes) + (emit ? a16(capq * 4) : 0);
+}
+
 template <typename KeyT, bool A_IDX, bool EMIT, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
     k_fine_probe(const KeyT* __restrict__ qkeys, const uint32_t* __restrict__ qidx, const uint32_t* __restrict__ qstart,
                  uint64_t n_fine, uint64_t capq, uint32_t fine_log2, BucketMap bm, uint64_t n_buckets,
                  const uint32_t* __restrict__ a_off, const KeyT* __restrict__ a_keys, const uint32_t* __restrict__ a_idx,
-                 uint32_t capa, uint32_t* __restrict__ pairs, uint64_t pair_cap, unsigned long long* d_count,
-                 const uint32_t* flags) {
+                 uint64_t n_a, uint32_t capa, uint32_t* __restrict__ pairs, uint64_t pair_cap,
+                 unsigned long long* d_count, const uint32_t* flags, bool a_bulk) {
   if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
+  constexpr uint32_t EPK = 16 / sizeof(KeyT);  // keys per 16 bytes
+  constexpr uint32_t QCH = FPROBE_QCH;
+  constexpr int NW = BLOCK / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t W = 1u << fine_log2;
-  uint32_t* soff = reinterpret_cast<uint32_t*>(smem_raw);
-  KeyT* sak = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(W + 1) * 4, 16));
-  uint32_t* sai = reinterpret_cast<uint32_t*>(sak + capa);
-  uint32_t* sx = A_IDX ? sai + capa : reinterpret_cast<uint32_t*>(sak + capa);  // per query: first match (local)
-  uint16_t* slb = reinterpret_cast<uint16_t*>(EMIT ? sx + capq : sx);           // per query: local bucket
-  __shared__ uint64_t red[BLOCK / 32 + 1];
-  __shared__ uint64_t s_run;
-  uint64_t counted = 0;
-  for (uint64_t f = blockIdx.x; f < n_fine; f += gridDim.x) {
+  const size_t off_bytes = align_up_dev(size_t(W + 4) * 4, 16);
+  const size_t key_bytes = align_up_dev(size_t(capa + 2 * EPK) * sizeof(KeyT), 16);
+  const size_t idx_bytes = A_IDX ? align_up_dev(size_t(capa + 8) * 4, 16) : 0;
+  const size_t qk_bytes = align_up_dev(capq * sizeof(KeyT), 16);
+  const size_t buf_bytes = fine_probe_buf_bytes(fine_log2, capa, capq, sizeof(KeyT), A_IDX, EMIT);
+  __shared__ uint64_t bar[2];
+  // per buffer: A's range [as, ae), where the copied keys / index start
+  // (al, ial) and end (ar, iar), plain offset loads still needed, the
+  // partition's query count
+  __shared__ uint32_t s_as[2], s_ae[2], s_al[2], s_ar[2], s_ial[2], s_iar[2], s_oplain[2], s_qm[2];
+  __shared__ uint64_t red[NW + 1];
+  const uint64_t n_live = umin64(n_fine, (n_buckets + W - 1) >> fine_log2);
+  auto buf_off = [&](uint32_t b) { return reinterpret_cast<uint32_t*>(smem_raw + b * buf_bytes); };
+  auto buf_keys = [&](uint32_t b) { return reinterpret_cast<KeyT*>(smem_raw + b * buf_bytes + off_bytes); };
+  auto buf_idx = [&](uint32_t b) {
+    return reinterpret_cast<uint32_t*>(smem_raw + b * buf_bytes + off_bytes + key_bytes);
+  };
+  auto buf_q = [&](uint32_t b) {
+    return reinterpret_cast<KeyT*>(smem_raw + b * buf_bytes + off_bytes + key_bytes + idx_bytes);
+  };
+  auto buf_qi = [&](uint32_t b) {
+    return reinterpret_cast<uint32_t*>(smem_raw + b * buf_bytes + off_bytes + key_bytes + idx_bytes + qk_bytes);
+  };
+  struct Meta {
+    uint32_t as, ae, qb, qe;
+  };
+  // thread 0: the partition's A range and queries (loaded one iteration early)
+  auto load_meta = [&](uint64_t f) -> Meta {
+    Meta mt{0, 0, 0, 0};
+    if (f < n_live) {
+      const uint64_t b0 = f << fine_log2;
+      const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
+      mt.as = a_off[b0];
+      mt.ae = a_off[b0 + nb];
+      mt.qb = qstart[f];
+      mt.qe = qstart[f + 1];
+    }
+    return mt;
+  };
+  // thread 0: start the bulk copies of partition f into buffer b.  A's
+  // copies are rounded out to 16 bytes where that stays inside A's arrays;
+  // only what cannot be covered that way is left to plain loads.  The
+  // queries sit at the start of their 16-byte aligned slot (capq is a
+  // multiple of 32), so their copies round up inside the slot.
+  auto issue = [&](uint64_t f, uint32_t b, const Meta& mt) {
     const uint64_t b0 = f << fine_log2;
-    if (b0 >= n_buckets) break;
     const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
-    const uint32_t a_s = a_off[b0];
-    const uint32_t cnt_a = a_off[b0 + nb] - a_s;
-    const bool spill = cnt_a > capa;
-    for (uint32_t j = threadIdx.x; j <= nb; j += BLOCK) soff[j] = a_off[b0 + j] - a_s;
+    const uint32_t as = mt.as, ae = mt.ae;
+    const bool fits = ae - as + 2 * EPK <= capa;
+    uint32_t al = as, ar = as, ial = as, iar = as, ob = 0;
+    if (a_bulk) {
+      // offsets: entries [0, nb] of the partition, rounded up within B + 1
+      const uint64_t oend = umin64((b0 + nb + 1 + 3) & ~3ull, (n_buckets + 1) & ~3ull);
+      ob = oend > b0 ? static_cast<uint32_t>((oend - b0) * 4) : 0u;
+      if (fits) {
+        al = as & ~(EPK - 1);
+        ar = static_cast<uint32_t>(umin64((uint64_t(ae) + EPK - 1) & ~uint64_t(EPK - 1), n_a & ~uint64_t(EPK - 1)));
+        if (ar < al) ar = al;
+        if (A_IDX) {
+          ial = as & ~3u;
+          iar = static_cast<uint32_t>(umin64((uint64_t(ae) + 3) & ~3ull, n_a & ~3ull));
+          if (iar < ial) iar = ial;
+        }
+      }
+    }
+    const uint32_t m = mt.qe - mt.qb;
+    s_as[b] = as;
+    s_ae[b] = ae;
+    s_al[b] = al;
+    s_ar[b] = ar;
+    s_ial[b] = ial;
+    s_iar[b] = iar;
+    s_oplain[b] = ob / 4;
+    s_qm[b] = m;
+    const uint32_t kb = (ar - al) * uint32_t(sizeof(KeyT));
+    const uint32_t ib = A_IDX ? (iar - ial) * 4u : 0u;
+    const uint32_t qkb = (m * uint32_t(sizeof(KeyT)) + 15u) & ~15u;
+    const uint32_t qib = EMIT ? ((m * 4u + 15u) & ~15u) : 0u;
+    mbar_arrive_expect_tx(&bar[b], ob + kb + ib + qkb + qib);
+    if (ob) bulk_g2s(buf_off(b), a_off + b0, ob, &bar[b]);
+    if (kb) bulk_g2s(buf_keys(b), a_keys + al, kb, &bar[b]);
+    if constexpr (A_IDX) {
+      if (ib) bulk_g2s(buf_idx(b), a_idx + ial, ib, &bar[b]);
+    }
+    if (qkb) bulk_g2s(buf_q(b), qkeys + f * capq, qkb, &bar[b]);
+    if constexpr (EMIT) {
+      if (qib) bulk_g2s(buf_qi(b), qidx + f * capq, qib, &bar[b]);
+    }
+  };
+  Meta next_meta{};  // thread 0: metadata of the partition after the one in flight
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+    if (blockIdx.x < n_live) issue(blockIdx.x, 0, load_meta(blockIdx.x));
+    next_meta = load_meta(blockIdx.x + gridDim.x);
+  }
+  __syncthreads();
+  uint64_t counted = 0;
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+
+  uint32_t it = 0;
+  for (uint64_t f = blockIdx.x; f < n_live; f += gridDim.x, it++) {
+    const uint32_t b = it & 1;
+    if (threadIdx.x == 0 && f + gridDim.x < n_live) {
+      fence_proxy_async_smem();
+      issue(f + gridDim.x, b ^ 1u, next_meta);
+      next_meta = load_meta(f + 2 * uint64_t(gridDim.x));  // consumed next iteration
+    }
+    const uint64_t b0 = f << fine_log2;
+    const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
+    mbar_wait(&bar[b], (it >> 1) & 1);
+    uint32_t* soff = buf_off(b);
+    KeyT* sk = buf_keys(b);
+    uint32_t* si = buf_idx(b);
+    const uint32_t as = s_as[b], ae = s_ae[b], al = s_al[b], ar = s_ar[b];
+    const bool spill = ae - as + 2 * EPK > capa;
+    // whatever the bulk copies could not cover (the end of A's arrays, or
+    // unaligned arrays)
+    for (uint32_t j = s_oplain[b] + threadIdx.x; j <= nb; j += BLOCK) soff[j] = a_off[b0 + j];
     if (!spill) {
-      for (uint32_t x = threadIdx.x; x < cnt_a; x += BLOCK) {
-        sak[x] = a_keys[a_s + x];
-        if constexpr (A_IDX) sai[x] = a_idx[a_s + x];
+      for (uint32_t x = ar + threadIdx.x; x < ae; x += BLOCK) sk[x - al] = a_keys[x];
+      if constexpr (A_IDX) {
+        const uint32_t ial = s_ial[b], iar = s_iar[b];
+        for (uint32_t x = iar + threadIdx.x; x < ae; x += BLOCK) si[x - ial] = a_idx[x];
       }
     }
     __syncthreads();
-    const uint32_t qb = qstart[f];
-    const uint32_t m = qstart[f + 1] - qb;
-    const KeyT* src = qkeys + f * capq;
-    const uint32_t* srci = qidx + f * capq;
-
-    // matches of key k in local bucket lb: count, first position (local to a_s)
-    auto scan_bucket = [&](KeyT k, uint32_t lb, uint32_t& first) -> uint32_t {
-      const uint32_t s = soff[lb], e = soff[lb + 1];
-      uint32_t c = 0;
-      first = 0;
-      if (spill) {
-        for (uint32_t x = s; x < e; x++)
-          if (a_keys[a_s + x] == k) {
-            if (c == 0) first = x;
-            c++;
-          }
-      } else {
-        for (uint32_t x = s; x < e; x++)
-          if (sak[x] == k) {
-            if (c == 0) first = x;
-            c++;
-          }
-      }
-      return c;
-    };
-    auto aref_of = [&](uint32_t x) -> uint32_t {
-      if constexpr (A_IDX) return spill ? a_idx[a_s + x] : sai[x];
-      return a_s + x;
+    const uint32_t m = s_qm[b];
+    const KeyT* sq = buf_q(b);
+    const uint32_t* sqi = buf_qi(b);
+    const uint32_t koff = as - al;  // sk[x + koff] is A's key at global position as + x
+    uint32_t ioff = 0;
+    if constexpr (A_IDX) ioff = as - s_ial[b];
+    auto a_key = [&](uint32_t x) -> KeyT { return spill ? a_keys[as + x] : sk[x + koff]; };
+    auto a_ref = [&](uint32_t x) -> uint32_t {
+      if constexpr (A_IDX) return spill ? a_idx[as + x] : si[x + ioff];
+      else return as + x;
     };
 
-    if constexpr (EMIT) {
+    for (uint32_t r0 = 0; r0 < m; r0 += QCH * BLOCK) {
+      uint32_t cnt[QCH], ref[QCH];
       uint64_t mine = 0;
-      for (uint32_t r = threadIdx.x; r < m; r += BLOCK) {
-        const KeyT k = src[r];
-        const uint32_t lb = static_cast<uint32_t>(bm.of_key(k) - b0);
-        uint32_t first;
-        const uint32_t c = scan_bucket(k, lb, first);
-        slb[r] = static_cast<uint16_t>(lb);
-        sx[r] = c == 0 ? 0xffffffffu : (c == 1 ? first : 0xfffffffeu);
-        mine += c;
-      }
-      uint64_t tot;
-      block_exclusive_scan<BLOCK>(mine, red, &tot);
-      if (threadIdx.x == 0) {
-        s_run = tot ? atomicAdd(d_count, static_cast<unsigned long long>(tot)) : 0ull;
-        if (s_run + tot > pair_cap) record_error(HG_ERR_PAIR_CAPACITY);
-      }
-      __syncthreads();
-      if (tot) {
-        uint64_t run = s_run;
-        for (uint32_t r0 = 0; r0 < m; r0 += BLOCK) {
-          const uint32_t r = r0 + threadIdx.x;
-          const uint32_t x = r < m ? sx[r] : 0xffffffffu;
-          uint32_t c = 0;
-          KeyT k = KeyT(0);
-          if (x == 0xfffffffeu) {  // several matches: count them again
-            k = src[r];
-            uint32_t first;
-            c = scan_bucket(k, slb[r], first);
-          } else if (x != 0xffffffffu) {
-            c = 1;
+#pragma unroll
+      for (uint32_t j = 0; j < QCH; j++) {
+        const uint32_t r = r0 + j * BLOCK + threadIdx.x;
+        cnt[j] = 0;
+        ref[j] = 0;
+        if (r < m) {
+          const KeyT k = sq[r];
+          const uint32_t lb = static_cast<uint32_t>(bm.of_key(k) - b0);
+          const uint32_t e = soff[lb + 1] - as;
+          for (uint32_t x = soff[lb] - as; x < e; x++) {
+            if (a_key(x) == k) {
+              if (cnt[j] == 0) ref[j] = a_ref(x);
+              cnt[j]++;
+            }
           }
-          uint64_t chunk;
-          uint64_t pos = run + block_exclusive_scan<BLOCK>(uint64_t(c), red, &chunk);
-          if (c == 1 && x != 0xfffffffeu) {
-            if (pos < pair_cap) reinterpret_cast<uint2*>(pairs)[pos] = make_uint2(aref_of(x), srci[r]);
-          } else if (c) {
-            const uint32_t qref = srci[r];
-            const uint32_t lb = slb[r];
-            const uint32_t s = soff[lb], e = soff[lb + 1];
-            for (uint32_t y = s; y < e; y++) {
-              const KeyT a = spill ? a_keys[a_s + y] : sak[y];
-              if (a == k) {
-                if (pos < pair_cap) reinterpret_cast<uint2*>(pairs)[pos] = make_uint2(aref_of(y), qref);
-                pos++;
+          mine += cnt[j];
+        }
+      }
+      if constexpr (!EMIT) {
+        counted += mine;
+      } else {
+        // block scan of the thread totals; warp 0 reserves the round's range
+        const uint64_t inc = warp_inclusive_scan(mine);
+        if (lane == 31) red[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+          const uint64_t w = lane < NW ? red[lane] : 0ull;
+          const uint64_t wi = warp_inclusive_scan(w);
+          const uint64_t tot = __shfl_sync(FULL_MASK, wi, NW - 1);
+          uint64_t base = 0;
+          if (lane == 0 && tot) {
+            base = atomicAdd(d_count, static_cast<unsigned long long>(tot));
+            if (base + tot > pair_cap) record_error(HG_ERR_PAIR_CAPACITY);
+          }
+          base = __shfl_sync(FULL_MASK, base, 0);
+          if (lane < NW) red[lane] = base + wi - w;
+        }
+        __syncthreads();
+        uint64_t pos = red[warp] + inc - mine;
+        if (mine) {
+#pragma unroll
+          for (uint32_t j = 0; j < QCH; j++) {
+            const uint32_t r = r0 + j * BLOCK + threadIdx.x;
+            if (cnt[j] == 1) {
+              if (pos < pair_cap) reinterpret_cast<uint2*>(pairs)[pos] = make_uint2(ref[j], sqi[r]);
+              pos++;
+            } else if (cnt[j] > 1) {
+              const KeyT k = sq[r];
+              const uint32_t qref = sqi[r];
+              const uint32_t lb = static_cast<uint32_t>(bm.of_key(k) - b0);
+              const uint32_t e = soff[lb + 1] - as;
+              for (uint32_t x = soff[lb] - as; x < e; x++) {
+                if (a_key(x) == k) {
+                  if (pos < pair_cap) reinterpret_cast<uint2*>(pairs)[pos] = make_uint2(a_ref(x), qref);
+                  pos++;
+                }
               }
             }
           }
-          run += chunk;
         }
-      }
-    } else {
-      for (uint32_t r = threadIdx.x; r < m; r += BLOCK) {
-        const KeyT k = src[r];
-        uint32_t first;
-        counted += scan_bucket(k, static_cast<uint32_t>(bm.of_key(k) - b0), first);
+        if (r0 + QCH * BLOCK < m) __syncthreads();  // red is rewritten by the next round
       }
     }
-    __syncthreads();
+    __syncthreads();  // all reads of buffer b end before it is refilled
   }
   if constexpr (!EMIT) {
     uint64_t tot;
     block_exclusive_scan<BLOCK>(counted, red, &tot);
     if (threadIdx.x == 0 && tot) atomicAdd(d_count, static_cast<unsigned long long>(tot));
   }
+}
+
+size_t fine_probe_smem(uint32_t fine_log2, uint32_t capa, uint64_t capq, int key_bytes, bool a_idx, bool emit) {
+  return 2 * fine_probe_buf_bytes(fine_log2, capa, capq, key_bytes, a_idx, emit);
 }
 
 hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, int key_bytes, bool emit,
@@ -262,12 +381,15 @@ hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, 
   p.tiles = (nq + PROBE_TILE - 1) / PROBE_TILE;
   const size_t a_rec = key_bytes + (a_idx ? 4 : 0);
   const size_t q_rec = key_bytes + 4;  // queries travel with their position
-  // pass 3 keeps a 16-bit local bucket and a 32-bit first match per query
-  bool part_ok = plan_geometry(nq, q_rec, n_a, a_rec, 4, 6, n_buckets, true, &p.g, FINE_PROBE_SMEM_BUDGET);
+  // pass 3 double-buffers A's slice (offsets, keys, index) and the
+  // partition's queries (keys, and positions when pairs are emitted)
+  bool part_ok = plan_geometry(nq, q_rec, n_a, 2 * a_rec, 8, 2 * (key_bytes + (emit ? 4 : 0)), n_buckets, true,
+                               &p.g, FINE_PROBE_SMEM_BUDGET);
   if (part_ok) {
     p.g.smem1 = pass1_smem(p.g.n_parts, key_bytes);
-    p.g.smem2 = split_smem(p.g.split_log2, key_bytes, true);
-    part_ok = p.g.smem1 <= SMEM_BUDGET && p.g.smem2 <= SMEM_BUDGET;
+    p.g.smem2 = split_smem(p.g.split_log2, key_bytes, true, p.g.n_parts);
+    p.g.smem3 = fine_probe_smem(p.g.fine_log2, p.g.smem_cap, p.g.fine_cap, key_bytes, a_idx, emit);
+    part_ok = p.g.smem1 <= SMEM_BUDGET && p.g.smem2 <= SMEM_BUDGET && p.g.smem3 <= SMEM_BUDGET;
   }
   const uint64_t a_bytes = n_a * a_rec + 4 * n_buckets;
   int path = force_path;
@@ -329,11 +451,19 @@ static hg_status run_probe_partitioned(const ProbePlan& p, const uint32_t* a_off
   unsigned* ticket = reinterpret_cast<unsigned*>(ws + p.off_ticket);
   uint64_t* status = reinterpret_cast<uint64_t*>(ws + p.off_status);
   HG_CUDA(cudaMemsetAsync(ws, 0, p.off_pkeys, s), "intersect: workspace memset");
-  hg_status st = run_partition_passes<KeyT, 1, true>(g, p.nq, q, q_idx, bm, ws, p.off_flags, p.off_ticket,
-                                                     p.off_pcount, p.off_pstatus, p.off_fcount, p.off_fstatus,
-                                                     p.off_pkeys, p.off_pidx, p.off_fkeys, p.off_fidx, "probe", s);
+  // queries on a 16-byte boundary are streamed with bulk (TMA) copies
+  const bool aligned = (reinterpret_cast<uintptr_t>(q) & 15u) == 0;
+  hg_status st = aligned ? run_partition_passes<KeyT, 16 / sizeof(KeyT), true>(
+                               g, p.nq, q, q_idx, bm, ws, p.off_flags, p.off_ticket, p.off_pcount, p.off_pstatus,
+                               p.off_fcount, p.off_fstatus, p.off_pkeys, p.off_pidx, p.off_fkeys, p.off_fidx, "probe", s)
+                         : run_partition_passes<KeyT, 1, true>(g, p.nq, q, q_idx, bm, ws, p.off_flags, p.off_ticket,
+                                                               p.off_pcount, p.off_pstatus, p.off_fcount,
+                                                               p.off_fstatus, p.off_pkeys, p.off_pidx, p.off_fkeys,
+                                                               p.off_fidx, "probe", s);
   if (st != HG_OK) return st;
   {
+    const bool a_bulk = ((reinterpret_cast<uintptr_t>(a_off) | reinterpret_cast<uintptr_t>(a_keys) |
+                          reinterpret_cast<uintptr_t>(a_idx)) & 15u) == 0;
     auto go = [&](auto kern) {
       const int bps = blocks_per_sm(kern, FINE_BLOCK, g.smem3);
       if (bps <= 0) {
@@ -346,7 +476,7 @@ static hg_status run_probe_partitioned(const ProbePlan& p, const uint32_t* a_off
       kern<<<std::max(grid, 1u), FINE_BLOCK, g.smem3, s>>>(
           reinterpret_cast<const KeyT*>(ws + p.off_fkeys), reinterpret_cast<const uint32_t*>(ws + p.off_fidx),
           reinterpret_cast<const uint32_t*>(ws + p.off_fcount), g.n_fine, g.fine_cap, g.fine_log2, bm, p.n_buckets,
-          a_off, a_keys, a_idx, g.smem_cap, pairs, cap, d_count, static_cast<const uint32_t*>(flags));
+          a_off, a_keys, a_idx, p.n_a, g.smem_cap, pairs, cap, d_count, static_cast<const uint32_t*>(flags), a_bulk);
       const cudaError_t e = cudaPeekAtLastError();
       if (e != cudaSuccess) st = cuda_fail(e, "fine-probe launch");
     };

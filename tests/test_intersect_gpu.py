@@ -150,3 +150,39 @@ def test_intersect_tables_matches_reference_semantics(hg):
     assert L.hg_intersect_tables(ta, tc, None, 0, ctypes.c_void_p(cnt.data_ptr()), s) == -9
     for t in (ta, tb, tc):
         L.hg_table_free(t)
+
+
+def test_partitioned_probe_of_unaligned_table(hg):
+    """A table whose arrays start off a 16-byte boundary is probed with plain
+    loads instead of bulk copies; results are unchanged."""
+    import ctypes
+
+    import torch
+    L = hg.lib()
+    n, B = 300_000, 1 << 18
+    a = oracle.gen_uniform(n, 8, 51)
+    q = oracle.gen_overlap(n, a, 0.4, 52)
+    da, dq = from_np_u(a), from_np_u(q)
+    off_buf = torch.empty(B + 2, dtype=torch.int32, device="cuda")
+    key_buf = torch.empty(n + 1, dtype=torch.int64, device="cuda")
+    idx_buf = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+    off, keys, idx = off_buf[1:], key_buf[1:], idx_buf[1:]
+    assert off.data_ptr() % 16 and keys.data_ptr() % 16 and idx.data_ptr() % 16
+    ws = torch.empty(hg.build_workspace_bytes(n, 8, B, True, 1), dtype=torch.uint8, device="cuda")
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    P = ctypes.c_void_p
+    assert L.hg_build_into_path(P(da.data_ptr()), n, 8, B, P(off.data_ptr()), P(keys.data_ptr()),
+                                P(idx.data_ptr()), P(ws.data_ptr()), ws.numel(), 1, s) == 0
+    wsz = ctypes.c_size_t()
+    assert L.hg_intersect_workspace_size_path(n, 1, B, n, 8, 1, 1, ctypes.byref(wsz)) == 0
+    pws = torch.empty(max(wsz.value, 1), dtype=torch.uint8, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    pairs = torch.empty((n, 2), dtype=torch.int32, device="cuda")
+    assert L.hg_intersect_into_path(P(off.data_ptr()), P(keys.data_ptr()), P(idx.data_ptr()), n, B, 8,
+                                    P(dq.data_ptr()), n, None, P(pairs.data_ptr()), n, P(cnt.data_ptr()),
+                                    P(pws.data_ptr()), pws.numel(), 1, s) == 0
+    c = int(cnt.item())
+    oc, op = _oracle_pairs(a, B, True, q)
+    assert c == oc
+    np.testing.assert_array_equal(_sorted_pairs(to_np_u(pairs[:c], 4)), _sorted_pairs(op))
+    assert hg.device_error() == 0

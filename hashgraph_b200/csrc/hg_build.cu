@@ -17,15 +17,18 @@
 // Partitioned (large tables; replaces the LRB locality pass
 // lrbCountHashD/lrbRehashD/lrbCountHashGlobalD/lrbCopyToGraphD,
 // include/SingleHashGraphOperators.cuh:102-154, and the 1-GPU multi pipeline):
-//   1. k_part_scatter: hash each key, bucket range p = b >> part_log2, append
-//                 (key, position) to partition p's slot range (warp-aggregated
-//                 slot reservation; the open tail line of every partition stays
-//                 in L2 so the scattered appends reach HBM as whole lines).
-//   2. k_scan_u32 over the P partition sizes -> partition starts.
-//   3. k_part_local: one CTA per partition: shared-memory bucket histogram,
-//                 segmented block scan, coalesced offsets write, then the
-//                 scatter of the partition's keys into its output slice.
-//   If any partition overflowed its slot range (heavy duplicates), pass 3
+//   1. k_multisplit: tiles of 4096 keys per CTA are ranked per coarse
+//                 partition (2^coarse_log2 buckets) in shared memory, one
+//                 global atomic per (tile, partition) reserves the run, and
+//                 the tile leaves partition-sorted as coalesced runs.
+//   2. k_scan_u32 over the coarse partition sizes.
+//   3. k_split:   each coarse partition is split up to 256 ways into fine
+//                 partitions of W = 2^fine_log2 buckets the same way.
+//   4. k_scan_u32 over the fine partition sizes.
+//   5. k_fine_build: one CTA per fine partition: bucket histogram in shared
+//                 memory, segmented block scan, coalesced offsets write, then
+//                 the scatter of the partition's keys into its output slice.
+//   If any partition overflowed its slot range (heavy duplicates), pass 5
 //   stands down and gated copies of the direct kernels rebuild the table;
 //   the decision is taken on the device, so the launch sequence is fixed.
 #include <algorithm>
@@ -37,7 +40,6 @@
 
 #include "hg_device.cuh"
 #include "hg_bulk.cuh"
-#include "hg_cluster.cuh"
 #include "hg_plan.h"
 #include "hg_prof.cuh"
 #include "hg_scan.cuh"
@@ -194,16 +196,19 @@ __global__ void k_fill_u32(uint32_t* p, uint64_t count, uint32_t value, const ui
 // Partitioned path (cluster kernels)
 // ---------------------------------------------------------------------------
 
-// Pass 1: cluster multisplit.  A cluster of CL CTAs takes a tile of
-// CL*TILE consecutive keys (TILE = BLOCK*KPT per CTA); every CTA ranks its
-// keys per coarse partition with shared-memory atomics, the cluster sums the
-// per-CTA histograms over DSMEM (CTA c owns partitions [c*P/CL, (c+1)*P/CL)),
-// each owner reserves the cluster's run in partition p with ONE global atomic
-// and hands every CTA its start, and each CTA writes its keys
-// partition-sorted (shared-memory counting sort) so the runs leave as
-// coalesced stores.  With BULK, the CTA's next tile is prefetched into shared
-// memory by a bulk copy (TMA) while the current one is processed.
-// Dynamic smem: hist[P] | lp[P] | start[P] | raw[2][TILE] | si[TILE] | sp[TILE] (u16)
+// Pass 1: multisplit into coarse partitions.  Each CTA takes tiles of TILE
+// consecutive keys (KPT per thread, in registers), ranks them per coarse
+// partition with shared-memory atomics, reserves its run in every partition
+// with ONE global atomic per (tile, partition), and writes its keys
+// partition-sorted (in-place counting sort in shared memory) so the runs
+// leave as coalesced stores.  The reservations are issued before the local
+// scan and sort and their results are consumed only after them, which hides
+// the atomics' round trip.  With BULK, the CTA's next tile is prefetched into
+// shared memory by a bulk copy (TMA) while the current one is processed.
+// Dynamic smem: eoff[P] (i64) | hist[P] | lp[P] | raw[2][TILE] | si[TILE] | sp[TILE] (u16)
+
+constexpr int64_t EOFF_NONE = INT64_MIN;      // a dropped (overflowing) run
+
 template <typename KeyT, bool WITH_IDX, int BLOCK, int KPT, bool BULK>
 __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict__ keys, const uint32_t* __restrict__ key_idx,
                                                          uint64_t n, BucketMap bm, uint32_t coarse_log2, uint32_t n_parts,
@@ -211,60 +216,54 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict_
                                                          KeyT* __restrict__ pkeys, uint32_t* __restrict__ pidx,
                                                          uint32_t* flags) {
   constexpr uint32_t TILE = BLOCK * KPT;
-  cg::cluster_group cluster = cg::this_cluster();
-  const unsigned CL = cluster.num_blocks();
-  const unsigned rank = cluster.block_rank();
+  constexpr uint32_t APT = PASS1_APT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint32_t* hist = reinterpret_cast<uint32_t*>(smem_raw);
+  int64_t* eoff = reinterpret_cast<int64_t*>(smem_raw);  // element offset of sorted position 0, per partition
+  uint32_t* hist = reinterpret_cast<uint32_t*>(eoff + n_parts);
   uint32_t* lp = hist + n_parts;
-  uint32_t* start = lp + n_parts;
-  KeyT* raw = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(n_parts) * 12, 16));
+  KeyT* raw = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(n_parts) * 16, 16));
   uint32_t* si = reinterpret_cast<uint32_t*>(raw + 2 * TILE);
   uint16_t* sp = reinterpret_cast<uint16_t*>(si + TILE);
   __shared__ uint32_t wsum[BLOCK / 32 + 1];
   __shared__ uint64_t bar[2];
-  const uint64_t cluster_id = blockIdx.x / CL, nclusters = gridDim.x / CL;
-  const uint64_t ctile = uint64_t(CL) * TILE;
-  const uint64_t ntiles = (n + ctile - 1) / ctile;
-  const uint32_t per = (n_parts + CL - 1) / CL;
-  const uint32_t p0 = min(n_parts, rank * per), p1 = min(n_parts, p0 + per);
-  auto tile_base = [&](uint64_t ct) { return ct * ctile + uint64_t(rank) * TILE; };
-  auto tile_cnt = [&](uint64_t ct) -> uint32_t {
-    const uint64_t b = tile_base(ct);
+  const uint64_t ntiles = (n + TILE - 1) / TILE;
+  auto tile_cnt = [&](uint64_t t) -> uint32_t {
+    const uint64_t b = t * TILE;
     return b < n ? static_cast<uint32_t>(umin64(TILE, n - b)) : 0u;
   };
   // bulk part of a tile: whole 16-byte units; the ragged tail is read with plain loads
   auto bulk_bytes = [&](uint32_t cnt) -> uint32_t { return (cnt * uint32_t(sizeof(KeyT))) & ~15u; };
+  for (uint32_t j = threadIdx.x; j < n_parts; j += BLOCK) hist[j] = 0u;
   if constexpr (BULK) {
     if (threadIdx.x == 0) {
       mbar_init(&bar[0], 1);
       mbar_init(&bar[1], 1);
       fence_mbar_init();
-      if (cluster_id < ntiles) bulk_load(raw, keys + tile_base(cluster_id), bulk_bytes(tile_cnt(cluster_id)), &bar[0]);
+      if (blockIdx.x < ntiles) bulk_load(raw, keys + uint64_t(blockIdx.x) * TILE, bulk_bytes(tile_cnt(blockIdx.x)), &bar[0]);
     }
-    __syncthreads();
   }
+  __syncthreads();
   bool overflow = false;
-  bool timed_out = false;
   uint32_t it = 0;
-  for (uint64_t ct = cluster_id; ct < ntiles; ct += nclusters, it++) {
-    const uint64_t base = tile_base(ct);
-    const uint32_t cnt = tile_cnt(ct);
+  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+    const uint64_t base = t * TILE;
+    const uint32_t cnt = tile_cnt(t);
     KeyT* cur = raw + (it & 1) * TILE;
     if constexpr (BULK) {
       // prefetch the next tile into the other buffer (its readers finished at
       // the __syncthreads that closed the previous iteration)
-      if (threadIdx.x == 0 && ct + nclusters < ntiles) {
+      if (threadIdx.x == 0 && t + gridDim.x < ntiles) {
         fence_proxy_async_smem();
-        const uint64_t nx = ct + nclusters;
-        bulk_load(raw + ((it + 1) & 1) * TILE, keys + tile_base(nx), bulk_bytes(tile_cnt(nx)), &bar[(it + 1) & 1]);
+        const uint64_t nx = t + gridDim.x;
+        bulk_load(raw + ((it + 1) & 1) * TILE, keys + nx * TILE, bulk_bytes(tile_cnt(nx)), &bar[(it + 1) & 1]);
       }
     }
-    for (uint32_t j = threadIdx.x; j < n_parts; j += BLOCK) hist[j] = 0u;
     KeyT k[KPT];
     uint32_t pr[KPT];
     if constexpr (BULK) {
-      if (!mbar_wait(&bar[it & 1], (it >> 1) & 1)) timed_out = true;
+      // one thread waits for the copy; the barrier publishes it to the rest
+      if (threadIdx.x == 0) mbar_wait(&bar[it & 1], (it >> 1) & 1);
+      __syncthreads();
       const uint32_t nb = bulk_bytes(cnt) / uint32_t(sizeof(KeyT));
 #pragma unroll
       for (int u = 0; u < KPT; u++) {
@@ -278,7 +277,6 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict_
         k[u] = r < cnt ? __ldcs(keys + base + r) : KeyT(0);
       }
     }
-    __syncthreads();
 #pragma unroll
     for (int u = 0; u < KPT; u++) {
       const uint32_t r = u * BLOCK + threadIdx.x;
@@ -288,42 +286,21 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict_
       }
     }
     __syncthreads();
-    // the histogram is complete: let the owners start while this CTA scans it
-    cluster.barrier_arrive();
-    for (uint32_t j = threadIdx.x; j < n_parts; j += BLOCK) lp[j] = hist[j];
+    // reservations: issued now, consumed after the local scan and sort
+    // (n_parts <= PASS1_APT * BLOCK)
+    uint32_t g[APT], hh[APT];
+#pragma unroll
+    for (uint32_t a = 0; a < APT; a++) {
+      const uint32_t j = a * BLOCK + threadIdx.x;
+      hh[a] = j < n_parts ? hist[j] : 0u;
+      g[a] = hh[a] ? atomicAdd(pcount + j, hh[a]) : 0u;
+      if (j < n_parts) {
+        lp[j] = hh[a];
+        hist[j] = 0u;  // ready for the next tile
+      }
+    }
     __syncthreads();
     block_scan_segments<BLOCK>(lp, n_parts, 0u, 0u, wsum, [](uint32_t, uint32_t) {});
-    cluster.barrier_wait();
-    // owners: sum the cluster's histograms for their partitions and reserve
-    // One (partition, CTA) pair per thread: lanes in groups of CL (a power of
-    // two dividing 32) hold one partition's per-CTA counts, scan them with
-    // shuffles, and the group's last lane reserves the cluster's run with one
-    // global atomic; every lane then hands its CTA the start.
-    for (uint32_t u0 = 0; u0 < (p1 - p0) * CL; u0 += BLOCK) {
-      const uint32_t u = u0 + threadIdx.x;
-      const uint32_t p = p0 + u / CL, c = u % CL;
-      const bool valid = p < p1;
-      const uint32_t h = valid ? cluster.map_shared_rank(hist, c)[p] : 0u;
-      uint32_t inc = h;
-#pragma unroll
-      for (unsigned o = 1; o < 16; o <<= 1) {
-        if (o < CL) {
-          const uint32_t t = __shfl_up_sync(FULL_MASK, inc, o, CL);
-          if (c >= o) inc += t;
-        }
-      }
-      const uint32_t tot = __shfl_sync(FULL_MASK, inc, CL - 1, CL);
-      uint32_t run = 0;
-      if (c == CL - 1 && tot) {
-        run = atomicAdd(pcount + p, tot);
-        if (uint64_t(run) + tot > cap) overflow = true;
-      }
-      run = __shfl_sync(FULL_MASK, run, CL - 1, CL);
-      if (valid) cluster.map_shared_rank(start, c)[p] = run + inc - h;
-    }
-    // the starts are written; the local counting sort needs only lp, so it
-    // runs while the cluster barrier completes
-    cluster.barrier_arrive();
 #pragma unroll
     for (int u = 0; u < KPT; u++) {
       const uint32_t r = u * BLOCK + threadIdx.x;
@@ -335,23 +312,31 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict_
         if constexpr (WITH_IDX) si[pos] = key_idx ? key_idx[base + r] : static_cast<uint32_t>(base + r);
       }
     }
-    __syncthreads();
-    cluster.barrier_wait();
-    for (uint32_t s = threadIdx.x; s < cnt; s += BLOCK) {
-      const uint32_t p = sp[s];
-      const uint64_t off = uint64_t(start[p]) + (s - lp[p]);
-      if (off < cap) {
-        pkeys[uint64_t(p) * cap + off] = cur[s];
-        if constexpr (WITH_IDX) pidx[uint64_t(p) * cap + off] = si[s];
-      } else {
-        overflow = true;
+    // sorted position s of partition p goes to element eoff[p] + s; a run
+    // that would pass the partition's slots is dropped (EOFF_NONE) and flags
+    // the overflow
+#pragma unroll
+    for (uint32_t a = 0; a < APT; a++) {
+      const uint32_t j = a * BLOCK + threadIdx.x;
+      if (j < n_parts) {
+        const bool fits = uint64_t(g[a]) + hh[a] <= cap;
+        overflow |= !fits;
+        eoff[j] = fits ? int64_t(j) * int64_t(cap) + int64_t(g[a]) - int64_t(lp[j]) : EOFF_NONE;
       }
     }
     __syncthreads();
-  }
-  if constexpr (BULK) {
-    // no copy is left in flight: the last iteration issued none
-    (void)timed_out;
+#pragma unroll
+    for (int u = 0; u < KPT; u++) {
+      const uint32_t s = u * BLOCK + threadIdx.x;
+      if (s < cnt) {
+        const int64_t e = eoff[sp[s]];
+        if (e != EOFF_NONE) {
+          pkeys[e + s] = cur[s];
+          if constexpr (WITH_IDX) pidx[e + s] = si[s];
+        }
+      }
+    }
+    __syncthreads();
   }
   if (overflow) atomicOr(flags, FLAG_OVERFLOW);
 }
@@ -361,7 +346,7 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict_
 // the next tile prefetched while this one is sorted): a shared-memory
 // counting sort by fine partition, one global atomic per (tile, fine
 // partition) to reserve the run, coalesced run writes.
-// Dynamic smem: hist[S] | lp[S] | base[S] | rk[2][TILE] | ri[2][TILE] | sp[TILE] (u16)
+// Dynamic smem: eoff[S] (i64) | hist[S] | lp[S] | rk[2][TILE] | ri[2][TILE] | sp[TILE] (u16) | pstart[P+1]
 template <typename KeyT, bool WITH_IDX, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys, const uint32_t* __restrict__ pidx,
                                                  const uint32_t* __restrict__ pstart, uint32_t n_parts, uint64_t cap1,
@@ -374,10 +359,10 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
   if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t S = 1u << split_log2;
-  uint32_t* hist = reinterpret_cast<uint32_t*>(smem_raw);
+  int64_t* eoff = reinterpret_cast<int64_t*>(smem_raw);  // element offset of sorted position 0, per fine partition
+  uint32_t* hist = reinterpret_cast<uint32_t*>(eoff + S);
   uint32_t* lp = hist + S;
-  uint32_t* base = lp + S;
-  KeyT* rk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(S) * 12, 16));
+  KeyT* rk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(S) * 16, 16));
   uint32_t* ri = reinterpret_cast<uint32_t*>(rk + 2 * TILE);
   uint16_t* sp = reinterpret_cast<uint16_t*>(ri + (WITH_IDX ? 2 * TILE : 0));
   uint32_t* sps = reinterpret_cast<uint32_t*>(sp + TILE);  // partition starts (n_parts + 1)
@@ -445,7 +430,7 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
     KeyT* ck = rk + buf * TILE;
     uint32_t* ci = ri + buf * TILE;
     for (uint32_t j = threadIdx.x; j < S; j += BLOCK) hist[j] = 0u;
-    mbar_wait(&bar[buf], (it >> 1) & 1);
+    if (threadIdx.x == 0) mbar_wait(&bar[buf], (it >> 1) & 1);  // published by the barrier below
     __syncthreads();
     KeyT kk[KPT];
     uint32_t ii[KPT], pp[KPT];
@@ -460,6 +445,15 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
       }
     }
     __syncthreads();
+    // reservations (S <= 2 * BLOCK): issued now, consumed after the local
+    // scan and sort, which hides the atomics' round trip
+    uint32_t g[2], hh[2];
+#pragma unroll
+    for (uint32_t a = 0; a < 2; a++) {
+      const uint32_t f = a * BLOCK + threadIdx.x;
+      hh[a] = f < S ? hist[f] : 0u;
+      g[a] = hh[a] ? atomicAdd(fcount + (q << split_log2) + f, hh[a]) : 0u;
+    }
     if (threadIdx.x < 32) {  // exclusive scan of S <= 1024 counts by one warp
       uint32_t run = 0;
       for (uint32_t j0 = 0; j0 < S; j0 += 32) {
@@ -469,12 +463,6 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
         if (j < S) lp[j] = run + inc - v;
         run += __shfl_sync(FULL_MASK, inc, 31);
       }
-    }
-    for (uint32_t f = threadIdx.x; f < S; f += BLOCK) {
-      const uint32_t h = hist[f];
-      const uint32_t b = h ? atomicAdd(fcount + (q << split_log2) + f, h) : 0u;
-      if (uint64_t(b) + h > capf) overflow = true;
-      base[f] = b;
     }
     __syncthreads();
 #pragma unroll
@@ -488,16 +476,28 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
         if constexpr (WITH_IDX) ci[pos] = ii[u];
       }
     }
+    // sorted position s of fine partition f goes to element eoff[f] + s; a
+    // run that would pass the partition's slots is dropped and flags the
+    // overflow
+#pragma unroll
+    for (uint32_t a = 0; a < 2; a++) {
+      const uint32_t f = a * BLOCK + threadIdx.x;
+      if (f < S) {
+        const bool fits = uint64_t(g[a]) + hh[a] <= capf;
+        overflow |= !fits;
+        eoff[f] = fits ? int64_t((q << split_log2) + f) * int64_t(capf) + int64_t(g[a]) - int64_t(lp[f]) : EOFF_NONE;
+      }
+    }
     __syncthreads();
-    for (uint32_t s = threadIdx.x; s < cnt; s += BLOCK) {
-      const uint32_t f = sp[s];
-      const uint64_t off = uint64_t(base[f]) + (s - lp[f]);
-      if (off < capf) {
-        const uint64_t at = ((q << split_log2) + f) * capf + off;
-        fkeys[at] = ck[s];
-        if constexpr (WITH_IDX) fidx[at] = ci[s];
-      } else {
-        overflow = true;
+#pragma unroll
+    for (int u = 0; u < KPT; u++) {
+      const uint32_t s = u * BLOCK + threadIdx.x;
+      if (s < cnt) {
+        const int64_t e = eoff[sp[s]];
+        if (e != EOFF_NONE) {
+          fkeys[e + s] = ck[s];
+          if constexpr (WITH_IDX) fidx[e + s] = ci[s];
+        }
       }
     }
     __syncthreads();
@@ -508,10 +508,12 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
 
 // Pass 3: one CTA per fine partition of W buckets.  The partition's records
 // are bulk-copied into shared memory (the next partition's copy is in flight
-// meanwhile), counted into W shared counters, the counters are scanned
-// (coalesced offsets write) and the records scattered into the partition's
+// meanwhile).  Each record is hashed once: a shared-memory atomic on its
+// bucket's counter gives its rank, kept with the bucket as (bucket << 16 |
+// rank).  The counters are scanned into the partition's offsets (coalesced
+// write) and every record goes to offsets[bucket] + rank in the partition's
 // output slice (a few tens of KB, completed while resident in L2).
-// Dynamic smem: ctr[W] | sk[2][capf] | si[2][capf]
+// Dynamic smem: ctr[2][W] | sk[2][capf] | si[2][capf] | sr[capf]
 template <typename KeyT, bool WITH_IDX, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ fkeys, const uint32_t* __restrict__ fidx,
                                                       const uint32_t* __restrict__ fstart, uint64_t n_fine, uint64_t capf,
@@ -519,16 +521,20 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ f
                                                       uint32_t* __restrict__ offsets, KeyT* __restrict__ keys_out,
                                                       uint32_t* __restrict__ idx_out, const uint32_t* flags) {
   if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
+  constexpr int NW = BLOCK / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t W = 1u << fine_log2;
-  uint32_t* ctr = reinterpret_cast<uint32_t*>(smem_raw);
-  KeyT* sk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(W) * 4, 16));
+  uint32_t* ctr2 = reinterpret_cast<uint32_t*>(smem_raw);
+  KeyT* sk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(W) * 8, 16));
   uint32_t* si = reinterpret_cast<uint32_t*>(sk + 2 * capf);
-  __shared__ uint32_t wsum[BLOCK / 32 + 1];
+  uint32_t* sr = si + (WITH_IDX ? 2 * capf : 0);
+  __shared__ uint32_t wsum[NW + 1];
   __shared__ uint64_t bar[2];
   __shared__ uint32_t s_base[2], s_m[2];
   if (blockIdx.x == 0 && threadIdx.x == 0) offsets[n_buckets] = fstart[n_fine];
   const uint64_t n_live = umin64(n_fine, (n_buckets + W - 1) >> fine_log2);  // partitions holding buckets
+  const bool off_vec = (reinterpret_cast<uintptr_t>(offsets) & 15u) == 0;
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
   // thread 0 loads a partition's start and size one iteration before it issues its copy
   auto load_meta = [&](uint64_t f) -> uint2 {
     return f < n_live ? make_uint2(fstart[f], fstart[f + 1]) : make_uint2(0u, 0u);
@@ -553,35 +559,72 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ f
     if (blockIdx.x < n_live) issue(blockIdx.x, 0, load_meta(blockIdx.x));
     next_meta = load_meta(blockIdx.x + gridDim.x);
   }
-  __syncthreads();
+  for (uint32_t j = threadIdx.x; j < W; j += BLOCK) ctr2[j] = 0u;
   uint32_t it = 0;
   for (uint64_t f = blockIdx.x; f < n_live; f += gridDim.x, it++) {
     const uint32_t buf = it & 1;
+    const uint64_t b0 = f << fine_log2;
+    const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
+    if (threadIdx.x == 0) mbar_wait(&bar[buf], (it >> 1) & 1);
+    // the copy landed (published by this barrier) and every thread finished
+    // the previous partition: its buffer and counters are free
+    __syncthreads();
     if (threadIdx.x == 0 && f + gridDim.x < n_live) {
       fence_proxy_async_smem();
       issue(f + gridDim.x, buf ^ 1u, next_meta);
       next_meta = load_meta(f + 2 * uint64_t(gridDim.x));  // consumed next iteration
     }
-    const uint64_t b0 = f << fine_log2;
-    const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
+    uint32_t* ctr = ctr2 + buf * W;
+    uint32_t* ctr_next = ctr2 + (buf ^ 1u) * W;
     const KeyT* ck = sk + buf * capf;
     const uint32_t* ci = si + buf * capf;
-    for (uint32_t j = threadIdx.x; j < nb; j += BLOCK) ctr[j] = 0u;
-    mbar_wait(&bar[buf], (it >> 1) & 1);
-    __syncthreads();
     const uint32_t base = s_base[buf];
     const uint32_t m = s_m[buf];
-    for (uint32_t r = threadIdx.x; r < m; r += BLOCK)
-      atomicAdd(&ctr[static_cast<uint32_t>(bm.of_key(ck[r]) - b0)], 1u);
-    __syncthreads();
-    block_scan_segments<BLOCK>(ctr, nb, base, base, wsum, [&](uint32_t j, uint32_t g) { offsets[b0 + j] = g; });
+    for (uint32_t j = threadIdx.x; j < W; j += BLOCK) ctr_next[j] = 0u;  // for the next partition
     for (uint32_t r = threadIdx.x; r < m; r += BLOCK) {
-      const KeyT k = ck[r];
-      const uint32_t pos = atomicAdd(&ctr[static_cast<uint32_t>(bm.of_key(k) - b0)], 1u);
-      keys_out[pos] = k;
-      if constexpr (WITH_IDX) idx_out[pos] = ci[r];
+      const uint32_t lb = static_cast<uint32_t>(bm.of_key(ck[r]) - b0);
+      sr[r] = (lb << 16) | atomicAdd(&ctr[lb], 1u);
     }
     __syncthreads();
+    if (nb == 4 * BLOCK) {
+      // four counters per thread: one block scan of the thread sums (two
+      // barriers; wsum is next written after the next partition's first)
+      const uint4 v = reinterpret_cast<const uint4*>(ctr)[threadIdx.x];
+      const uint32_t sum = v.x + v.y + v.z + v.w;
+      const uint32_t inc = warp_inclusive_scan(sum);
+      if (lane == 31) wsum[warp] = inc;
+      __syncthreads();
+      if (warp == 0) {
+        const uint32_t w = lane < NW ? wsum[lane] : 0u;
+        const uint32_t wi = warp_inclusive_scan(w);
+        if (lane < NW) wsum[lane] = wi - w;
+      }
+      __syncthreads();
+      uint4 o;
+      o.x = base + wsum[warp] + inc - sum;
+      o.y = o.x + v.x;
+      o.z = o.y + v.y;
+      o.w = o.z + v.z;
+      reinterpret_cast<uint4*>(ctr)[threadIdx.x] = o;
+      uint32_t* dst = offsets + b0 + 4 * threadIdx.x;
+      if (off_vec) {
+        *reinterpret_cast<uint4*>(dst) = o;
+      } else {
+        dst[0] = o.x;
+        dst[1] = o.y;
+        dst[2] = o.z;
+        dst[3] = o.w;
+      }
+      __syncthreads();  // the scatter reads any bucket's start
+    } else {
+      block_scan_segments<BLOCK>(ctr, nb, base, base, wsum, [&](uint32_t j, uint32_t g) { offsets[b0 + j] = g; });
+    }
+    for (uint32_t r = threadIdx.x; r < m; r += BLOCK) {
+      const uint32_t v = sr[r];
+      const uint32_t pos = ctr[v >> 16] + (v & 0xffffu);
+      keys_out[pos] = ck[r];
+      if constexpr (WITH_IDX) idx_out[pos] = ci[r];
+    }
   }
 }
 
@@ -667,11 +710,11 @@ static uint32_t ceil_log2_u64(uint64_t x) {
 }
 
 size_t pass1_smem(uint64_t n_parts, int key_bytes) {
-  return align_up(12 * n_parts, 16) + size_t(PASS1_TILE) * (2 * key_bytes + 6);
+  return align_up(16 * n_parts, 16) + size_t(PASS1_TILE) * (2 * key_bytes + 6);
 }
 
 size_t split_smem(uint32_t split_log2, int key_bytes, bool with_index, uint64_t n_parts) {
-  return align_up(12 * (size_t(1) << split_log2), 16) +
+  return align_up(16 * (size_t(1) << split_log2), 16) +
          size_t(SPLIT_TILE) * (2 * key_bytes + (with_index ? 8 : 0) + 2) + (n_parts + 1) * 4;
 }
 
@@ -712,8 +755,14 @@ bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size
   }
   const uint64_t W = 1ull << g.fine_log2;
   g.split_log2 = std::min<uint32_t>(s_max, ceil_log2_u64((n_buckets + W - 1) / W));
+  // pass 1 reserves at most PASS1_MAX_PARTS partitions per tile: split wider
+  // (up to 1024 ways) when the coarse partitions would be more
+  while (g.split_log2 < 10 && ((n_buckets + (1ull << (g.fine_log2 + g.split_log2)) - 1) >>
+                               (g.fine_log2 + g.split_log2)) > PASS1_MAX_PARTS)
+    g.split_log2++;
   g.coarse_log2 = g.fine_log2 + g.split_log2;
   g.n_parts = (n_buckets + (1ull << g.coarse_log2) - 1) >> g.coarse_log2;
+  if (g.n_parts > PASS1_MAX_PARTS) return false;
   g.n_fine = g.n_parts << g.split_log2;
   g.part_cap = slack_capacity(double(n_stream) * double(std::min<uint64_t>(1ull << g.coarse_log2, n_buckets)) /
                                   double(n_buckets), 256);
@@ -743,8 +792,12 @@ hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_in
   p.key_bytes = key_bytes;
   p.with_index = with_index;
   const size_t rec = key_bytes + (with_index ? 4 : 0);
-  // pass 3 double-buffers its partition's records: 2 * rec per staged record
-  bool part_ok = plan_geometry(n, rec, n, 2 * rec, 4, 0, n_buckets, false, &p.g);
+  // pass 3 double-buffers its partition's records (2 * rec per staged
+  // record) and its bucket counters (8 bytes per bucket), and keeps a 4-byte
+  // (bucket, rank) word per record
+  bool part_ok = plan_geometry(n, rec, n, 2 * rec + 4, 8, 0, n_buckets, false, &p.g);
+  // ranks within a bucket and local bucket numbers are packed in 16 bits
+  if (part_ok && (p.g.fine_cap >= 65536 || p.g.fine_log2 > 16)) part_ok = false;
   if (part_ok) {
     p.g.smem1 = pass1_smem(p.g.n_parts, key_bytes);
     p.g.smem2 = split_smem(p.g.split_log2, key_bytes, with_index, p.g.n_parts);
@@ -780,21 +833,6 @@ hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_in
   p.total = std::max<size_t>(off, WS_ALIGN);
   *plan = p;
   return HG_OK;
-}
-
-// Cluster size for pass 1: 16 CTAs (twice the keys per reservation) when the
-// device runs 16-CTA clusters of this shape on at least as many SMs as 8-CTA
-// ones, else 8.
-template <typename Kern>
-static unsigned pick_cluster(Kern kern, unsigned block, size_t smem, int* nclusters) {
-  const int c16 = cluster_capacity(kern, block, smem, 16);
-  const int c8 = cluster_capacity(kern, block, smem, 8);
-  if (c16 > 0 && c16 * 16 >= c8 * 8) {
-    *nclusters = c16;
-    return 16;
-  }
-  *nclusters = c8;
-  return 8;
 }
 
 // Raises a kernel's dynamic shared-memory limit to the device maximum (minus
@@ -848,16 +886,15 @@ static hg_status run_partition_passes(const PartGeometry& g, uint64_t n, const K
   uint32_t* fidx = WI ? reinterpret_cast<uint32_t*>(ws + off_fidx) : nullptr;
   if (n > 0) {
     auto kern = k_multisplit<KeyT, WI, PASS1_BLOCK, PASS1_KPT, (V > 1)>;
-    int ncl = 0;
-    const unsigned cl = pick_cluster(kern, PASS1_BLOCK, g.smem1, &ncl);
-    if (ncl <= 0) return lib_fail(HG_ERR_CUDA, "no co-resident cluster for the multisplit kernel");
-    const uint64_t ntiles = (n + uint64_t(cl) * PASS1_TILE - 1) / (uint64_t(cl) * PASS1_TILE);
-    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ntiles, uint64_t(ncl))) * cl;
+    const int bps = blocks_per_sm(kern, PASS1_BLOCK, g.smem1);
+    if (bps <= 0) return lib_fail(HG_ERR_CUDA, "multisplit kernel cannot be resident");
+    const uint64_t ntiles = (n + PASS1_TILE - 1) / PASS1_TILE;
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ntiles, uint64_t(device_sm_count()) * bps));
     Phase ph(s, who[0] == 'b' ? "multisplit" : "probe_multisplit");
     count_launch();
-    HG_CUDA(launch_cluster(kern, grid, PASS1_BLOCK, g.smem1, cl, s, keys, key_idx, n, bm, g.coarse_log2,
-                           static_cast<uint32_t>(g.n_parts), g.part_cap, pcount, pkeys, pidx, flags),
-            "multisplit launch");
+    kern<<<grid, PASS1_BLOCK, g.smem1, s>>>(keys, key_idx, n, bm, g.coarse_log2, static_cast<uint32_t>(g.n_parts),
+                                          g.part_cap, pcount, pkeys, pidx, flags);
+    HG_CUDA(cudaPeekAtLastError(), "multisplit launch");
   }
   launch_scan(pcount, g.n_parts, pstatus, ticket + 1, nullptr, pcount + g.n_parts, nullptr, s,
               who[0] == 'b' ? "part_scan" : "probe_part_scan");

@@ -53,13 +53,20 @@ struct BucketMap {
     }
     return m;
   }
+  // high 64 bits of x * d for a 32-bit d, from 32x32 products: with
+  // x = xh*2^32 + xl, x*d = (xh*d + hi32(xl*d))*2^32 + lo32(xl*d), and the
+  // low word cannot carry into bit 64, so the result is bits 32.. of
+  // xh*d + hi32(xl*d).
   __host__ __device__ __forceinline__ uint32_t of_hash(uint32_t h) const {
     if (wide) return h;
+    const uint64_t x = magic * h;
+    const uint32_t xl = static_cast<uint32_t>(x), xh = static_cast<uint32_t>(x >> 32);
 #ifdef __CUDA_ARCH__
-    return static_cast<uint32_t>(__umul64hi(magic * h, static_cast<uint64_t>(d)));
+    const uint32_t c = __umulhi(xl, d);
 #else
-    return static_cast<uint32_t>((static_cast<__uint128_t>(magic * h) * d) >> 64);
+    const uint32_t c = static_cast<uint32_t>((static_cast<uint64_t>(xl) * d) >> 32);
 #endif
+    return static_cast<uint32_t>((static_cast<uint64_t>(xh) * d + c) >> 32);
   }
   __host__ __device__ __forceinline__ uint32_t of_key(uint64_t key) const {
     return of_hash(murmur3_low32(key));

@@ -24,10 +24,12 @@ constexpr size_t FINE_PROBE_SMEM_BUDGET = 113 * 1024;  // pass-3 probe CTAs: two
 constexpr int PASS1_BLOCK = 512;
 constexpr int PASS1_KPT = 8;                     // pass-1 keys per thread per tile (registers)
 constexpr int PASS1_TILE = PASS1_BLOCK * PASS1_KPT;
+constexpr int PASS1_APT = 4;                     // pass-1 partition reservations per thread and tile
+constexpr uint64_t PASS1_MAX_PARTS = uint64_t(PASS1_APT) * PASS1_BLOCK;
 constexpr int SPLIT_BLOCK = 512;
 constexpr int SPLIT_TILE = 8 * SPLIT_BLOCK;     // k_split sorts a tile in registers: 8 records per thread
 constexpr int FINE_BLOCK = 512;
-constexpr uint32_t SPLIT_LOG2_MAX = 8;          // pass 2 splits a coarse partition up to 256 ways
+constexpr uint32_t SPLIT_LOG2_MAX = 8;          // pass 2 splits a coarse partition 256 ways (up to 1024)
 
 // Geometry of the partitioned (three-pass) paths, shared by build and probe:
 // pass 1 splits the keys into n_parts coarse partitions of 2^coarse_log2

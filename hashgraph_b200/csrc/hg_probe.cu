@@ -13,9 +13,9 @@
 // The count-only form skips the look-back and adds tile sums atomically.
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "hg_bulk.cuh"
-#include "hg_cluster.cuh"
 #include "hg_device.cuh"
 #include "hg_plan.h"
 #include "hg_prof.cuh"
@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(PROBE_BLOCK)
 // bucket).  A round covers FPROBE_QCH*BLOCK queries, so a partition normally
 // takes one.
 // Dynamic smem: [2] x { off[W+4] | keys[capa + 2*EPK] | idx[capa + 8] | qkeys[capq] | qidx[capq] }
-constexpr int FPROBE_QCH = 8;
+constexpr int FPROBE_QCH = 5;
 
 __host__ __device__ inline size_t fine_probe_buf_bytes(uint32_t fine_log2, uint32_t capa, uint64_t capq,
                                                        int key_bytes, bool a_idx, bool emit) {
@@ -251,109 +251,143 @@ __global__ void __launch_bounds__(BLOCK)
   uint32_t it = 0;
   for (uint64_t f = blockIdx.x; f < n_live; f += gridDim.x, it++) {
     const uint32_t b = it & 1;
+    const uint64_t b0 = f << fine_log2;
+    const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
+    if (threadIdx.x == 0) mbar_wait(&bar[b], (it >> 1) & 1);
+    // the copy into buffer b landed (published by this barrier), and every
+    // thread finished the previous partition, so buffer b ^ 1 is free
+    __syncthreads();
     if (threadIdx.x == 0 && f + gridDim.x < n_live) {
       fence_proxy_async_smem();
       issue(f + gridDim.x, b ^ 1u, next_meta);
       next_meta = load_meta(f + 2 * uint64_t(gridDim.x));  // consumed next iteration
     }
-    const uint64_t b0 = f << fine_log2;
-    const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
-    mbar_wait(&bar[b], (it >> 1) & 1);
     uint32_t* soff = buf_off(b);
     KeyT* sk = buf_keys(b);
     uint32_t* si = buf_idx(b);
     const uint32_t as = s_as[b], ae = s_ae[b], al = s_al[b], ar = s_ar[b];
     const bool spill = ae - as + 2 * EPK > capa;
     // whatever the bulk copies could not cover (the end of A's arrays, or
-    // unaligned arrays)
-    for (uint32_t j = s_oplain[b] + threadIdx.x; j <= nb; j += BLOCK) soff[j] = a_off[b0 + j];
-    if (!spill) {
-      for (uint32_t x = ar + threadIdx.x; x < ae; x += BLOCK) sk[x - al] = a_keys[x];
-      if constexpr (A_IDX) {
-        const uint32_t ial = s_ial[b], iar = s_iar[b];
-        for (uint32_t x = iar + threadIdx.x; x < ae; x += BLOCK) si[x - ial] = a_idx[x];
+    // unaligned arrays): plain loads, rare, so the barrier is taken only then
+    const uint32_t oplain = s_oplain[b];
+    const bool plain = oplain <= nb || (!spill && (ar < ae || (A_IDX && s_iar[b] < ae)));
+    if (plain) {
+      for (uint32_t j = oplain + threadIdx.x; j <= nb; j += BLOCK) soff[j] = a_off[b0 + j];
+      if (!spill) {
+        for (uint32_t x = ar + threadIdx.x; x < ae; x += BLOCK) sk[x - al] = a_keys[x];
+        if constexpr (A_IDX) {
+          const uint32_t ial = s_ial[b], iar = s_iar[b];
+          for (uint32_t x = iar + threadIdx.x; x < ae; x += BLOCK) si[x - ial] = a_idx[x];
+        }
       }
+      __syncthreads();
     }
-    __syncthreads();
     const uint32_t m = s_qm[b];
     const KeyT* sq = buf_q(b);
     const uint32_t* sqi = buf_qi(b);
     const uint32_t koff = as - al;  // sk[x + koff] is A's key at global position as + x
     uint32_t ioff = 0;
     if constexpr (A_IDX) ioff = as - s_ial[b];
-    auto a_key = [&](uint32_t x) -> KeyT { return spill ? a_keys[as + x] : sk[x + koff]; };
-    auto a_ref = [&](uint32_t x) -> uint32_t {
-      if constexpr (A_IDX) return spill ? a_idx[as + x] : si[x + ioff];
-      else return as + x;
-    };
-
-    for (uint32_t r0 = 0; r0 < m; r0 += QCH * BLOCK) {
-      uint32_t cnt[QCH], ref[QCH];
-      uint64_t mine = 0;
+    // SPILL: A's slice did not fit and is read in place from global memory
+    auto probe_partition = [&](auto spill_c) {
+      constexpr bool SPILL = decltype(spill_c)::value;
+      auto a_key = [&](uint32_t x) -> KeyT {
+        if constexpr (SPILL) return a_keys[as + x];
+        else return sk[x + koff];
+      };
+      auto a_ref = [&](uint32_t x) -> uint32_t {
+        if constexpr (A_IDX) {
+          if constexpr (SPILL) return a_idx[as + x];
+          else return si[x + ioff];
+        } else {
+          return as + x;
+        }
+      };
+      for (uint32_t r0 = 0; r0 < m; r0 += QCH * BLOCK) {
+        uint32_t cnt[QCH], ref[QCH], xs[QCH], xe[QCH];
+        KeyT kq[QCH];
 #pragma unroll
-      for (uint32_t j = 0; j < QCH; j++) {
-        const uint32_t r = r0 + j * BLOCK + threadIdx.x;
-        cnt[j] = 0;
-        ref[j] = 0;
-        if (r < m) {
-          const KeyT k = sq[r];
-          const uint32_t lb = static_cast<uint32_t>(bm.of_key(k) - b0);
-          const uint32_t e = soff[lb + 1] - as;
-          for (uint32_t x = soff[lb] - as; x < e; x++) {
-            if (a_key(x) == k) {
-              if (cnt[j] == 0) ref[j] = a_ref(x);
-              cnt[j]++;
-            }
+        for (uint32_t j = 0; j < QCH; j++) {
+          cnt[j] = ref[j] = xs[j] = xe[j] = 0;
+          kq[j] = 0;
+          if (r0 + j * BLOCK >= m) continue;  // uniform: chunk j holds no query
+          const uint32_t r = r0 + j * BLOCK + threadIdx.x;
+          if (r < m) {
+            kq[j] = sq[r];
+            const uint32_t lb = static_cast<uint32_t>(bm.of_key(kq[j]) - b0);
+            xs[j] = soff[lb] - as;
+            xe[j] = soff[lb + 1] - as;
           }
-          mine += cnt[j];
         }
-      }
-      if constexpr (!EMIT) {
-        counted += mine;
-      } else {
-        // block scan of the thread totals; warp 0 reserves the round's range
-        const uint64_t inc = warp_inclusive_scan(mine);
-        if (lane == 31) red[warp] = inc;
-        __syncthreads();
-        if (warp == 0) {
-          const uint64_t w = lane < NW ? red[lane] : 0ull;
-          const uint64_t wi = warp_inclusive_scan(w);
-          const uint64_t tot = __shfl_sync(FULL_MASK, wi, NW - 1);
-          uint64_t base = 0;
-          if (lane == 0 && tot) {
-            base = atomicAdd(d_count, static_cast<unsigned long long>(tot));
-            if (base + tot > pair_cap) record_error(HG_ERR_PAIR_CAPACITY);
-          }
-          base = __shfl_sync(FULL_MASK, base, 0);
-          if (lane < NW) red[lane] = base + wi - w;
-        }
-        __syncthreads();
-        uint64_t pos = red[warp] + inc - mine;
-        if (mine) {
+        // walk the thread's buckets side by side: the warp runs as many steps
+        // as its longest bucket, not the sum of every query's longest
+        for (bool more = true; more;) {
+          more = false;
 #pragma unroll
           for (uint32_t j = 0; j < QCH; j++) {
-            const uint32_t r = r0 + j * BLOCK + threadIdx.x;
-            if (cnt[j] == 1) {
-              if (pos < pair_cap) reinterpret_cast<uint2*>(pairs)[pos] = make_uint2(ref[j], sqi[r]);
-              pos++;
-            } else if (cnt[j] > 1) {
-              const KeyT k = sq[r];
-              const uint32_t qref = sqi[r];
-              const uint32_t lb = static_cast<uint32_t>(bm.of_key(k) - b0);
-              const uint32_t e = soff[lb + 1] - as;
-              for (uint32_t x = soff[lb] - as; x < e; x++) {
-                if (a_key(x) == k) {
-                  if (pos < pair_cap) reinterpret_cast<uint2*>(pairs)[pos] = make_uint2(a_ref(x), qref);
-                  pos++;
+            if (xs[j] < xe[j]) {
+              const uint32_t x = xs[j]++;
+              if (a_key(x) == kq[j]) {
+                if (cnt[j] == 0) ref[j] = a_ref(x);
+                cnt[j]++;
+              }
+              more |= xs[j] < xe[j];
+            }
+          }
+        }
+        uint64_t mine = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < QCH; j++) mine += cnt[j];
+        if constexpr (!EMIT) {
+          counted += mine;
+        } else {
+          // block scan of the thread totals; warp 0 reserves the round's range
+          const uint64_t inc = warp_inclusive_scan(mine);
+          if (lane == 31) red[warp] = inc;
+          __syncthreads();
+          if (warp == 0) {
+            const uint64_t w = lane < NW ? red[lane] : 0ull;
+            const uint64_t wi = warp_inclusive_scan(w);
+            const uint64_t tot = __shfl_sync(FULL_MASK, wi, NW - 1);
+            uint64_t base = 0;
+            if (lane == 0 && tot) {
+              base = atomicAdd(d_count, static_cast<unsigned long long>(tot));
+              if (base + tot > pair_cap) record_error(HG_ERR_PAIR_CAPACITY);
+            }
+            base = __shfl_sync(FULL_MASK, base, 0);
+            if (lane < NW) red[lane] = base + wi - w;
+          }
+          __syncthreads();
+          uint64_t pos = red[warp] + inc - mine;
+          if (mine) {
+            uint2* out = reinterpret_cast<uint2*>(pairs);
+#pragma unroll
+            for (uint32_t j = 0; j < QCH; j++) {
+              if (r0 + j * BLOCK >= m) continue;
+              const uint32_t r = r0 + j * BLOCK + threadIdx.x;
+              if (cnt[j] == 1) {
+                if (pos < pair_cap) out[pos] = make_uint2(ref[j], sqi[r]);
+                pos++;
+              } else if (cnt[j] > 1) {
+                const KeyT k = sq[r];
+                const uint32_t qref = sqi[r];
+                const uint32_t lb = static_cast<uint32_t>(bm.of_key(k) - b0);
+                const uint32_t e = soff[lb + 1] - as;
+                for (uint32_t x = soff[lb] - as; x < e; x++) {
+                  if (a_key(x) == k) {
+                    if (pos < pair_cap) out[pos] = make_uint2(a_ref(x), qref);
+                    pos++;
+                  }
                 }
               }
             }
           }
+          if (r0 + QCH * BLOCK < m) __syncthreads();  // red is rewritten by the next round
         }
-        if (r0 + QCH * BLOCK < m) __syncthreads();  // red is rewritten by the next round
       }
-    }
-    __syncthreads();  // all reads of buffer b end before it is refilled
+    };
+    if (spill) probe_partition(std::true_type{});
+    else probe_partition(std::false_type{});
   }
   if constexpr (!EMIT) {
     uint64_t tot;

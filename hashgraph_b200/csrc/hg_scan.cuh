@@ -114,4 +114,46 @@ __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint64_
   return excl;
 }
 
+// Exclusive scan of ctr[0..nb) in shared memory by a block of BLOCK threads:
+// warp w scans the contiguous segment [w*seg, (w+1)*seg) in chunks of 32
+// (coalesced), after a block scan of the segment totals.  Replaces ctr[j] by
+// base_local + exclusive prefix and calls out(j, global_value) for each j with
+// global_value = base_global + exclusive prefix.  Returns the total.
+// `wsum` needs BLOCK/32 + 1 entries.  Contains __syncthreads().
+template <int BLOCK, typename Out>
+__device__ __forceinline__ uint32_t block_scan_segments(uint32_t* ctr, uint32_t nb, uint32_t base_local,
+                                                        uint32_t base_global, uint32_t* wsum, Out out) {
+  constexpr int NW = BLOCK / 32;
+  const unsigned warp = threadIdx.x >> 5, lane = lane_id();
+  const uint32_t seg = ((nb + NW - 1) / NW + 31) & ~31u;
+  const uint32_t s0 = min(nb, warp * seg), s1 = min(nb, s0 + seg);
+  uint32_t part = 0;
+  for (uint32_t j = s0 + lane; j < s1; j += 32) part += ctr[j];
+  part = warp_sum(part);
+  if (lane == 0) wsum[warp] = part;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t w = lane < NW ? wsum[lane] : 0u;
+    const uint32_t wi = warp_inclusive_scan(w);
+    if (lane < NW) wsum[lane] = wi - w;
+    if (lane == NW - 1) wsum[NW] = wi;
+  }
+  __syncthreads();
+  uint32_t run = wsum[warp];
+  for (uint32_t j0 = s0; j0 < s1; j0 += 32) {
+    const uint32_t j = j0 + lane;
+    const uint32_t v = j < s1 ? ctr[j] : 0u;
+    const uint32_t inc = warp_inclusive_scan(v);
+    if (j < s1) {
+      const uint32_t ex = run + inc - v;
+      ctr[j] = base_local + ex;
+      out(j, base_global + ex);
+    }
+    run += __shfl_sync(FULL_MASK, inc, 31);
+  }
+  const uint32_t total = wsum[NW];
+  __syncthreads();
+  return total;
+}
+
 }  // namespace hg

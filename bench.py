@@ -111,6 +111,26 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per key of each
+# partition kernel, from one ncu capture at 2^25 u64 keys, 2^25 buckets,
+# table without index, 25% overlap, same per-CTA geometry as 2^28 (the
+# capture summarised under profiles/).  Traffic grows with the keys
+# processed, so a full launch's traffic is this figure times its keys.
+MEASURED_TRAFFIC_PER_KEY = {
+    (8, False): {"multisplit": 14.5, "split": 14.4, "fine_build": 18.4,
+                 "probe_multisplit": 18.6, "probe_split": 22.3, "fine_probe_emit": 25.9},
+}
+
+
+def measured_traffic(phase, kb, with_index, n, nq, B):
+    """Per-launch DRAM traffic of `phase` scaled from the capture, or None
+    when the workload's shape differs from the captured one."""
+    per = MEASURED_TRAFFIC_PER_KEY.get((kb, with_index), {}).get(phase)
+    if per is None or n != nq or B != n:
+        return None
+    return per * n
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -176,7 +196,8 @@ def sum_over_ranks(x, world):
 # ---------------------------------------------------------------------------
 def algorithmic_bytes(phase, kb, n, nq, B, with_index, pairs):
     """Bytes each kernel's role must move (its inputs read once, its outputs
-    written once); the per-unit figures are stated in DESIGN.md."""
+    written once): per key, K read and K (+4 index) written by a partition
+    pass; the fine passes add the 4-byte offsets and the 8-byte pairs."""
     rec = kb + (4 if with_index else 0)
     qrec = kb + 4
     return {
@@ -348,7 +369,9 @@ def run_ours(args, rank, world, local):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (each set %d MiB vs 126 MB L2); no flush" % (n * kb >> 20)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": measured_traffic(dom, kb, with_index, n, nq, B),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 2^25, scaled by keys",
                      "peak_source": peak_kind, "algorithmic_bytes": alg,
                      "avg_launch_ms": phase_avg[dom]},
         "step_roofline": {"compulsory_bytes": build_bytes + isect_bytes,

@@ -390,6 +390,183 @@ def run_ours(args, rank, world, local):
 
 
 # ---------------------------------------------------------------------------
+# batched build + intersect (many independent pairs per step)
+# ---------------------------------------------------------------------------
+def batched_sizes(n_pairs, lo_log2, hi_log2, seed=4):
+    """Pair i: n_i = floor(2^U(lo, hi)) keys (log-uniform), B_i = n_i buckets,
+    n_i queries with overlap fraction U(0, 1); seeded."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    sizes = np.floor(2.0 ** rng.uniform(lo_log2, hi_log2, n_pairs)).astype(np.int64)
+    fracs = rng.uniform(0.0, 1.0, n_pairs)
+    return sizes, fracs
+
+
+def run_batched(args, rank, world, local):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import hashgraph_b200 as hg
+
+    kb = 8
+    sizes, fracs = batched_sizes(args.pairs, 6, 20)
+    n_total = int(sizes.sum())
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    L = hg.lib()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    # every pair's keys and queries are views of two arena tensors
+    a_all = torch.empty(n_total, dtype=torch.int64, device=dev)
+    q_all = torch.empty(n_total, dtype=torch.int64, device=dev)
+    starts = np.concatenate([[0], np.cumsum(sizes)])
+    a_views = [a_all[starts[i]:starts[i + 1]] for i in range(args.pairs)]
+    q_views = [q_all[starts[i]:starts[i + 1]] for i in range(args.pairs)]
+    for i in range(args.pairs):
+        n = int(sizes[i])
+        check = hg._capi.check
+        check(L.hg_gen_uniform(ctypes.c_void_p(a_views[i].data_ptr()), n, kb, 100_000 + i, sptr), "gen")
+        m = hg.overlap_count(n, n, float(fracs[i]))
+        check(L.hg_gen_overlap(ctypes.c_void_p(q_views[i].data_ptr()), n, kb,
+                               ctypes.c_void_p(a_views[i].data_ptr()), n, m, 200_000 + i, sptr), "gen")
+    B = [int(x) for x in sizes]
+    batch = hg.Batch(a_views, q_views, B, with_index=False, pair_caps=B)
+    for _ in range(args.warmup):
+        batch.run()
+    torch.cuda.synchronize(dev)
+    if hg.device_error() != 0:
+        raise RuntimeError("device error during warm-up")
+    matches = int(batch.counts[: args.pairs].sum().item())
+
+    hg.profile_enable(True)
+    hg.profile_read()
+    clocks = ClockSampler(local)
+    launches0 = hg.launch_count()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps)]
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    time.sleep(0.3)
+    for k in range(args.steps):
+        ev[2 * k].record(stream)
+        batch.run()
+        ev[2 * k + 1].record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    launches = hg.launch_count() - launches0
+    clk = clocks.stop()
+    phases = hg.profile_read()
+    hg.profile_enable(False)
+    total_ms = sum(ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps))
+    total_ms_max = max_over_ranks(total_ms, world)
+    if hg.device_error() != 0:
+        raise RuntimeError("device error during timed steps")
+    value = sum_over_ranks(n_total * args.steps, world) / (total_ms_max * 1e-3)
+    per_phase = {}
+    for name, ms in phases:
+        per_phase.setdefault(name, []).append(ms)
+    phase_avg = {k: sum(v) / len(v) for k, v in per_phase.items()}
+    dom = max(per_phase, key=lambda k: sum(per_phase[k]))
+    peak, peak_kind = load_peaks()
+    sum_b = n_total + args.pairs  # buckets + 1 per pair
+    alg = {"batch_count": n_total * kb, "batch_scan": 8 * sum_b, "batch_scatter": 2 * n_total * kb,
+           "batch_probe": n_total * kb * 2 + 4 * sum_b + 8 * matches, "batch_clear": 4 * sum_b}.get(dom)
+    achieved = alg / (phase_avg[dom] * 1e-3) / 1e9 if alg else None
+    compulsory = n_total * kb * 2 + 4 * sum_b + (n_total * kb * 2 + 4 * sum_b + 8 * matches)
+    step_s = total_ms / args.steps * 1e-3
+
+    # the same pairs as one build + intersect call each (the launch-bound form)
+    ws_b = ctypes.c_size_t(0)
+    ws_q = ctypes.c_size_t(0)
+    nmax = int(sizes.max())
+    hg._capi.check(L.hg_build_workspace_size_path(nmax, kb, nmax, 0, 0, ctypes.byref(ws_b)), "ws")
+    hg._capi.check(L.hg_intersect_workspace_size_path(nmax, 0, nmax, nmax, kb, 1, 0, ctypes.byref(ws_q)), "ws")
+    ws = torch.empty(max(ws_b.value, ws_q.value, 1), dtype=torch.uint8, device=dev)
+
+    def plain_step():
+        for i in range(args.pairs):
+            n = int(sizes[i])
+            hg._capi.check(L.hg_build_into_path(
+                ctypes.c_void_p(a_views[i].data_ptr()), n, kb, n, ctypes.c_void_p(batch.offsets[i].data_ptr()),
+                ctypes.c_void_p(batch.table_keys[i].data_ptr()), None, ctypes.c_void_p(ws.data_ptr()),
+                ws.numel(), 0, sptr), "plain build")
+            hg._capi.check(L.hg_intersect_into_path(
+                ctypes.c_void_p(batch.offsets[i].data_ptr()), ctypes.c_void_p(batch.table_keys[i].data_ptr()),
+                None, n, n, kb, ctypes.c_void_p(q_views[i].data_ptr()), n, None,
+                ctypes.c_void_p(batch.pairs[i].data_ptr()), n,
+                ctypes.c_void_p(batch.counts.data_ptr() + 8 * i), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+                0, sptr), "plain intersect")
+
+    plain_step()
+    torch.cuda.synchronize(dev)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    plain_step()
+    p1.record(stream)
+    torch.cuda.synchronize(dev)
+    plain_ms = p0.elapsed_time(p1)
+    if int(batch.counts[: args.pairs].sum().item()) != matches:
+        raise RuntimeError("plain calls and the batch disagree on the match count")
+
+    e2e = None
+    if not args.skip_e2e:
+        h_a = torch.empty(n_total, dtype=torch.int64, pin_memory=True)
+        h_q = torch.empty(n_total, dtype=torch.int64, pin_memory=True)
+        h_a.copy_(a_all)
+        h_q.copy_(q_all)
+        h_counts = torch.empty(args.pairs, dtype=torch.int64, pin_memory=True)
+        h_pairs = torch.empty((n_total, 2), dtype=torch.int32, pin_memory=True)
+        pstart = starts
+        d2h = 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.steps):
+            a_all.copy_(h_a, non_blocking=True)
+            q_all.copy_(h_q, non_blocking=True)
+            batch.run()
+            h_counts.copy_(batch.counts[: args.pairs], non_blocking=True)
+            stream.synchronize()
+            d2h += 8 * args.pairs
+            cnt = h_counts.numpy()
+            for i in range(args.pairs):
+                c = int(cnt[i])
+                if c:
+                    h_pairs[pstart[i]:pstart[i] + c].copy_(batch.pairs[i][:c], non_blocking=True)
+                    d2h += 8 * c
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+        e2e = {"value": sum_over_ranks(n_total * args.steps, world) / (e2e_ms * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": int(2 * n_total * kb), "d2h_bytes_per_step": int(d2h // args.steps)}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded splitmix64 keys generated on the device; definitions shared with the oracle)",
+        "config": {"workload": f"batched: {args.pairs} pairs, A_i = 2^U(6,20) u64 uniform keys into B_i = n_i "
+                               f"buckets, n_i queries with U(0,1) drawn from A_i, pairs emitted; one "
+                               f"hg_batch_run per step",
+                   "pairs": args.pairs, "keys_total": n_total, "matches": matches,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs (%d MiB per set) larger than L2; no flush" % (n_total * kb >> 20)},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "peak_source": peak_kind, "algorithmic_bytes": alg, "avg_launch_ms": phase_avg[dom]},
+        "step_roofline": {"compulsory_bytes": compulsory, "achieved_gbs": compulsory / step_s / 1e9,
+                          "frac_of_measured_hbm": compulsory / step_s / 1e9 / peak},
+        "plain_calls": {"ms_per_step": plain_ms, "value": n_total / (plain_ms * 1e-3), "unit": UNIT,
+                        "calls": 2 * args.pairs,
+                        "note": "one hg_build_into + hg_intersect_into (direct path) per pair, same buffers"},
+        "phases_ms": phase_avg, "clocks": clk, "e2e": e2e, "gpu_launches": launches, "cpu_baseline": None,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # CPU baseline / reference arm
 # ---------------------------------------------------------------------------
 def cpu_run(workload, n_sample, repeats=3):
@@ -428,8 +605,51 @@ def cpu_baseline(workload, n_sample):
                       f"build {tb:.3f} s + intersect {ti:.3f} s"}
 
 
+def run_reference_batched(args):
+    """The oracle's multithreaded build + probe over the batched workload's
+    pairs, in order, until about --cpu-sample keys (a bounded sample)."""
+    import oracle
+    sizes, fracs = batched_sizes(args.pairs, 6, 20)
+    cores = oracle.max_threads()
+    inputs, total = [], 0
+    for i in range(args.pairs):
+        n = int(sizes[i])
+        a = oracle.gen_uniform(n, 8, 100_000 + i)
+        q = oracle.gen_overlap(n, a, float(fracs[i]), 200_000 + i)
+        inputs.append((a, q, n))
+        total += n
+        if total >= args.cpu_sample // 4:
+            break
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        for a, q, n in inputs:
+            off, kk, ii = oracle.build(a, n, False, threads=cores)
+            oracle.intersect(off, kk, ii, q, pair_cap=n, threads=cores)
+        if k >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    value = total * len(times) / sum(times)
+    sample = (f"the first {len(inputs)} of {args.pairs} pairs ({total} keys per set), each built and "
+              "probed by the oracle's multithreaded restatement (the reference has no CPU path)")
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(times) / len(times) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded splitmix64 keys; same generators as our arm)",
+        "config": {"workload": f"batched: {args.pairs} pairs, A_i = 2^U(6,20) u64 uniform keys into B_i = n_i "
+                               "buckets, n_i queries with U(0,1) drawn from A_i, pairs emitted",
+                   "pairs": args.pairs},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
+        return
+    if args.workload == "batched":
+        run_reference_batched(args)
         return
     import oracle
     kb, n, bfn, kind, seed_a, seed_q, overlap, with_index = WORKLOADS[args.workload]
@@ -466,7 +686,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="large")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched"], default="large")
+    ap.add_argument("--pairs", type=int, default=4096, help="pairs of the batched workload")
     ap.add_argument("--n", type=int, default=0, help="override keys per set (parity/profiling runs)")
     ap.add_argument("--cpu-sample", type=int, default=1 << 26)
     ap.add_argument("--skip-cpu", action="store_true")
@@ -482,7 +703,10 @@ def main():
         return
     rank, world, local = dist_setup(args.gpus)
     try:
-        run_ours(args, rank, world, local)
+        if args.workload == "batched":
+            run_batched(args, rank, world, local)
+        else:
+            run_ours(args, rank, world, local)
     finally:
         if world > 1:
             import torch.distributed as dist

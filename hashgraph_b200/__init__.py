@@ -12,14 +12,14 @@ from __future__ import annotations
 
 import ctypes
 
-from ._capi import (ERR_DEVICE_TIMEOUT, ERR_PAIR_CAPACITY, HGError, build_library, check, lib,
-                    status_str)
+from ._capi import (ERR_DEVICE_TIMEOUT, ERR_PAIR_CAPACITY, BatchPair, HGError, build_library, check,
+                    lib, status_str)
 
 __all__ = [
     "HGError", "Table", "build_library", "lib", "hash_keys", "intersect", "device_error",
     "gen_uniform", "gen_overlap", "gen_zipf", "zipf_cdf", "PATH_AUTO", "PATH_DIRECT",
     "PATH_PARTITIONED", "ERR_PAIR_CAPACITY", "ERR_DEVICE_TIMEOUT", "status_str",
-    "profile_enable", "profile_read", "launch_count",
+    "profile_enable", "profile_read", "launch_count", "Batch",
 ]
 
 PATH_AUTO, PATH_DIRECT, PATH_PARTITIONED = -1, 0, 1
@@ -186,6 +186,86 @@ def intersect(a: Table, queries, query_idx=None, emit: bool = True, pair_cap: in
         nq, _ptr(query_idx), _ptr(pairs), int(pair_cap) if emit else 0, _ptr(count), _ptr(ws),
         ws.numel(), path, _stream(stream)), "hg_intersect_into")
     return count, pairs
+
+
+class Batch:
+    """Batched build + intersect of many (table, queries) pairs (hg_batch_*).
+
+    ``keys[i]`` is built into a table of ``n_buckets[i]`` buckets (with the
+    input positions when ``with_index[i]``) and ``queries[i]`` are probed
+    against it.  The output tensors are allocated here and kept on the object:
+    ``offsets[i]``, ``table_keys[i]``, ``table_idx[i]`` (or None),
+    ``pairs[i]`` ([pair_caps[i], 2] int32, or None when emit is False) and
+    ``counts`` (int64, one exact match count per pair).  ``run()`` launches
+    the whole batch (a fixed sequence of five kernels, capturable into a CUDA
+    graph); the input tensors must stay alive and may be refilled between
+    runs.  All pairs share one key width.
+    """
+
+    def __init__(self, keys, queries, n_buckets, with_index=False, pair_caps=None, emit=True,
+                 stream=None):
+        torch = _torch()
+        n_pairs = len(keys)
+        if len(queries) != n_pairs or len(n_buckets) != n_pairs:
+            raise ValueError("keys, queries and n_buckets must have one entry per pair")
+        if isinstance(with_index, bool):
+            with_index = [with_index] * n_pairs
+        if pair_caps is None:
+            pair_caps = [q.numel() for q in queries]
+        kb = _key_bytes(keys[0]) if n_pairs else 8
+        self.key_bytes = kb
+        self.keys, self.queries = list(keys), list(queries)
+        dev = keys[0].device if n_pairs else torch.device("cuda")
+        self.counts = torch.zeros(max(n_pairs, 1), dtype=torch.int64, device=dev)
+        self.offsets, self.table_keys, self.table_idx, self.pairs = [], [], [], []
+        descs = (BatchPair * max(n_pairs, 1))()
+        for i in range(n_pairs):
+            k, q = keys[i], queries[i]
+            _check_cuda(k, "keys")
+            _check_cuda(q, "queries")
+            if _key_bytes(k) != kb or _key_bytes(q) != kb:
+                raise HGError(-8, "all keys and queries of a batch share one width")
+            B = int(n_buckets[i])
+            off = torch.empty(B + 1, dtype=torch.int32, device=dev)
+            tk = torch.empty(max(k.numel(), 1), dtype=k.dtype, device=dev)
+            ti = torch.empty(max(k.numel(), 1), dtype=torch.int32, device=dev) if with_index[i] else None
+            pr = torch.empty((max(int(pair_caps[i]), 1), 2), dtype=torch.int32, device=dev) if emit else None
+            self.offsets.append(off)
+            self.table_keys.append(tk)
+            self.table_idx.append(ti)
+            self.pairs.append(pr)
+            d = descs[i]
+            d.d_keys, d.n, d.n_buckets = k.data_ptr() if k.numel() else None, k.numel(), B
+            d.d_query, d.nq = q.data_ptr() if q.numel() else None, q.numel()
+            d.d_offsets, d.d_keys_out = off.data_ptr(), tk.data_ptr()
+            d.d_idx_out = ti.data_ptr() if ti is not None else None
+            d.d_pairs = pr.data_ptr() if pr is not None else None
+            d.pair_cap = int(pair_caps[i]) if emit else 0
+            d.d_count = self.counts.data_ptr() + 8 * i
+        self.n_pairs = n_pairs
+        self._h = ctypes.c_void_p()
+        check(lib().hg_batch_create(descs, n_pairs, kb, _stream(stream), ctypes.byref(self._h)),
+              "hg_batch_create")
+
+    def run(self, stream=None) -> "Batch":
+        check(lib().hg_batch_run(self._h, _stream(stream)), "hg_batch_run")
+        return self
+
+    def device_bytes(self) -> int:
+        out = ctypes.c_size_t(0)
+        check(lib().hg_batch_device_bytes(self._h, ctypes.byref(out)), "hg_batch_device_bytes")
+        return int(out.value)
+
+    def free(self, stream=None) -> None:
+        if self._h:
+            lib().hg_batch_free(self._h, _stream(stream))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------

@@ -38,6 +38,16 @@ _i32 = ctypes.c_int32
 _int = ctypes.c_int
 _sz = ctypes.c_size_t
 _pp = ctypes.POINTER(ctypes.c_void_p)
+class BatchPair(ctypes.Structure):
+    """hg_batch_pair of include/hashgraph_b200.h."""
+    _fields_ = [
+        ("d_keys", ctypes.c_void_p), ("n", ctypes.c_uint64), ("n_buckets", ctypes.c_uint64),
+        ("d_query", ctypes.c_void_p), ("nq", ctypes.c_uint64), ("d_offsets", ctypes.c_void_p),
+        ("d_keys_out", ctypes.c_void_p), ("d_idx_out", ctypes.c_void_p), ("d_pairs", ctypes.c_void_p),
+        ("pair_cap", ctypes.c_uint64), ("d_count", ctypes.c_void_p),
+    ]
+
+
 SIGNATURES = {
     "hg_status_str": (ctypes.c_char_p, [_i32]),
     "hg_version": (ctypes.c_char_p, []),
@@ -72,6 +82,11 @@ SIGNATURES = {
     "hg_gen_bounded": (_i32, [_p, _u64, _int, _u64, _u64, _p]),
     "hg_gather_pair_keys": (_i32, [_p, _int, _p, _u64, _int, _p, _p]),
     "hg_export_reference_layout": (_i32, [_p, _p, _p, _u64, _u64, _int, _p, _p, _p]),
+    "hg_batch_create": (_i32, [ctypes.POINTER(BatchPair), _int, _int, _p, _pp]),
+    "hg_batch_run": (_i32, [_p, _p]),
+    "hg_batch_device_bytes": (_i32, [_p, ctypes.POINTER(_sz)]),
+    "hg_batch_free": (None, [_p, _p]),
+    "hg_batch_build_intersect": (_i32, [ctypes.POINTER(BatchPair), _int, _int, _p]),
     "hg_profile_enable": (_i32, [_int]),
     "hg_profile_read": (_i32, [_int, ctypes.POINTER(_int), ctypes.POINTER(ctypes.c_char_p),
                                ctypes.POINTER(ctypes.c_float)]),

@@ -6,3 +6,4 @@
 #include "hg_gen.cu"
 #include "hg_api.cu"
 #include "hg_noalloc.cu"
+#include "hg_batch.cu"

@@ -200,6 +200,59 @@ hg_status hg_intersect_tables(const hg_table* a, const hg_table* b, uint32_t* d_
                               uint64_t pair_cap, unsigned long long* d_count, hg_stream_t stream);
 
 /* ------------------------------------------------------------------------
+ * Batched build + intersect: many independent (table, queries) pairs in one
+ * launch sequence.  No counterpart in the reference, which builds and
+ * intersects one MultiHashGraph at a time (test/MultiHashGraphTest.cu:288-338,
+ * src/MultiHashGraph.cu:408-740); each pair's result equals the one
+ * hg_build_into + hg_intersect_into (direct path) would give it: the same
+ * offsets, the same buckets, the same count and the same pairs in the same
+ * query order (keys inside one bucket in unspecified order, as for every
+ * build).
+ *
+ * For each pair i: build table i from d_keys[0..n) into d_offsets
+ * [n_buckets + 1], d_keys_out [n] and, when d_idx_out is not NULL, d_idx_out
+ * [n] (input positions); then probe d_query[0..nq) against it: *d_count gets
+ * the exact match count and, when d_pairs is not NULL, the first pair_cap
+ * (a_ref, q_ref) pairs are written (a_ref = index or CSR position, q_ref =
+ * query position).  A pair whose count exceeds pair_cap sets
+ * HG_ERR_PAIR_CAPACITY in the device error word.  All pairs share the key
+ * width.  Every pointer is device memory owned by the caller; the buffers
+ * must not overlap between pairs.
+ * ---------------------------------------------------------------------- */
+typedef struct hg_batch_pair {
+  const void* d_keys;
+  uint64_t n;
+  uint64_t n_buckets;
+  const void* d_query;
+  uint64_t nq;
+  uint32_t* d_offsets;
+  void* d_keys_out;
+  uint32_t* d_idx_out;
+  uint32_t* d_pairs;
+  uint64_t pair_cap;
+  unsigned long long* d_count;
+} hg_batch_pair;
+
+typedef struct hg_batch hg_batch;
+
+/* Plans the batch (tile lists per kernel), allocates its device workspace
+ * (stream-ordered) and uploads the pair descriptors on `stream`.  The
+ * descriptors are copied: `pairs` may be reused after the call returns. */
+hg_status hg_batch_create(const hg_batch_pair* pairs, int n_pairs, int key_bytes, hg_stream_t stream,
+                          hg_batch** out);
+/* Launches the batch's kernels on `stream` (five launches and one memset,
+ * whatever the number of pairs).  Issues no allocation, no host copy and no
+ * synchronisation, so it can be captured into a CUDA graph and the graph
+ * replayed after the callers' input buffers are refilled. */
+hg_status hg_batch_run(const hg_batch* batch, hg_stream_t stream);
+/* Device bytes the batch holds (workspace and descriptors). */
+hg_status hg_batch_device_bytes(const hg_batch* batch, size_t* bytes);
+/* Frees the batch's device memory stream-ordered on `stream`. */
+void hg_batch_free(hg_batch* batch, hg_stream_t stream);
+/* create + run + free in one call. */
+hg_status hg_batch_build_intersect(const hg_batch_pair* pairs, int n_pairs, int key_bytes, hg_stream_t stream);
+
+/* ------------------------------------------------------------------------
  * Instrumentation (no counterpart in the reference, which prints host wall
  * times under HOST_PROFILE, src/MultiHashGraph.cu:55-57,431-615).
  * ---------------------------------------------------------------------- */

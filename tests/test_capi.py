@@ -65,6 +65,20 @@ def test_argument_checks_without_device(capi):
     assert L.hg_build_into(None, 10, 8, 10, None, None, None, None, 0, None) == -1
     assert L.hg_table_create(10, 8, 10, 0, None) == -1
     assert L.hg_zipf_cdf(None, 10, 1.1) == -1
+    # batched build + intersect: descriptors are checked before any device call
+    h = ctypes.c_void_p()
+    pairs = (capi.BatchPair * 1)()
+    assert L.hg_batch_create(pairs, 1, 3, None, ctypes.byref(h)) == -8
+    assert L.hg_batch_create(pairs, -1, 8, None, ctypes.byref(h)) == -1
+    assert L.hg_batch_create(pairs, 1, 8, None, None) == -1
+    pairs[0].n, pairs[0].n_buckets = 10, 0  # no buckets
+    assert L.hg_batch_create(pairs, 1, 8, None, ctypes.byref(h)) == -1
+    pairs[0].n_buckets, pairs[0].d_offsets, pairs[0].d_count = 16, 16, 16  # keys but no key buffer
+    assert L.hg_batch_create(pairs, 1, 8, None, ctypes.byref(h)) == -1
+    pairs[0].d_keys, pairs[0].d_keys_out, pairs[0].n = 16, 16, 1 << 32
+    assert L.hg_batch_create(pairs, 1, 8, None, ctypes.byref(h)) == -6
+    assert not h.value
+    assert L.hg_batch_run(None, None) == -1
 
 
 def test_workspace_plans(capi):

@@ -567,6 +567,105 @@ def run_batched(args, rank, world, local):
 
 
 # ---------------------------------------------------------------------------
+# serving: Poisson arrivals of build / intersect requests against resident tables
+# ---------------------------------------------------------------------------
+def serving_requests(n_req, rate, arena_keys, lo_log2=10, hi_log2=24, seed=5):
+    """Request list: Poisson arrivals at `rate`/s, 30% builds (table ids in
+    order) and 70% intersects against one of the last 128 built tables;
+    sizes 2^U(lo, hi).  A build takes the key-arena slice [off, off+n); an
+    intersect's queries are the slice starting half-way into its table's
+    slice (so about half of them, up to the table's size, match)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    t, reqs, built = 0.0, [], []
+    for k in range(n_req):
+        t += rng.exponential(1.0 / rate)
+        size = int(2 ** rng.uniform(lo_log2, hi_log2))
+        if k < 16 or rng.uniform() < 0.3:
+            off = int(rng.integers(0, arena_keys - size))
+            built.append((len(built), off, size))
+            reqs.append(("build", len(built) - 1, t, off, size))
+        else:
+            tid, toff, tn = built[int(rng.integers(max(0, len(built) - 128), len(built)))]
+            qoff = (toff + tn // 2) % max(1, arena_keys - size)
+            reqs.append(("intersect", tid, t, qoff, size))
+    return reqs
+
+
+def run_serving(args, rank, world, local):
+    import torch
+
+    import hashgraph_b200 as hg
+    from hashgraph_b200.serve import Request, Server, latency_summary, run_open_loop
+
+    dev = torch.device("cuda", local)
+    arena_keys = 1 << 27
+    arena = hg.gen_uniform(arena_keys, 8, 6, device=dev)
+    specs = serving_requests(args.requests, args.rate, arena_keys)
+
+    def make(spec):
+        kind, tid, t, off, size = spec
+        sl = arena[off:off + size]
+        if kind == "build":
+            return Request("build", tid, t, keys=sl, n_buckets=size)
+        return Request("intersect", tid, t, queries=sl, pair_cap=size)
+
+    server = Server(budget_bytes=120 << 30, max_tables=512, n_streams=args.streams, max_keys=1 << 24, device=dev)
+    # warm-up: one build and one intersect of each size decade, outside the timed run
+    for lg in range(10, 25, 2):
+        w = [Request("build", -1, 0.0, keys=arena[: 1 << lg], n_buckets=1 << lg),
+             Request("intersect", -1, 0.0, queries=arena[: 1 << lg], pair_cap=1 << lg)]
+        for r in w:
+            server.submit(r)
+        server.poll(block=True)
+    torch.cuda.synchronize(dev)
+    reqs = [make(sp) for sp in specs]
+    clocks = ClockSampler(local)
+    launches0 = hg.launch_count()
+    clocks.start()
+    makespan = run_open_loop(server, reqs)
+    clk = clocks.stop()
+    launches = hg.launch_count() - launches0
+    done = [r for r in reqs if r.latency_s is not None]
+    keys_total = sum((r.keys.numel() if r.kind == "build" else r.queries.numel()) for r in reqs)
+    value = keys_total / makespan
+    by_kind = {k: latency_summary([r for r in done if r.kind == k]) for k in ("build", "intersect")}
+    missed = sum(1 for r in reqs if r.missed)
+
+    # each intersect's count against a serial run of the same request list
+    serial = Server(budget_bytes=1 << 50, max_tables=1 << 30, n_streams=1, max_keys=1 << 24, device=dev)
+    mismatches, checked = 0, 0
+    for sp, r in zip(specs, reqs):
+        q = make(sp)
+        serial.submit(q)
+        serial.poll(block=True)
+        if q.kind == "intersect" and not r.missed:
+            checked += 1
+            mismatches += int(q.count != r.count)
+    if mismatches:
+        raise RuntimeError(f"{mismatches} of {checked} served intersects differ from the serial run")
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": 1,
+        "ms_per_step": makespan * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64", "data": "synthetic (seeded splitmix64 key arena on the device; requests take slices)",
+        "config": {"workload": f"serving: {args.requests} requests, Poisson arrivals at {args.rate}/s, 30% build / "
+                               f"70% intersect, sizes 2^U(10,24) u64, <= 512 resident tables, 120 GB budget, "
+                               f"LRU, {args.streams} streams",
+                   "requests": args.requests, "rate_per_s": args.rate, "keys_total": keys_total,
+                   "offered_keys_per_s": keys_total / (specs[-1][2] - specs[0][2]) if len(specs) > 1 else None,
+                   "parallelism": "single GPU"},
+        "latency": by_kind, "latency_all": latency_summary(done), "missed_intersects": missed,
+        "evictions": server.store.evictions, "serial_check": {"intersects_checked": checked, "mismatches": 0},
+        "clocks": clk, "e2e": None, "gpu_launches": launches, "cpu_baseline": None,
+        "note": "value = keys of all requests / makespan (first arrival to last completion); latency = "
+                "arrival to device completion of the request's last kernel",
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # CPU baseline / reference arm
 # ---------------------------------------------------------------------------
 def cpu_run(workload, n_sample, repeats=3):
@@ -645,11 +744,54 @@ def run_reference_batched(args):
     print(json.dumps(out), flush=True)
 
 
+def run_reference_serving(args):
+    """The oracle's multithreaded build + probe over the serving request list,
+    serially (no arrivals), until about --cpu-sample keys."""
+    import numpy as np
+
+    import oracle
+    arena_keys = 1 << 27
+    specs = serving_requests(args.requests, args.rate, arena_keys)
+    cores = oracle.max_threads()
+    need = max(s[3] + s[4] for s in specs)
+    arena = oracle.gen_uniform(min(need, arena_keys), 8, 6)
+    tables, total, t_sum, k = {}, 0, 0.0, 0
+    for kind, tid, _, off, size in specs:
+        sl = arena[off:off + size]
+        t0 = time.perf_counter()
+        if kind == "build":
+            tables[tid] = oracle.build(sl, size, False, threads=cores)
+        elif tid in tables:
+            o, kk, ii = tables[tid]
+            oracle.intersect(o, kk, ii, sl, pair_cap=size, threads=cores)
+        t_sum += time.perf_counter() - t0
+        total += size
+        k += 1
+        if total >= args.cpu_sample:
+            break
+    value = total / t_sum
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": 1, "steps": 1,
+        "warmup": 0, "ms_per_step": t_sum * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded splitmix64 key arena; same request list)",
+        "config": {"workload": f"serving: {args.requests} requests at {args.rate}/s, 30% build / 70% intersect, "
+                               "sizes 2^U(10,24) u64", "requests": args.requests},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"the first {k} requests ({total} keys), run back to back by the oracle's "
+                                   "multithreaded restatement (the reference has no CPU path)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
     if args.workload == "batched":
         run_reference_batched(args)
+        return
+    if args.workload == "serving":
+        run_reference_serving(args)
         return
     import oracle
     kb, n, bfn, kind, seed_a, seed_q, overlap, with_index = WORKLOADS[args.workload]
@@ -686,7 +828,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched"], default="large")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "serving"], default="large")
+    ap.add_argument("--requests", type=int, default=3000, help="requests of the serving workload")
+    ap.add_argument("--rate", type=float, default=20000.0, help="serving arrivals per second")
+    ap.add_argument("--streams", type=int, default=4, help="serving CUDA streams")
     ap.add_argument("--pairs", type=int, default=4096, help="pairs of the batched workload")
     ap.add_argument("--n", type=int, default=0, help="override keys per set (parity/profiling runs)")
     ap.add_argument("--cpu-sample", type=int, default=1 << 26)
@@ -705,6 +850,8 @@ def main():
     try:
         if args.workload == "batched":
             run_batched(args, rank, world, local)
+        elif args.workload == "serving":
+            run_serving(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

@@ -103,7 +103,7 @@ class Table:
     """
 
     def __init__(self, n_buckets: int, key_bytes: int, with_index: bool, capacity: int,
-                 device=None, path: int = PATH_AUTO):
+                 device=None, path: int = PATH_AUTO, workspace: bool = True):
         torch = _torch()
         self.device = torch.device(device or "cuda")
         self.n_buckets = int(n_buckets)
@@ -117,8 +117,9 @@ class Table:
         self.keys = torch.empty(max(self.capacity, 1), dtype=kdt, device=self.device)
         self.idx = (torch.empty(max(self.capacity, 1), dtype=torch.int32, device=self.device)
                     if with_index else None)
-        ws = build_workspace_bytes(self.capacity, key_bytes, n_buckets, with_index, path)
-        self.workspace = torch.empty(ws, dtype=torch.uint8, device=self.device)
+        # workspace=False: arrays only (the caller builds with its own workspace)
+        ws = build_workspace_bytes(self.capacity, key_bytes, n_buckets, with_index, path) if workspace else 0
+        self.workspace = torch.empty(max(ws, 1), dtype=torch.uint8, device=self.device)
 
     @classmethod
     def build(cls, keys, n_buckets: int, with_index: bool = False, path: int = PATH_AUTO,
@@ -142,6 +143,25 @@ class Table:
             _stream(stream)), "hg_build_into")
         self.n = n
         return self
+
+    def save(self, path: str, stream=None) -> None:
+        """Writes the built table to a table file (hg_table_save_arrays)."""
+        check(lib().hg_table_save_arrays(str(path).encode(), _ptr(self.offsets), _ptr(self.keys),
+                                         _ptr(self.idx), self.n, self.n_buckets, self.key_bytes,
+                                         _stream(stream)), "hg_table_save")
+
+    @classmethod
+    def load(cls, path: str, device=None, stream=None) -> "Table":
+        """Reads a table file onto `device` (hg_table_load_arrays)."""
+        n, nb = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        kb, wi = ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().hg_table_file_info(str(path).encode(), ctypes.byref(n), ctypes.byref(nb), ctypes.byref(kb),
+                                       ctypes.byref(wi)), "hg_table_file_info")
+        t = cls(nb.value, kb.value, bool(wi.value), n.value, device)
+        check(lib().hg_table_load_arrays(str(path).encode(), _ptr(t.offsets), _ptr(t.keys), _ptr(t.idx),
+                                         n.value, nb.value, kb.value, _stream(stream)), "hg_table_load")
+        t.n = n.value
+        return t
 
     def view_keys(self):
         return self.keys[: self.n]

@@ -87,6 +87,12 @@ SIGNATURES = {
     "hg_batch_device_bytes": (_i32, [_p, ctypes.POINTER(_sz)]),
     "hg_batch_free": (None, [_p, _p]),
     "hg_batch_build_intersect": (_i32, [ctypes.POINTER(BatchPair), _int, _int, _p]),
+    "hg_table_save": (_i32, [_p, ctypes.c_char_p, _p]),
+    "hg_table_load": (_i32, [ctypes.c_char_p, _pp, _p]),
+    "hg_table_save_arrays": (_i32, [ctypes.c_char_p, _p, _p, _p, _u64, _u64, _int, _p]),
+    "hg_table_file_info": (_i32, [ctypes.c_char_p, ctypes.POINTER(_u64), ctypes.POINTER(_u64),
+                                  ctypes.POINTER(_int), ctypes.POINTER(_int)]),
+    "hg_table_load_arrays": (_i32, [ctypes.c_char_p, _p, _p, _p, _u64, _u64, _int, _p]),
     "hg_profile_enable": (_i32, [_int]),
     "hg_profile_read": (_i32, [_int, ctypes.POINTER(_int), ctypes.POINTER(ctypes.c_char_p),
                                ctypes.POINTER(ctypes.c_float)]),

@@ -169,6 +169,18 @@ extern "C" hg_status hg_table_create(uint64_t capacity, int key_bytes, uint64_t 
 extern "C" hg_status hg_table_build(hg_table* t, const void* d_keys, uint64_t n, hg_stream_t stream) {
   if (!t || (n > 0 && !d_keys)) return HG_ERR_INVALID_ARGUMENT;
   if (n > t->capacity) return HG_ERR_TOO_LARGE;
+  if (!t->ws) {  // a loaded table gets its build workspace on its first rebuild
+    BuildPlan cap_plan;
+    hg_status cst = plan_build(t->capacity, t->key_bytes, t->n_buckets, t->with_index, &cap_plan);
+    if (cst != HG_OK) return cst;
+    const cudaError_t e = cudaMalloc(&t->ws, cap_plan.total);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      t->ws = nullptr;
+      return cuda_status(e);
+    }
+    t->ws_bytes = cap_plan.total;
+  }
   BuildPlan plan;
   hg_status st = plan_build(n, t->key_bytes, t->n_buckets, t->with_index, &plan);
   if (st != HG_OK) return st;

@@ -171,14 +171,27 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scatter(const BatchPairDe
     const uint64_t base = (t - P.ktile0) * BATCH_KTILE;
     const BucketMap bm = P.bm;
     uint32_t* cursor = P.offsets + 1;
+    // all the tile's cursor bumps are issued before any of their results is
+    // used, so the warp waits for one atomic round trip, not BATCH_KPT
+    KeyT k[BATCH_KPT];
+    uint32_t got[BATCH_KPT], rank[BATCH_KPT], leader[BATCH_KPT];
 #pragma unroll
     for (uint32_t u = 0; u < BATCH_KPT; u++) {
       const uint64_t i = base + u * BATCH_BLOCK + threadIdx.x;
       const bool ok = i < P.n;
-      const KeyT k = ok ? keys[i] : KeyT(0);
-      const uint32_t pos = warp_aggregated_inc(cursor, ok ? bm.of_key(k) : 0u, ok);
-      if (ok) {
-        out[pos] = k;
+      k[u] = ok ? keys[i] : KeyT(0);
+      const uint32_t b = ok ? bm.of_key(k[u]) : 0u;
+      const unsigned peers = __match_any_sync(FULL_MASK, ok ? uint64_t(b) : (1ull << 40));
+      leader[u] = __ffs(peers) - 1;
+      rank[u] = __popc(peers & lanemask_lt());
+      got[u] = (ok && lane_id() == leader[u]) ? atomicAdd(cursor + b, uint32_t(__popc(peers))) : 0u;
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < BATCH_KPT; u++) {
+      const uint64_t i = base + u * BATCH_BLOCK + threadIdx.x;
+      const uint32_t pos = __shfl_sync(FULL_MASK, got[u], leader[u]) + rank[u];
+      if (i < P.n) {
+        out[pos] = k[u];
         if (idx) idx[pos] = static_cast<uint32_t>(i);
       }
     }
@@ -222,9 +235,18 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_probe(const BatchPairDev*
         hi[j] = a_off[b + 1];
       }
     }
+    // every query's first bucket entry is loaded before any is compared, so
+    // the four dependent loads overlap; the rest of a bucket follows
+    KeyT first[BATCH_QPT];
 #pragma unroll
-    for (uint32_t j = 0; j < BATCH_QPT; j++)
-      for (uint32_t x = lo[j]; x < hi[j]; x++) c += (a_keys[x] == key[j]);
+    for (uint32_t j = 0; j < BATCH_QPT; j++) first[j] = lo[j] < hi[j] ? a_keys[lo[j]] : KeyT(0);
+#pragma unroll
+    for (uint32_t j = 0; j < BATCH_QPT; j++) {
+      if (lo[j] < hi[j]) {
+        c += (first[j] == key[j]);
+        for (uint32_t x = lo[j] + 1; x < hi[j]; x++) c += (a_keys[x] == key[j]);
+      }
+    }
     uint64_t tile_total;
     const uint64_t excl = block_exclusive_scan<BATCH_BLOCK>(c, red, &tile_total);
     if (threadIdx.x < 32) {

@@ -7,3 +7,4 @@
 #include "hg_api.cu"
 #include "hg_noalloc.cu"
 #include "hg_batch.cu"
+#include "hg_io.cu"

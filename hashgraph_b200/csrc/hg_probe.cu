@@ -61,9 +61,17 @@ __global__ void __launch_bounds__(PROBE_BLOCK)
         hi[j] = a_off[b + 1];
       }
     }
+    // first bucket entries of all the thread's queries are loaded together
+    KeyT first[PROBE_QPT];
 #pragma unroll
-    for (int j = 0; j < PROBE_QPT; j++)
-      for (uint32_t x = lo[j]; x < hi[j]; x++) c += (a_keys[x] == key[j]);
+    for (int j = 0; j < PROBE_QPT; j++) first[j] = lo[j] < hi[j] ? a_keys[lo[j]] : KeyT(0);
+#pragma unroll
+    for (int j = 0; j < PROBE_QPT; j++) {
+      if (lo[j] < hi[j]) {
+        c += (first[j] == key[j]);
+        for (uint32_t x = lo[j] + 1; x < hi[j]; x++) c += (a_keys[x] == key[j]);
+      }
+    }
     if constexpr (!EMIT) {
       counted += c;
       __syncthreads();

@@ -148,6 +148,31 @@ hg_status hg_table_device_bytes(const hg_table* table, size_t* bytes);
 void hg_table_free(hg_table* table);
 
 /* ------------------------------------------------------------------------
+ * Table files: a built table saved to disk and loaded back onto the current
+ * device (no counterpart in the reference, whose tables live in one process).
+ * Layout: a 64-byte header (magic "HGB2TBL", version 1, key width, index
+ * flag, hash id, n, n_buckets, FNV-1a 64 checksum of the payload), then
+ * offsets[n_buckets + 1] (uint32), keys[n], idx[n] (uint32, when indexed),
+ * little-endian.  Loading checks the magic, version, sizes against the file
+ * length, offsets[0] == 0, offsets[n_buckets] == n and the checksum.
+ * The copies run on `stream` through a pinned staging buffer; the calls
+ * return when the data is on disk / on the device.
+ * ---------------------------------------------------------------------- */
+hg_status hg_table_save(const hg_table* table, const char* path, hg_stream_t stream);
+hg_status hg_table_load(const char* path, hg_table** out, hg_stream_t stream);
+/* The same on caller-owned device arrays (d_idx NULL: no index saved). */
+hg_status hg_table_save_arrays(const char* path, const uint32_t* d_offsets, const void* d_keys,
+                               const uint32_t* d_idx, uint64_t n, uint64_t n_buckets, int key_bytes,
+                               hg_stream_t stream);
+/* Header of a table file (host only, no device work). */
+hg_status hg_table_file_info(const char* path, uint64_t* n, uint64_t* n_buckets, int* key_bytes,
+                             int* with_index);
+/* Loads into caller-owned arrays sized by hg_table_file_info; n, n_buckets
+ * and key_bytes must match the file's. */
+hg_status hg_table_load_arrays(const char* path, uint32_t* d_offsets, void* d_keys, uint32_t* d_idx,
+                               uint64_t n, uint64_t n_buckets, int key_bytes, hg_stream_t stream);
+
+/* ------------------------------------------------------------------------
  * Intersect.  Multiset join on equal keys, bucket by bucket, as
  * MultiHashGraph::intersect (src/MultiHashGraph.cu:631-740, simpleIntersect
  * include/MultiHashGraphDeviceOperators.cuh:513-543): every (a, q) with

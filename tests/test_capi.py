@@ -115,3 +115,26 @@ def test_zipf_cdf_matches_oracle(capi):
     ours = np.empty(U, dtype=np.uint64)
     assert L.hg_zipf_cdf(ours.ctypes.data_as(ctypes.c_void_p), U, 1.1) == 0
     np.testing.assert_array_equal(ours, oracle.zipf_cdf(U, 1.1))
+
+
+def test_table_file_header_checks_without_device(capi, tmp_path):
+    """hg_table_file_info reads only the header: no device needed."""
+    import struct
+    L = capi.lib()
+    n, nb = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    kb, wi = ctypes.c_int(0), ctypes.c_int(0)
+    args = (ctypes.byref(n), ctypes.byref(nb), ctypes.byref(kb), ctypes.byref(wi))
+    assert L.hg_table_file_info(str(tmp_path / "missing").encode(), *args) == -1
+    # a valid header for 3 u64 keys in 2 buckets with index: 64 + 12 + 24 + 12 bytes
+    hdr = b"HGB2TBL\0" + struct.pack("<4I3Q2Q", 1, 8, 1, 1, 3, 2, 0, 0, 0)
+    good = tmp_path / "good.hgt"
+    good.write_bytes(hdr + bytes(12 + 24 + 12))
+    assert L.hg_table_file_info(str(good).encode(), *args) == 0
+    assert (n.value, nb.value, kb.value, wi.value) == (3, 2, 8, 1)
+    (tmp_path / "short.hgt").write_bytes(hdr + bytes(10))
+    assert L.hg_table_file_info(str(tmp_path / "short.hgt").encode(), *args) == -1
+    (tmp_path / "magic.hgt").write_bytes(b"XGB2TBL\0" + hdr[8:] + bytes(48))
+    assert L.hg_table_file_info(str(tmp_path / "magic.hgt").encode(), *args) == -1
+    wide = b"HGB2TBL\0" + struct.pack("<4I3Q2Q", 1, 5, 1, 1, 3, 2, 0, 0, 0)
+    (tmp_path / "width.hgt").write_bytes(wide + bytes(48))
+    assert L.hg_table_file_info(str(tmp_path / "width.hgt").encode(), *args) == -8

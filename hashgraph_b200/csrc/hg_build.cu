@@ -795,7 +795,12 @@ hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_in
   // pass 3 double-buffers its partition's records (2 * rec per staged
   // record) and its bucket counters (8 bytes per bucket), and keeps a 4-byte
   // (bucket, rank) word per record
-  bool part_ok = plan_geometry(n, rec, n, 2 * rec + 4, 8, 0, n_buckets, false, &p.g);
+  size_t budget = FINE_SMEM_BUDGET;
+  if (const char* e = std::getenv("HG_BUILD_SMEM_KB")) {  // tuning override of the fine-build CTA's budget
+    const int kb = std::atoi(e);
+    if (kb >= 16 && kb <= 220) budget = size_t(kb) * 1024;
+  }
+  bool part_ok = plan_geometry(n, rec, n, 2 * rec + 4, 8, 0, n_buckets, false, &p.g, budget);
   // ranks within a bucket and local bucket numbers are packed in 16 bits
   if (part_ok && (p.g.fine_cap >= 65536 || p.g.fine_log2 > 16)) part_ok = false;
   if (part_ok) {
@@ -930,17 +935,27 @@ static hg_status run_partitioned(const BuildPlan& p, const KeyT* keys, uint32_t*
                                                    p.off_pkeys, p.off_pidx, p.off_fkeys, p.off_fidx, "build", s);
   if (st != HG_OK) return st;
   {
-    auto kern = k_fine_build<KeyT, WI, FINE_BLOCK>;
-    const int bps = blocks_per_sm(kern, FINE_BLOCK, g.smem3);
-    if (bps <= 0) return lib_fail(HG_ERR_CUDA, "fine-build kernel cannot be resident");
-    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(g.n_fine, uint64_t(device_sm_count()) * bps));
-    Phase ph(s, "fine_build");
-    count_launch();
-    kern<<<std::max(grid, 1u), FINE_BLOCK, g.smem3, s>>>(
-        reinterpret_cast<const KeyT*>(ws + p.off_fkeys),
-        WI ? reinterpret_cast<const uint32_t*>(ws + p.off_fidx) : nullptr,
-        reinterpret_cast<const uint32_t*>(ws + p.off_fcount), g.n_fine, g.fine_cap, g.fine_log2, bm, p.n_buckets,
-        offsets, keys_out, idx_out, flags);
+    hg_status lst = HG_OK;
+    auto go = [&](auto kern, unsigned block) {
+      const int bps = blocks_per_sm(kern, block, g.smem3);
+      if (bps <= 0) {
+        lst = lib_fail(HG_ERR_CUDA, "fine-build kernel cannot be resident");
+        return;
+      }
+      const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(g.n_fine, uint64_t(device_sm_count()) * bps));
+      Phase ph(s, "fine_build");
+      count_launch();
+      kern<<<std::max(grid, 1u), block, g.smem3, s>>>(
+          reinterpret_cast<const KeyT*>(ws + p.off_fkeys),
+          WI ? reinterpret_cast<const uint32_t*>(ws + p.off_fidx) : nullptr,
+          reinterpret_cast<const uint32_t*>(ws + p.off_fcount), g.n_fine, g.fine_cap, g.fine_log2, bm, p.n_buckets,
+          offsets, keys_out, idx_out, flags);
+    };
+    // tuning override: HG_BUILD_BLOCK=1024 runs the fine build with 1024 threads per CTA
+    const char* bb = std::getenv("HG_BUILD_BLOCK");
+    if (bb && std::atoi(bb) == 1024) go(k_fine_build<KeyT, WI, 1024>, 1024u);
+    else go(k_fine_build<KeyT, WI, FINE_BLOCK>, unsigned(FINE_BLOCK));
+    if (lst != HG_OK) return lst;
     HG_CUDA(cudaPeekAtLastError(), "fine-build launch");
   }
   // Fallback for an overflowed partition (heavy duplicates): the direct build,

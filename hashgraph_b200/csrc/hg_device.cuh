@@ -32,24 +32,27 @@ __host__ __device__ __forceinline__ uint32_t murmur3_low32(uint64_t key) {
   return h;
 }
 
-// Exact `h % d` for 32-bit h and a divisor fixed per launch: the published
-// direct-remainder method of Lemire, Kaser and Kurz ("Faster remainder by
-// direct computation", 2019).  magic = floor((2^64-1)/d) + 1; the remainder is
-// the high 64 bits of (magic*h mod 2^64) * d.  d >= 2^32 (one bucket per hash
-// value or more) means bucket = h.
+// Exact `h % d` for 32-bit h and a divisor fixed per launch.  A power-of-two
+// d (including d = 2^32, one bucket per hash value) is a mask.  Any other d
+// uses the published direct-remainder method of Lemire, Kaser and Kurz
+// ("Faster remainder by direct computation", 2019): magic =
+// floor((2^64-1)/d) + 1; the remainder is the high 64 bits of
+// (magic*h mod 2^64) * d.
 struct BucketMap {
   uint64_t magic;
   uint32_t d;
-  uint32_t wide;  // 1 when n_buckets >= 2^32
+  uint32_t mask;  // d - 1 when d is a power of two (0xffffffff for d = 2^32)
+  uint32_t pow2;  // 1 when d is a power of two
 
   static BucketMap make(uint64_t n_buckets) {
     BucketMap m;
+    m.pow2 = (n_buckets & (n_buckets - 1)) == 0 ? 1u : 0u;
     if (n_buckets >= (1ull << 32)) {
-      m.magic = 0; m.d = 0; m.wide = 1;
+      m.magic = 0; m.d = 0; m.mask = 0xffffffffu;
     } else {
       m.d = static_cast<uint32_t>(n_buckets);
       m.magic = UINT64_MAX / m.d + 1;
-      m.wide = 0;
+      m.mask = m.pow2 ? m.d - 1 : 0u;
     }
     return m;
   }
@@ -58,7 +61,7 @@ struct BucketMap {
   // low word cannot carry into bit 64, so the result is bits 32.. of
   // xh*d + hi32(xl*d).
   __host__ __device__ __forceinline__ uint32_t of_hash(uint32_t h) const {
-    if (wide) return h;
+    if (pow2) return h & mask;
     const uint64_t x = magic * h;
     const uint32_t xl = static_cast<uint32_t>(x), xh = static_cast<uint32_t>(x >> 32);
 #ifdef __CUDA_ARCH__

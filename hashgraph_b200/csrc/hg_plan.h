@@ -20,7 +20,7 @@ enum BuildPath : int { BUILD_DIRECT = 0, BUILD_PARTITIONED = 1 };
 
 constexpr size_t SMEM_BUDGET = 220 * 1024;  // dynamic shared memory per CTA (B200 opt-in max 227 KB)
 constexpr size_t FINE_SMEM_BUDGET = 100 * 1024;        // pass-3 build CTAs: two per SM (double-buffered)
-constexpr size_t FINE_PROBE_SMEM_BUDGET = 113 * 1024;  // pass-3 probe CTAs: two per SM (double-buffered)
+constexpr size_t FINE_PROBE_SMEM_BUDGET = 220 * 1024;  // pass-3 probe CTAs: one per SM (double-buffered)
 constexpr int PASS1_BLOCK = 512;
 constexpr int PASS1_KPT = 8;                     // pass-1 keys per thread per tile (registers)
 constexpr int PASS1_TILE = PASS1_BLOCK * PASS1_KPT;
@@ -29,6 +29,7 @@ constexpr uint64_t PASS1_MAX_PARTS = uint64_t(PASS1_APT) * PASS1_BLOCK;
 constexpr int SPLIT_BLOCK = 512;
 constexpr int SPLIT_TILE = 8 * SPLIT_BLOCK;     // k_split sorts a tile in registers: 8 records per thread
 constexpr int FINE_BLOCK = 512;
+constexpr int FINE_PROBE_BLOCK = 1024;          // one 1024-thread probe CTA per SM
 constexpr uint32_t SPLIT_LOG2_MAX = 8;          // pass 2 splits a coarse partition 256 ways (up to 1024)
 
 // Geometry of the partitioned (three-pass) paths, shared by build and probe:

@@ -13,6 +13,7 @@
 // The count-only form skips the look-back and adds tile sums atomically.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <type_traits>
 
 #include "hg_bulk.cuh"
@@ -408,6 +409,15 @@ size_t fine_probe_smem(uint32_t fine_log2, uint32_t capa, uint64_t capq, int key
   return 2 * fine_probe_buf_bytes(fine_log2, capa, capq, key_bytes, a_idx, emit);
 }
 
+// Shared-memory budget of one fine-probe CTA (tuning override HG_PROBE_SMEM_KB).
+static size_t probe_smem_budget() {
+  if (const char* e = std::getenv("HG_PROBE_SMEM_KB")) {
+    const int kb = std::atoi(e);
+    if (kb >= 16 && kb <= 220) return size_t(kb) * 1024;
+  }
+  return FINE_PROBE_SMEM_BUDGET;
+}
+
 hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, int key_bytes, bool emit,
                      ProbePlan* plan, int force_path) {
   if (key_bytes != 4 && key_bytes != 8) return HG_ERR_KEY_WIDTH;
@@ -426,7 +436,7 @@ hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, 
   // pass 3 double-buffers A's slice (offsets, keys, index) and the
   // partition's queries (keys, and positions when pairs are emitted)
   bool part_ok = plan_geometry(nq, q_rec, n_a, 2 * a_rec, 8, 2 * (key_bytes + (emit ? 4 : 0)), n_buckets, true,
-                               &p.g, FINE_PROBE_SMEM_BUDGET);
+                               &p.g, probe_smem_budget());
   if (part_ok) {
     p.g.smem1 = pass1_smem(p.g.n_parts, key_bytes);
     p.g.smem2 = split_smem(p.g.split_log2, key_bytes, true, p.g.n_parts);
@@ -506,8 +516,8 @@ static hg_status run_probe_partitioned(const ProbePlan& p, const uint32_t* a_off
   {
     const bool a_bulk = ((reinterpret_cast<uintptr_t>(a_off) | reinterpret_cast<uintptr_t>(a_keys) |
                           reinterpret_cast<uintptr_t>(a_idx)) & 15u) == 0;
-    auto go = [&](auto kern) {
-      const int bps = blocks_per_sm(kern, FINE_BLOCK, g.smem3);
+    auto go = [&](auto kern, unsigned block) {
+      const int bps = blocks_per_sm(kern, block, g.smem3);
       if (bps <= 0) {
         st = lib_fail(HG_ERR_CUDA, "fine-probe kernel cannot be resident");
         return;
@@ -515,15 +525,22 @@ static hg_status run_probe_partitioned(const ProbePlan& p, const uint32_t* a_off
       const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(g.n_fine, uint64_t(device_sm_count()) * bps));
       Phase ph(s, EMIT ? "fine_probe_emit" : "fine_probe_count");
       count_launch();
-      kern<<<std::max(grid, 1u), FINE_BLOCK, g.smem3, s>>>(
+      kern<<<std::max(grid, 1u), block, g.smem3, s>>>(
           reinterpret_cast<const KeyT*>(ws + p.off_fkeys), reinterpret_cast<const uint32_t*>(ws + p.off_fidx),
           reinterpret_cast<const uint32_t*>(ws + p.off_fcount), g.n_fine, g.fine_cap, g.fine_log2, bm, p.n_buckets,
           a_off, a_keys, a_idx, p.n_a, g.smem_cap, pairs, cap, d_count, static_cast<const uint32_t*>(flags), a_bulk);
       const cudaError_t e = cudaPeekAtLastError();
       if (e != cudaSuccess) st = cuda_fail(e, "fine-probe launch");
     };
-    if (a_idx) go(k_fine_probe<KeyT, true, EMIT, FINE_BLOCK>);
-    else go(k_fine_probe<KeyT, false, EMIT, FINE_BLOCK>);
+    // tuning override: HG_PROBE_BLOCK=512 runs the fine probe with 512 threads per CTA
+    const char* pb = std::getenv("HG_PROBE_BLOCK");
+    if (pb && std::atoi(pb) == 512) {
+      if (a_idx) go(k_fine_probe<KeyT, true, EMIT, 512>, 512u);
+      else go(k_fine_probe<KeyT, false, EMIT, 512>, 512u);
+    } else {
+      if (a_idx) go(k_fine_probe<KeyT, true, EMIT, FINE_PROBE_BLOCK>, unsigned(FINE_PROBE_BLOCK));
+      else go(k_fine_probe<KeyT, false, EMIT, FINE_PROBE_BLOCK>, unsigned(FINE_PROBE_BLOCK));
+    }
     if (st != HG_OK) return st;
   }
   // Fallback when a query partition overflowed (heavy duplicates): the direct

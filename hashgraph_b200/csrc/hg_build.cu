@@ -299,8 +299,20 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict_
         hist[j] = 0u;  // ready for the next tile
       }
     }
-    __syncthreads();
-    block_scan_segments<BLOCK>(lp, n_parts, 0u, 0u, wsum, [](uint32_t, uint32_t) {});
+    if (n_parts <= BLOCK) {
+      // one partition per thread: warp scans, then every warp adds the
+      // totals of the warps before it (two barriers in all)
+      const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+      const uint32_t inc = warp_inclusive_scan(hh[0]);
+      if (lane == 31) wsum[warp] = inc;
+      __syncthreads();
+      const uint32_t before = warp_sum((lane < (BLOCK / 32) && lane < warp) ? wsum[lane] : 0u);
+      if (threadIdx.x < n_parts) lp[threadIdx.x] = before + inc - hh[0];
+      __syncthreads();
+    } else {
+      __syncthreads();
+      block_scan_segments<BLOCK>(lp, n_parts, 0u, 0u, wsum, [](uint32_t, uint32_t) {});
+    }
 #pragma unroll
     for (int u = 0; u < KPT; u++) {
       const uint32_t r = u * BLOCK + threadIdx.x;
@@ -371,6 +383,7 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
   __shared__ uint64_t bar[2];
   __shared__ uint64_t s_next;
   __shared__ uint32_t s_next_cnt;
+  __shared__ uint32_t s_wsum[BLOCK / 32];
   const uint32_t coarse_log2 = fine_log2 + split_log2;
   const uint64_t vtiles = uint64_t(n_parts) * tiles_per_part;
   // first valid virtual tile at or after vt (stepping by the grid); vtiles if none
@@ -454,7 +467,16 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
       hh[a] = f < S ? hist[f] : 0u;
       g[a] = hh[a] ? atomicAdd(fcount + (q << split_log2) + f, hh[a]) : 0u;
     }
-    if (threadIdx.x < 32) {  // exclusive scan of S <= 1024 counts by one warp
+    if (S <= BLOCK) {
+      // one fine partition per thread: warp scans, then every warp adds the
+      // totals of the warps before it
+      const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+      const uint32_t inc = warp_inclusive_scan(hh[0]);
+      if (lane == 31) s_wsum[warp] = inc;
+      __syncthreads();
+      const uint32_t before = warp_sum((lane < (BLOCK / 32) && lane < warp) ? s_wsum[lane] : 0u);
+      if (threadIdx.x < S) lp[threadIdx.x] = before + inc - hh[0];
+    } else if (threadIdx.x < 32) {  // exclusive scan of S <= 1024 counts by one warp
       uint32_t run = 0;
       for (uint32_t j0 = 0; j0 < S; j0 += 32) {
         const uint32_t j = j0 + threadIdx.x;
@@ -587,21 +609,18 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ f
     }
     __syncthreads();
     if (nb == 4 * BLOCK) {
-      // four counters per thread: one block scan of the thread sums (two
-      // barriers; wsum is next written after the next partition's first)
+      // four counters per thread: warp scans of the thread sums; after one
+      // barrier every warp sums the totals of the warps before it itself
+      // (wsum is next written after the next partition's first barrier)
       const uint4 v = reinterpret_cast<const uint4*>(ctr)[threadIdx.x];
       const uint32_t sum = v.x + v.y + v.z + v.w;
       const uint32_t inc = warp_inclusive_scan(sum);
       if (lane == 31) wsum[warp] = inc;
       __syncthreads();
-      if (warp == 0) {
-        const uint32_t w = lane < NW ? wsum[lane] : 0u;
-        const uint32_t wi = warp_inclusive_scan(w);
-        if (lane < NW) wsum[lane] = wi - w;
-      }
-      __syncthreads();
+      const uint32_t wt = (lane < NW && lane < warp) ? wsum[lane] : 0u;
+      const uint32_t before = warp_sum(wt);
       uint4 o;
-      o.x = base + wsum[warp] + inc - sum;
+      o.x = base + before + inc - sum;
       o.y = o.x + v.x;
       o.z = o.y + v.y;
       o.w = o.z + v.z;

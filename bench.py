@@ -117,8 +117,8 @@ class ClockSampler:
 # capture summarised under profiles/).  Traffic grows with the keys
 # processed, so a full launch's traffic is this figure times its keys.
 MEASURED_TRAFFIC_PER_KEY = {
-    (8, False): {"multisplit": 14.5, "split": 14.4, "fine_build": 18.4,
-                 "probe_multisplit": 18.6, "probe_split": 22.3, "fine_probe_emit": 25.9},
+    (8, False): {"multisplit": 14.5, "split": 14.4, "fine_build": 18.5,
+                 "probe_multisplit": 18.3, "probe_split": 22.4, "fine_probe_emit": 25.8},
 }
 
 

@@ -774,11 +774,17 @@ bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size
   }
   const uint64_t W = 1ull << g.fine_log2;
   g.split_log2 = std::min<uint32_t>(s_max, ceil_log2_u64((n_buckets + W - 1) / W));
-  // pass 1 reserves at most PASS1_MAX_PARTS partitions per tile: split wider
-  // (up to 1024 ways) when the coarse partitions would be more
-  while (g.split_log2 < 10 && ((n_buckets + (1ull << (g.fine_log2 + g.split_log2)) - 1) >>
-                               (g.fine_log2 + g.split_log2)) > PASS1_MAX_PARTS)
+  // Pass 1 slows down sharply above PASS1_GOOD_PARTS coarse partitions (runs
+  // of a few keys per tile, more reservations): split wider, up to 1024 ways,
+  // until the coarse partitions are at most that many (measured on 2^30 u32
+  // keys + index: 512 partitions with a 1024-way split beat 2048 with 256-way
+  // by 14%).  PASS1_MAX_PARTS is the hard limit of the pass-1 kernel.
+  auto parts_at = [&](uint32_t sl) {
+    return (n_buckets + (1ull << (g.fine_log2 + sl)) - 1) >> (g.fine_log2 + sl);
+  };
+  while (g.split_log2 < 10 && !std::getenv("HG_SPLIT_LOG2") && parts_at(g.split_log2) > PASS1_GOOD_PARTS)
     g.split_log2++;
+  while (g.split_log2 < 10 && parts_at(g.split_log2) > PASS1_MAX_PARTS) g.split_log2++;
   g.coarse_log2 = g.fine_log2 + g.split_log2;
   g.n_parts = (n_buckets + (1ull << g.coarse_log2) - 1) >> g.coarse_log2;
   if (g.n_parts > PASS1_MAX_PARTS) return false;

@@ -26,6 +26,7 @@ constexpr int PASS1_KPT = 8;                     // pass-1 keys per thread per t
 constexpr int PASS1_TILE = PASS1_BLOCK * PASS1_KPT;
 constexpr int PASS1_APT = 4;                     // pass-1 partition reservations per thread and tile
 constexpr uint64_t PASS1_MAX_PARTS = uint64_t(PASS1_APT) * PASS1_BLOCK;
+constexpr uint64_t PASS1_GOOD_PARTS = PASS1_BLOCK;  // one partition per pass-1 thread
 constexpr int SPLIT_BLOCK = 512;
 constexpr int SPLIT_TILE = 8 * SPLIT_BLOCK;     // k_split sorts a tile in registers: 8 records per thread
 constexpr int FINE_BLOCK = 512;

@@ -209,53 +209,94 @@ __global__ void k_fill_u32(uint32_t* p, uint64_t count, uint32_t value, const ui
 
 constexpr int64_t EOFF_NONE = INT64_MIN;      // a dropped (overflowing) run
 
-template <typename KeyT, bool WITH_IDX, int BLOCK, int KPT, bool BULK>
-__global__ void __launch_bounds__(BLOCK, 2) k_multisplit(const KeyT* __restrict__ keys, const uint32_t* __restrict__ key_idx,
-                                                         uint64_t n, BucketMap bm, uint32_t coarse_log2, uint32_t n_parts,
-                                                         uint64_t cap, uint32_t* __restrict__ pcount,
-                                                         KeyT* __restrict__ pkeys, uint32_t* __restrict__ pidx,
-                                                         uint32_t* flags) {
+// One pass-1 tile: where its keys come from and where its partitions go.
+template <typename KeyT>
+struct SplitTile {
+  const KeyT* keys;         // source array; the tile is keys[base .. base + cnt)
+  const uint32_t* key_idx;  // optional positions of the source keys (else base + r)
+  uint64_t base;
+  uint32_t cnt;
+  BucketMap bm;
+  uint32_t shift;           // partition = bucket >> shift
+  uint32_t n_parts;
+  uint64_t cap;             // record slots per partition
+  uint32_t* pcount;         // per-partition counters
+  KeyT* pkeys;              // partition p's slots start at p * cap
+  uint32_t* pidx;
+};
+
+// Pass-1 tiles of one table: tile t holds keys [t*TILE, (t+1)*TILE).
+template <typename KeyT, uint32_t TILE>
+struct TableTiles {
+  const KeyT* keys;
+  const uint32_t* key_idx;
+  uint64_t n;
+  BucketMap bm;
+  uint32_t shift, n_parts;
+  uint64_t cap;
+  uint32_t* pcount;
+  KeyT* pkeys;
+  uint32_t* pidx;
+  __device__ __forceinline__ uint64_t ntiles() const { return (n + TILE - 1) / TILE; }
+  __device__ __forceinline__ SplitTile<KeyT> at(uint64_t t) const {
+    const uint64_t b = t * TILE;
+    const uint32_t c = b < n ? static_cast<uint32_t>(umin64(TILE, n - b)) : 0u;
+    return SplitTile<KeyT>{keys, key_idx, b, c, bm, shift, n_parts, cap, pcount, pkeys, pidx};
+  }
+};
+
+template <typename KeyT, bool WITH_IDX, int BLOCK, int KPT, bool BULK, typename Src>
+__global__ void __launch_bounds__(BLOCK, 2) k_multisplit(Src src, uint32_t max_parts, uint32_t* flags) {
   constexpr uint32_t TILE = BLOCK * KPT;
   constexpr uint32_t APT = PASS1_APT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   int64_t* eoff = reinterpret_cast<int64_t*>(smem_raw);  // element offset of sorted position 0, per partition
-  uint32_t* hist = reinterpret_cast<uint32_t*>(eoff + n_parts);
-  uint32_t* lp = hist + n_parts;
-  KeyT* raw = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(n_parts) * 16, 16));
+  uint32_t* hist = reinterpret_cast<uint32_t*>(eoff + max_parts);
+  uint32_t* lp = hist + max_parts;
+  KeyT* raw = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(max_parts) * 16, 16));
   uint32_t* si = reinterpret_cast<uint32_t*>(raw + 2 * TILE);
   uint16_t* sp = reinterpret_cast<uint16_t*>(si + TILE);
   __shared__ uint32_t wsum[BLOCK / 32 + 1];
   __shared__ uint64_t bar[2];
-  const uint64_t ntiles = (n + TILE - 1) / TILE;
-  auto tile_cnt = [&](uint64_t t) -> uint32_t {
-    const uint64_t b = t * TILE;
-    return b < n ? static_cast<uint32_t>(umin64(TILE, n - b)) : 0u;
-  };
+  const uint64_t ntiles = src.ntiles();
   // bulk part of a tile: whole 16-byte units; the ragged tail is read with plain loads
   auto bulk_bytes = [&](uint32_t cnt) -> uint32_t { return (cnt * uint32_t(sizeof(KeyT))) & ~15u; };
-  for (uint32_t j = threadIdx.x; j < n_parts; j += BLOCK) hist[j] = 0u;
+  for (uint32_t j = threadIdx.x; j < max_parts; j += BLOCK) hist[j] = 0u;
   if constexpr (BULK) {
     if (threadIdx.x == 0) {
       mbar_init(&bar[0], 1);
       mbar_init(&bar[1], 1);
       fence_mbar_init();
-      if (blockIdx.x < ntiles) bulk_load(raw, keys + uint64_t(blockIdx.x) * TILE, bulk_bytes(tile_cnt(blockIdx.x)), &bar[0]);
+      if (blockIdx.x < ntiles) {
+        const SplitTile<KeyT> v = src.at(blockIdx.x);
+        bulk_load(raw, v.keys + v.base, bulk_bytes(v.cnt), &bar[0]);
+      }
     }
   }
   __syncthreads();
   bool overflow = false;
   uint32_t it = 0;
   for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
-    const uint64_t base = t * TILE;
-    const uint32_t cnt = tile_cnt(t);
+    const SplitTile<KeyT> v = src.at(t);
+    const KeyT* keys = v.keys;
+    const uint32_t* key_idx = v.key_idx;
+    const uint64_t base = v.base;
+    const uint32_t cnt = v.cnt;
+    const BucketMap bm = v.bm;
+    const uint32_t coarse_log2 = v.shift;
+    const uint32_t n_parts = v.n_parts;
+    const uint64_t cap = v.cap;
+    uint32_t* pcount = v.pcount;
+    KeyT* pkeys = v.pkeys;
+    uint32_t* pidx = v.pidx;
     KeyT* cur = raw + (it & 1) * TILE;
     if constexpr (BULK) {
       // prefetch the next tile into the other buffer (its readers finished at
       // the __syncthreads that closed the previous iteration)
       if (threadIdx.x == 0 && t + gridDim.x < ntiles) {
         fence_proxy_async_smem();
-        const uint64_t nx = t + gridDim.x;
-        bulk_load(raw + ((it + 1) & 1) * TILE, keys + nx * TILE, bulk_bytes(tile_cnt(nx)), &bar[(it + 1) & 1]);
+        const SplitTile<KeyT> nv = src.at(t + gridDim.x);
+        bulk_load(raw + ((it + 1) & 1) * TILE, nv.keys + nv.base, bulk_bytes(nv.cnt), &bar[(it + 1) & 1]);
       }
     }
     KeyT k[KPT];
@@ -536,12 +577,52 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
 // write) and every record goes to offsets[bucket] + rank in the partition's
 // output slice (a few tens of KB, completed while resident in L2).
 // Dynamic smem: ctr[2][W] | sk[2][capf] | si[2][capf] | sr[capf]
-template <typename KeyT, bool WITH_IDX, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ fkeys, const uint32_t* __restrict__ fidx,
-                                                      const uint32_t* __restrict__ fstart, uint64_t n_fine, uint64_t capf,
-                                                      uint32_t fine_log2, BucketMap bm, uint64_t n_buckets,
-                                                      uint32_t* __restrict__ offsets, KeyT* __restrict__ keys_out,
-                                                      uint32_t* __restrict__ idx_out, const uint32_t* flags) {
+// One pass-3 partition of a build: its records and the table they go to.
+template <typename KeyT>
+struct FinePart {
+  const KeyT* rkeys;      // the partition's record slots
+  const uint32_t* ridx;
+  uint64_t b0;            // first bucket of the partition in its table
+  uint32_t nb;            // buckets of the partition
+  BucketMap bm;
+  uint32_t* offsets;      // the table's arrays
+  KeyT* keys_out;
+  uint32_t* idx_out;
+};
+
+// Pass-3 partitions of one table: partition f holds buckets [f*W, (f+1)*W);
+// its records sit at slot f*capf and its output starts at fstart[f].
+template <typename KeyT>
+struct TableFine {
+  const KeyT* fkeys;
+  const uint32_t* fidx;
+  const uint32_t* fstart;
+  uint64_t n_fine, capf;
+  uint32_t fine_log2;
+  BucketMap bm;
+  uint64_t n_buckets;
+  uint32_t* offsets;
+  KeyT* keys_out;
+  uint32_t* idx_out;
+  __device__ __forceinline__ uint64_t count() const {
+    return umin64(n_fine, (n_buckets + (1ull << fine_log2) - 1) >> fine_log2);  // partitions holding buckets
+  }
+  // (first, end) of partition f's records in the table's CSR order
+  __device__ __forceinline__ uint2 meta(uint64_t f) const { return make_uint2(fstart[f], fstart[f + 1]); }
+  __device__ __forceinline__ FinePart<KeyT> at(uint64_t f) const {
+    const uint64_t b0 = f << fine_log2;
+    const uint32_t nb = static_cast<uint32_t>(umin64(1ull << fine_log2, n_buckets - b0));
+    return FinePart<KeyT>{fkeys + f * capf, fidx + f * capf, b0, nb, bm, offsets, keys_out, idx_out};
+  }
+  // thread 0 of the CTA that takes partition f: the table's last offset
+  __device__ __forceinline__ void finish(uint64_t f) const {
+    if (f == 0) offsets[n_buckets] = fstart[n_fine];
+  }
+};
+
+template <typename KeyT, bool WITH_IDX, int BLOCK, typename Src>
+__global__ void __launch_bounds__(BLOCK) k_fine_build(Src src, uint64_t capf, uint32_t fine_log2,
+                                                      const uint32_t* flags) {
   if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
   constexpr int NW = BLOCK / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -553,24 +634,21 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ f
   __shared__ uint32_t wsum[NW + 1];
   __shared__ uint64_t bar[2];
   __shared__ uint32_t s_base[2], s_m[2];
-  if (blockIdx.x == 0 && threadIdx.x == 0) offsets[n_buckets] = fstart[n_fine];
-  const uint64_t n_live = umin64(n_fine, (n_buckets + W - 1) >> fine_log2);  // partitions holding buckets
-  const bool off_vec = (reinterpret_cast<uintptr_t>(offsets) & 15u) == 0;
+  const uint64_t n_live = src.count();
   const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
   // thread 0 loads a partition's start and size one iteration before it issues its copy
-  auto load_meta = [&](uint64_t f) -> uint2 {
-    return f < n_live ? make_uint2(fstart[f], fstart[f + 1]) : make_uint2(0u, 0u);
-  };
+  auto load_meta = [&](uint64_t f) -> uint2 { return f < n_live ? src.meta(f) : make_uint2(0u, 0u); };
   auto issue = [&](uint64_t f, uint32_t buf, uint2 mt) {
     const uint32_t m = mt.y - mt.x;
     s_base[buf] = mt.x;
     s_m[buf] = m;
+    const FinePart<KeyT> fp = src.at(f);
     const uint32_t bk = (m * uint32_t(sizeof(KeyT)) + 15u) & ~15u;  // stays inside the partition's slots
     const uint32_t bi = WITH_IDX ? ((m * 4u + 15u) & ~15u) : 0u;
     mbar_arrive_expect_tx(&bar[buf], bk + bi);
-    if (bk) bulk_g2s(sk + buf * capf, fkeys + f * capf, bk, &bar[buf]);
+    if (bk) bulk_g2s(sk + buf * capf, fp.rkeys, bk, &bar[buf]);
     if constexpr (WITH_IDX) {
-      if (bi) bulk_g2s(si + buf * capf, fidx + f * capf, bi, &bar[buf]);
+      if (bi) bulk_g2s(si + buf * capf, fp.ridx, bi, &bar[buf]);
     }
   };
   uint2 next_meta = make_uint2(0u, 0u);
@@ -585,9 +663,18 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ f
   uint32_t it = 0;
   for (uint64_t f = blockIdx.x; f < n_live; f += gridDim.x, it++) {
     const uint32_t buf = it & 1;
-    const uint64_t b0 = f << fine_log2;
-    const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
-    if (threadIdx.x == 0) mbar_wait(&bar[buf], (it >> 1) & 1);
+    const FinePart<KeyT> fp = src.at(f);
+    const uint64_t b0 = fp.b0;
+    const uint32_t nb = fp.nb;
+    const BucketMap bm = fp.bm;
+    uint32_t* offsets = fp.offsets;
+    KeyT* keys_out = fp.keys_out;
+    uint32_t* idx_out = fp.idx_out;
+    const bool off_vec = (reinterpret_cast<uintptr_t>(offsets) & 15u) == 0;
+    if (threadIdx.x == 0) {
+      src.finish(f);
+      mbar_wait(&bar[buf], (it >> 1) & 1);
+    }
     // the copy landed (published by this barrier) and every thread finished
     // the previous partition: its buffer and counters are free
     __syncthreads();
@@ -642,7 +729,9 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(const KeyT* __restrict__ f
       const uint32_t v = sr[r];
       const uint32_t pos = ctr[v >> 16] + (v & 0xffffu);
       keys_out[pos] = ck[r];
-      if constexpr (WITH_IDX) idx_out[pos] = ci[r];
+      if constexpr (WITH_IDX) {
+        if (idx_out) idx_out[pos] = ci[r];
+      }
     }
   }
 }
@@ -915,15 +1004,16 @@ static hg_status run_partition_passes(const PartGeometry& g, uint64_t n, const K
   KeyT* fkeys = reinterpret_cast<KeyT*>(ws + off_fkeys);
   uint32_t* fidx = WI ? reinterpret_cast<uint32_t*>(ws + off_fidx) : nullptr;
   if (n > 0) {
-    auto kern = k_multisplit<KeyT, WI, PASS1_BLOCK, PASS1_KPT, (V > 1)>;
+    auto kern = k_multisplit<KeyT, WI, PASS1_BLOCK, PASS1_KPT, (V > 1), TableTiles<KeyT, PASS1_TILE>>;
     const int bps = blocks_per_sm(kern, PASS1_BLOCK, g.smem1);
     if (bps <= 0) return lib_fail(HG_ERR_CUDA, "multisplit kernel cannot be resident");
     const uint64_t ntiles = (n + PASS1_TILE - 1) / PASS1_TILE;
     const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ntiles, uint64_t(device_sm_count()) * bps));
     Phase ph(s, who[0] == 'b' ? "multisplit" : "probe_multisplit");
     count_launch();
-    kern<<<grid, PASS1_BLOCK, g.smem1, s>>>(keys, key_idx, n, bm, g.coarse_log2, static_cast<uint32_t>(g.n_parts),
-                                          g.part_cap, pcount, pkeys, pidx, flags);
+    using Src = TableTiles<KeyT, PASS1_TILE>;
+    const Src src{keys, key_idx, n, bm, g.coarse_log2, static_cast<uint32_t>(g.n_parts), g.part_cap, pcount, pkeys, pidx};
+    kern<<<grid, PASS1_BLOCK, g.smem1, s>>>(src, static_cast<uint32_t>(g.n_parts), flags);
     HG_CUDA(cudaPeekAtLastError(), "multisplit launch");
   }
   launch_scan(pcount, g.n_parts, pstatus, ticket + 1, nullptr, pcount + g.n_parts, nullptr, s,
@@ -961,6 +1051,11 @@ static hg_status run_partitioned(const BuildPlan& p, const KeyT* keys, uint32_t*
   if (st != HG_OK) return st;
   {
     hg_status lst = HG_OK;
+    using Src = TableFine<KeyT>;
+    const Src src{reinterpret_cast<const KeyT*>(ws + p.off_fkeys),
+                  WI ? reinterpret_cast<const uint32_t*>(ws + p.off_fidx) : nullptr,
+                  reinterpret_cast<const uint32_t*>(ws + p.off_fcount), g.n_fine, g.fine_cap, g.fine_log2, bm,
+                  p.n_buckets, offsets, keys_out, idx_out};
     auto go = [&](auto kern, unsigned block) {
       const int bps = blocks_per_sm(kern, block, g.smem3);
       if (bps <= 0) {
@@ -970,16 +1065,12 @@ static hg_status run_partitioned(const BuildPlan& p, const KeyT* keys, uint32_t*
       const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(g.n_fine, uint64_t(device_sm_count()) * bps));
       Phase ph(s, "fine_build");
       count_launch();
-      kern<<<std::max(grid, 1u), block, g.smem3, s>>>(
-          reinterpret_cast<const KeyT*>(ws + p.off_fkeys),
-          WI ? reinterpret_cast<const uint32_t*>(ws + p.off_fidx) : nullptr,
-          reinterpret_cast<const uint32_t*>(ws + p.off_fcount), g.n_fine, g.fine_cap, g.fine_log2, bm, p.n_buckets,
-          offsets, keys_out, idx_out, flags);
+      kern<<<std::max(grid, 1u), block, g.smem3, s>>>(src, g.fine_cap, g.fine_log2, flags);
     };
     // tuning override: HG_BUILD_BLOCK=1024 runs the fine build with 1024 threads per CTA
     const char* bb = std::getenv("HG_BUILD_BLOCK");
-    if (bb && std::atoi(bb) == 1024) go(k_fine_build<KeyT, WI, 1024>, 1024u);
-    else go(k_fine_build<KeyT, WI, FINE_BLOCK>, unsigned(FINE_BLOCK));
+    if (bb && std::atoi(bb) == 1024) go(k_fine_build<KeyT, WI, 1024, Src>, 1024u);
+    else go(k_fine_build<KeyT, WI, FINE_BLOCK, Src>, unsigned(FINE_BLOCK));
     if (lst != HG_OK) return lst;
     HG_CUDA(cudaPeekAtLastError(), "fine-build launch");
   }

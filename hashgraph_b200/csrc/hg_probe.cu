@@ -143,13 +143,61 @@ __host__ __device__ inline size_t fine_probe_buf_bytes(uint32_t fine_log2, uint3
          (a_idx ? a16((size_t(capa) + 8) * 4) : 0) + a16(capq * key_bytes) + (emit ? a16(capq * 4) : 0);
 }
 
-template <typename KeyT, bool A_IDX, bool EMIT, int BLOCK>
+// One pass-3 partition of a probe: its query slots, the table it probes and
+// where its pairs go.
+template <typename KeyT>
+struct ProbePart {
+  const KeyT* qk;               // the partition's query slots (keys, positions)
+  const uint32_t* qi;
+  uint64_t b0;                  // first bucket of the partition in the table
+  uint32_t nb;                  // buckets of the partition
+  BucketMap bm;
+  uint64_t n_buckets;           // the table's
+  const uint32_t* a_off;        // the table (a_idx may be NULL)
+  const KeyT* a_keys;
+  const uint32_t* a_idx;
+  uint64_t n_a;
+  bool a_bulk;                  // the table's arrays are 16-byte aligned
+  uint32_t* pairs;
+  uint64_t pair_cap;
+  unsigned long long* d_count;
+};
+
+// Pass-3 partitions of one probe: partition f covers buckets [f*W, (f+1)*W)
+// and its queries sit at slot f*capq.
+template <typename KeyT>
+struct TableProbe {
+  static constexpr bool kOneTable = true;  // one count for the whole launch
+  const KeyT* qkeys;
+  const uint32_t* qidx;
+  const uint32_t* qstart;
+  uint64_t n_fine, capq;
+  uint32_t fine_log2;
+  BucketMap bm;
+  uint64_t n_buckets;
+  const uint32_t* a_off;
+  const KeyT* a_keys;
+  const uint32_t* a_idx;
+  uint64_t n_a;
+  bool a_bulk;
+  uint32_t* pairs;
+  uint64_t pair_cap;
+  unsigned long long* d_count;
+  __device__ __forceinline__ uint64_t count() const {
+    return umin64(n_fine, (n_buckets + (1ull << fine_log2) - 1) >> fine_log2);
+  }
+  __device__ __forceinline__ uint2 meta(uint64_t f) const { return make_uint2(qstart[f], qstart[f + 1]); }
+  __device__ __forceinline__ ProbePart<KeyT> at(uint64_t f) const {
+    const uint64_t b0 = f << fine_log2;
+    const uint32_t nb = static_cast<uint32_t>(umin64(1ull << fine_log2, n_buckets - b0));
+    return ProbePart<KeyT>{qkeys + f * capq, qidx + f * capq, b0, nb, bm, n_buckets, a_off, a_keys, a_idx, n_a,
+                           a_bulk, pairs, pair_cap, d_count};
+  }
+};
+
+template <typename KeyT, bool A_IDX, bool EMIT, int BLOCK, typename Src>
 __global__ void __launch_bounds__(BLOCK)
-    k_fine_probe(const KeyT* __restrict__ qkeys, const uint32_t* __restrict__ qidx, const uint32_t* __restrict__ qstart,
-                 uint64_t n_fine, uint64_t capq, uint32_t fine_log2, BucketMap bm, uint64_t n_buckets,
-                 const uint32_t* __restrict__ a_off, const KeyT* __restrict__ a_keys, const uint32_t* __restrict__ a_idx,
-                 uint64_t n_a, uint32_t capa, uint32_t* __restrict__ pairs, uint64_t pair_cap,
-                 unsigned long long* d_count, const uint32_t* flags, bool a_bulk) {
+    k_fine_probe(Src src, uint64_t capq, uint32_t fine_log2, uint32_t capa, const uint32_t* flags) {
   if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
   constexpr uint32_t EPK = 16 / sizeof(KeyT);  // keys per 16 bytes
   constexpr uint32_t QCH = FPROBE_QCH;
@@ -167,7 +215,7 @@ __global__ void __launch_bounds__(BLOCK)
   // partition's query count
   __shared__ uint32_t s_as[2], s_ae[2], s_al[2], s_ar[2], s_ial[2], s_iar[2], s_oplain[2], s_qm[2];
   __shared__ uint64_t red[NW + 1];
-  const uint64_t n_live = umin64(n_fine, (n_buckets + W - 1) >> fine_log2);
+  const uint64_t n_live = src.count();
   auto buf_off = [&](uint32_t b) { return reinterpret_cast<uint32_t*>(smem_raw + b * buf_bytes); };
   auto buf_keys = [&](uint32_t b) { return reinterpret_cast<KeyT*>(smem_raw + b * buf_bytes + off_bytes); };
   auto buf_idx = [&](uint32_t b) {
@@ -186,12 +234,12 @@ __global__ void __launch_bounds__(BLOCK)
   auto load_meta = [&](uint64_t f) -> Meta {
     Meta mt{0, 0, 0, 0};
     if (f < n_live) {
-      const uint64_t b0 = f << fine_log2;
-      const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
-      mt.as = a_off[b0];
-      mt.ae = a_off[b0 + nb];
-      mt.qb = qstart[f];
-      mt.qe = qstart[f + 1];
+      const ProbePart<KeyT> pp = src.at(f);
+      mt.as = pp.a_off[pp.b0];
+      mt.ae = pp.a_off[pp.b0 + pp.nb];
+      const uint2 q = src.meta(f);
+      mt.qb = q.x;
+      mt.qe = q.y;
     }
     return mt;
   };
@@ -201,12 +249,16 @@ __global__ void __launch_bounds__(BLOCK)
   // queries sit at the start of their 16-byte aligned slot (capq is a
   // multiple of 32), so their copies round up inside the slot.
   auto issue = [&](uint64_t f, uint32_t b, const Meta& mt) {
-    const uint64_t b0 = f << fine_log2;
-    const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
+    const ProbePart<KeyT> pp = src.at(f);
+    const uint64_t b0 = pp.b0, n_buckets = pp.n_buckets, n_a = pp.n_a;
+    const uint32_t nb = pp.nb;
+    const uint32_t* a_off = pp.a_off;
+    const KeyT* a_keys = pp.a_keys;
+    const uint32_t* a_idx = pp.a_idx;
     const uint32_t as = mt.as, ae = mt.ae;
     const bool fits = ae - as + 2 * EPK <= capa;
     uint32_t al = as, ar = as, ial = as, iar = as, ob = 0;
-    if (a_bulk) {
+    if (pp.a_bulk) {
       // offsets: entries [0, nb] of the partition, rounded up within B + 1
       const uint64_t oend = umin64((b0 + nb + 1 + 3) & ~3ull, (n_buckets + 1) & ~3ull);
       ob = oend > b0 ? static_cast<uint32_t>((oend - b0) * 4) : 0u;
@@ -214,7 +266,7 @@ __global__ void __launch_bounds__(BLOCK)
         al = as & ~(EPK - 1);
         ar = static_cast<uint32_t>(umin64((uint64_t(ae) + EPK - 1) & ~uint64_t(EPK - 1), n_a & ~uint64_t(EPK - 1)));
         if (ar < al) ar = al;
-        if (A_IDX) {
+        if (A_IDX && a_idx) {
           ial = as & ~3u;
           iar = static_cast<uint32_t>(umin64((uint64_t(ae) + 3) & ~3ull, n_a & ~3ull));
           if (iar < ial) iar = ial;
@@ -231,7 +283,7 @@ __global__ void __launch_bounds__(BLOCK)
     s_oplain[b] = ob / 4;
     s_qm[b] = m;
     const uint32_t kb = (ar - al) * uint32_t(sizeof(KeyT));
-    const uint32_t ib = A_IDX ? (iar - ial) * 4u : 0u;
+    const uint32_t ib = (A_IDX && a_idx) ? (iar - ial) * 4u : 0u;
     const uint32_t qkb = (m * uint32_t(sizeof(KeyT)) + 15u) & ~15u;
     const uint32_t qib = EMIT ? ((m * 4u + 15u) & ~15u) : 0u;
     mbar_arrive_expect_tx(&bar[b], ob + kb + ib + qkb + qib);
@@ -240,9 +292,9 @@ __global__ void __launch_bounds__(BLOCK)
     if constexpr (A_IDX) {
       if (ib) bulk_g2s(buf_idx(b), a_idx + ial, ib, &bar[b]);
     }
-    if (qkb) bulk_g2s(buf_q(b), qkeys + f * capq, qkb, &bar[b]);
+    if (qkb) bulk_g2s(buf_q(b), pp.qk, qkb, &bar[b]);
     if constexpr (EMIT) {
-      if (qib) bulk_g2s(buf_qi(b), qidx + f * capq, qib, &bar[b]);
+      if (qib) bulk_g2s(buf_qi(b), pp.qi, qib, &bar[b]);
     }
   };
   Meta next_meta{};  // thread 0: metadata of the partition after the one in flight
@@ -260,8 +312,16 @@ __global__ void __launch_bounds__(BLOCK)
   uint32_t it = 0;
   for (uint64_t f = blockIdx.x; f < n_live; f += gridDim.x, it++) {
     const uint32_t b = it & 1;
-    const uint64_t b0 = f << fine_log2;
-    const uint32_t nb = static_cast<uint32_t>(umin64(W, n_buckets - b0));
+    const ProbePart<KeyT> pp = src.at(f);
+    const uint64_t b0 = pp.b0;
+    const uint32_t nb = pp.nb;
+    const BucketMap bm = pp.bm;
+    const uint32_t* a_off = pp.a_off;
+    const KeyT* a_keys = pp.a_keys;
+    const uint32_t* a_idx = pp.a_idx;
+    uint32_t* pairs = pp.pairs;
+    const uint64_t pair_cap = pp.pair_cap;
+    unsigned long long* d_count = pp.d_count;
     if (threadIdx.x == 0) mbar_wait(&bar[b], (it >> 1) & 1);
     // the copy into buffer b landed (published by this barrier), and every
     // thread finished the previous partition, so buffer b ^ 1 is free
@@ -279,12 +339,12 @@ __global__ void __launch_bounds__(BLOCK)
     // whatever the bulk copies could not cover (the end of A's arrays, or
     // unaligned arrays): plain loads, rare, so the barrier is taken only then
     const uint32_t oplain = s_oplain[b];
-    const bool plain = oplain <= nb || (!spill && (ar < ae || (A_IDX && s_iar[b] < ae)));
+    const bool plain = oplain <= nb || (!spill && (ar < ae || (A_IDX && a_idx && s_iar[b] < ae)));
     if (plain) {
       for (uint32_t j = oplain + threadIdx.x; j <= nb; j += BLOCK) soff[j] = a_off[b0 + j];
       if (!spill) {
         for (uint32_t x = ar + threadIdx.x; x < ae; x += BLOCK) sk[x - al] = a_keys[x];
-        if constexpr (A_IDX) {
+        if (A_IDX && a_idx) {
           const uint32_t ial = s_ial[b], iar = s_iar[b];
           for (uint32_t x = iar + threadIdx.x; x < ae; x += BLOCK) si[x - ial] = a_idx[x];
         }
@@ -306,6 +366,7 @@ __global__ void __launch_bounds__(BLOCK)
       };
       auto a_ref = [&](uint32_t x) -> uint32_t {
         if constexpr (A_IDX) {
+          if (!a_idx) return as + x;  // a table without index: CSR positions
           if constexpr (SPILL) return a_idx[as + x];
           else return si[x + ioff];
         } else {
@@ -348,7 +409,13 @@ __global__ void __launch_bounds__(BLOCK)
 #pragma unroll
         for (uint32_t j = 0; j < QCH; j++) mine += cnt[j];
         if constexpr (!EMIT) {
-          counted += mine;
+          if constexpr (Src::kOneTable) {
+            counted += mine;
+          } else {  // partitions of several tables: one count per partition
+            uint64_t tot;
+            block_exclusive_scan<BLOCK>(mine, red, &tot);
+            if (threadIdx.x == 0 && tot) atomicAdd(d_count, static_cast<unsigned long long>(tot));
+          }
         } else {
           // block scan of the thread totals; warp 0 reserves the round's range
           const uint64_t inc = warp_inclusive_scan(mine);
@@ -398,10 +465,10 @@ __global__ void __launch_bounds__(BLOCK)
     if (spill) probe_partition(std::true_type{});
     else probe_partition(std::false_type{});
   }
-  if constexpr (!EMIT) {
+  if constexpr (!EMIT && Src::kOneTable) {
     uint64_t tot;
     block_exclusive_scan<BLOCK>(counted, red, &tot);
-    if (threadIdx.x == 0 && tot) atomicAdd(d_count, static_cast<unsigned long long>(tot));
+    if (threadIdx.x == 0 && tot) atomicAdd(src.d_count, static_cast<unsigned long long>(tot));
   }
 }
 
@@ -516,6 +583,10 @@ static hg_status run_probe_partitioned(const ProbePlan& p, const uint32_t* a_off
   {
     const bool a_bulk = ((reinterpret_cast<uintptr_t>(a_off) | reinterpret_cast<uintptr_t>(a_keys) |
                           reinterpret_cast<uintptr_t>(a_idx)) & 15u) == 0;
+    using Src = TableProbe<KeyT>;
+    const Src src{reinterpret_cast<const KeyT*>(ws + p.off_fkeys), reinterpret_cast<const uint32_t*>(ws + p.off_fidx),
+                  reinterpret_cast<const uint32_t*>(ws + p.off_fcount), g.n_fine, g.fine_cap, g.fine_log2, bm,
+                  p.n_buckets, a_off, a_keys, a_idx, p.n_a, a_bulk, pairs, cap, d_count};
     auto go = [&](auto kern, unsigned block) {
       const int bps = blocks_per_sm(kern, block, g.smem3);
       if (bps <= 0) {
@@ -525,21 +596,19 @@ static hg_status run_probe_partitioned(const ProbePlan& p, const uint32_t* a_off
       const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(g.n_fine, uint64_t(device_sm_count()) * bps));
       Phase ph(s, EMIT ? "fine_probe_emit" : "fine_probe_count");
       count_launch();
-      kern<<<std::max(grid, 1u), block, g.smem3, s>>>(
-          reinterpret_cast<const KeyT*>(ws + p.off_fkeys), reinterpret_cast<const uint32_t*>(ws + p.off_fidx),
-          reinterpret_cast<const uint32_t*>(ws + p.off_fcount), g.n_fine, g.fine_cap, g.fine_log2, bm, p.n_buckets,
-          a_off, a_keys, a_idx, p.n_a, g.smem_cap, pairs, cap, d_count, static_cast<const uint32_t*>(flags), a_bulk);
+      kern<<<std::max(grid, 1u), block, g.smem3, s>>>(src, g.fine_cap, g.fine_log2, g.smem_cap,
+                                                      static_cast<const uint32_t*>(flags));
       const cudaError_t e = cudaPeekAtLastError();
       if (e != cudaSuccess) st = cuda_fail(e, "fine-probe launch");
     };
     // tuning override: HG_PROBE_BLOCK=512 runs the fine probe with 512 threads per CTA
     const char* pb = std::getenv("HG_PROBE_BLOCK");
     if (pb && std::atoi(pb) == 512) {
-      if (a_idx) go(k_fine_probe<KeyT, true, EMIT, 512>, 512u);
-      else go(k_fine_probe<KeyT, false, EMIT, 512>, 512u);
+      if (a_idx) go(k_fine_probe<KeyT, true, EMIT, 512, Src>, 512u);
+      else go(k_fine_probe<KeyT, false, EMIT, 512, Src>, 512u);
     } else {
-      if (a_idx) go(k_fine_probe<KeyT, true, EMIT, FINE_PROBE_BLOCK>, unsigned(FINE_PROBE_BLOCK));
-      else go(k_fine_probe<KeyT, false, EMIT, FINE_PROBE_BLOCK>, unsigned(FINE_PROBE_BLOCK));
+      if (a_idx) go(k_fine_probe<KeyT, true, EMIT, FINE_PROBE_BLOCK, Src>, unsigned(FINE_PROBE_BLOCK));
+      else go(k_fine_probe<KeyT, false, EMIT, FINE_PROBE_BLOCK, Src>, unsigned(FINE_PROBE_BLOCK));
     }
     if (st != HG_OK) return st;
   }

@@ -217,7 +217,7 @@ class Batch:
     ``offsets[i]``, ``table_keys[i]``, ``table_idx[i]`` (or None),
     ``pairs[i]`` ([pair_caps[i], 2] int32, or None when emit is False) and
     ``counts`` (int64, one exact match count per pair).  ``run()`` launches
-    the whole batch (a fixed sequence of five kernels, capturable into a CUDA
+    the whole batch (a fixed sequence of kernels, capturable into a CUDA
     graph); the input tensors must stay alive and may be refilled between
     runs.  All pairs share one key width.
     """

@@ -57,17 +57,35 @@ struct BatchPairDev {
   BucketMap bm;
   uint64_t ktile0, stile0, qtile0;  // first flattened tile of each kind
   uint64_t qtiles;                  // query tiles of this pair
+  // partitioned form (pb: the table, pq: the queries); the direct kernels
+  // take such a pair only if its partitioned pass overflowed
+  uint32_t pb, pq;
+  uint32_t nfb, nfq;                // fine partitions of the table / of the queries
+  uint64_t fb0, fq0;                // first fine partition in the batch's lists
+  uint64_t mt0, mq0;                // first pass-1 tile of the keys / of the queries
+  uint32_t a_bulk;                  // the table's arrays are 16-byte aligned
 };
+
+// Flags of a batch run: [0] a table's partitioned build overflowed, [1] a
+// partitioned probe overflowed; the direct kernels then redo those pairs.
+__device__ __forceinline__ bool batch_skip_build(const BatchPairDev& P, const uint32_t* flags) {
+  return P.pb && !(*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW);
+}
+__device__ __forceinline__ bool batch_skip_probe(const BatchPairDev& P, const uint32_t* flags) {
+  return P.pq && !(*reinterpret_cast<const volatile uint32_t*>(flags + 1) & FLAG_OVERFLOW);
+}
 
 // Every pair's offsets to zero (tile lt of a pair clears entries
 // [lt*STILE, ...) of offsets[1..B]; tile 0 also offsets[0]); every count to 0.
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_clear(const BatchPairDev* __restrict__ pairs, int n_pairs,
-                                                            const uint32_t* __restrict__ stile_pair, uint64_t n_stiles) {
+                                                            const uint32_t* __restrict__ stile_pair, uint64_t n_stiles,
+                                                            const uint32_t* flags) {
   for (uint64_t i = uint64_t(blockIdx.x) * BATCH_BLOCK + threadIdx.x; i < uint64_t(n_pairs);
        i += uint64_t(gridDim.x) * BATCH_BLOCK)
     *pairs[i].count = 0ull;
   for (uint64_t t = blockIdx.x; t < n_stiles; t += gridDim.x) {
     const BatchPairDev& P = pairs[stile_pair[t]];
+    if (batch_skip_build(P, flags)) continue;
     const uint64_t lt = t - P.stile0;
     const uint64_t j0 = lt * BATCH_STILE;
     const uint64_t j1 = umin64(j0 + BATCH_STILE, P.n_buckets);
@@ -79,9 +97,11 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_clear(const BatchPairDev*
 
 template <typename KeyT>
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_count(const BatchPairDev* __restrict__ pairs,
-                                                            const uint32_t* __restrict__ ktile_pair, uint64_t n_ktiles) {
+                                                            const uint32_t* __restrict__ ktile_pair, uint64_t n_ktiles,
+                                                            const uint32_t* flags) {
   for (uint64_t t = blockIdx.x; t < n_ktiles; t += gridDim.x) {
     const BatchPairDev& P = pairs[ktile_pair[t]];
+    if (batch_skip_build(P, flags)) continue;
     const KeyT* keys = static_cast<const KeyT*>(P.keys);
     const uint64_t base = (t - P.ktile0) * BATCH_KTILE;
     const BucketMap bm = P.bm;
@@ -103,7 +123,8 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_count(const BatchPairDev*
 template <int ITEMS>
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scan(const BatchPairDev* __restrict__ pairs,
                                                            const uint32_t* __restrict__ stile_pair, uint64_t n_stiles,
-                                                           uint64_t* __restrict__ status, unsigned* ticket) {
+                                                           uint64_t* __restrict__ status, unsigned* ticket,
+                                                           const uint32_t* flags) {
   constexpr int TILE = BATCH_BLOCK * ITEMS;
   static_assert(TILE == BATCH_STILE, "scan tile");
   __shared__ uint32_t s[TILE + TILE / 32];
@@ -115,6 +136,10 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scan(const BatchPairDev* 
     const uint64_t t = s_tile;
     if (t >= n_stiles) break;
     const BatchPairDev& P = pairs[stile_pair[t]];
+    if (batch_skip_build(P, flags)) {
+      __syncthreads();  // every thread read s_tile before thread 0 takes the next ticket
+      continue;
+    }
     const uint64_t lt = t - P.stile0;
     uint32_t* data = P.offsets + 1;
     const uint64_t count = P.n_buckets;
@@ -162,9 +187,10 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scan(const BatchPairDev* 
 template <typename KeyT>
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scatter(const BatchPairDev* __restrict__ pairs,
                                                               const uint32_t* __restrict__ ktile_pair,
-                                                              uint64_t n_ktiles) {
+                                                              uint64_t n_ktiles, const uint32_t* flags) {
   for (uint64_t t = blockIdx.x; t < n_ktiles; t += gridDim.x) {
     const BatchPairDev& P = pairs[ktile_pair[t]];
+    if (batch_skip_build(P, flags)) continue;
     const KeyT* keys = static_cast<const KeyT*>(P.keys);
     KeyT* out = static_cast<KeyT*>(P.keys_out);
     uint32_t* idx = P.idx_out;
@@ -204,7 +230,8 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scatter(const BatchPairDe
 template <typename KeyT>
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_probe(const BatchPairDev* __restrict__ pairs,
                                                             const uint32_t* __restrict__ qtile_pair, uint64_t n_qtiles,
-                                                            uint64_t* __restrict__ status, unsigned* ticket) {
+                                                            uint64_t* __restrict__ status, unsigned* ticket,
+                                                            const uint32_t* flags) {
   __shared__ uint64_t red[BATCH_BLOCK / 32 + 1];
   __shared__ uint64_t s_tile, s_prefix;
   while (true) {
@@ -213,6 +240,10 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_probe(const BatchPairDev*
     const uint64_t t = s_tile;
     if (t >= n_qtiles) break;
     const BatchPairDev& P = pairs[qtile_pair[t]];
+    if (batch_skip_probe(P, flags)) {
+      __syncthreads();  // every thread read s_tile before thread 0 takes the next ticket
+      continue;
+    }
     const uint64_t lt = t - P.qtile0;
     const KeyT* q = static_cast<const KeyT*>(P.query);
     const KeyT* a_keys = static_cast<const KeyT*>(P.keys_out);
@@ -277,13 +308,108 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_probe(const BatchPairDev*
   }
 }
 
+// ---------------------------------------------------------------------------
+// Partitioned form of large pairs: the pass-1 multisplit of each pair goes
+// straight to its fine partitions (at most PASS1_GOOD_PARTS of them: no split
+// pass), then the fine build and the fine probe of the single-table path run
+// over every pair's partitions at once.  These sources feed those kernels.
+// ---------------------------------------------------------------------------
+template <typename KeyT, bool QUERIES>
+struct BatchSplitTiles {
+  const BatchPairDev* pairs;
+  const uint32_t* tile_pair;
+  uint64_t n_tiles;
+  uint32_t shift;        // fine width (log2): partition = bucket >> shift
+  uint64_t cap;          // record slots per fine partition
+  uint32_t* fcount;
+  KeyT* fkeys;
+  uint32_t* fidx;
+  __device__ __forceinline__ uint64_t ntiles() const { return n_tiles; }
+  __device__ __forceinline__ SplitTile<KeyT> at(uint64_t t) const {
+    const BatchPairDev& P = pairs[tile_pair[t]];
+    const uint64_t base = (t - (QUERIES ? P.mq0 : P.mt0)) * PASS1_TILE;
+    const uint64_t n = QUERIES ? P.nq : P.n;
+    const uint32_t cnt = base < n ? static_cast<uint32_t>(umin64(PASS1_TILE, n - base)) : 0u;
+    const uint64_t f0 = QUERIES ? P.fq0 : P.fb0;
+    return SplitTile<KeyT>{static_cast<const KeyT*>(QUERIES ? P.query : P.keys), nullptr, base, cnt, P.bm, shift,
+                           QUERIES ? P.nfq : P.nfb, cap, fcount + f0, fkeys + f0 * cap,
+                           fidx ? fidx + f0 * cap : nullptr};
+  }
+};
+
+template <typename KeyT>
+struct BatchFine {
+  const BatchPairDev* pairs;
+  const uint32_t* part_pair;
+  uint64_t n_parts;
+  const KeyT* fkeys;
+  const uint32_t* fidx;
+  uint64_t capf;
+  const uint32_t* fstart;  // scanned counts over every pair's partitions
+  uint32_t fine_log2;
+  __device__ __forceinline__ uint64_t count() const { return n_parts; }
+  __device__ __forceinline__ uint2 meta(uint64_t f) const {
+    const uint32_t s0 = fstart[pairs[part_pair[f]].fb0];  // the pair's first record
+    return make_uint2(fstart[f] - s0, fstart[f + 1] - s0);
+  }
+  __device__ __forceinline__ FinePart<KeyT> at(uint64_t f) const {
+    const BatchPairDev& P = pairs[part_pair[f]];
+    const uint64_t b0 = (f - P.fb0) << fine_log2;
+    const uint32_t nb = static_cast<uint32_t>(umin64(1ull << fine_log2, P.n_buckets - b0));
+    return FinePart<KeyT>{fkeys + f * capf, fidx ? fidx + f * capf : nullptr, b0, nb, P.bm, P.offsets,
+                          static_cast<KeyT*>(P.keys_out), P.idx_out};
+  }
+  __device__ __forceinline__ void finish(uint64_t f) const {
+    const BatchPairDev& P = pairs[part_pair[f]];
+    if (f == P.fb0) P.offsets[P.n_buckets] = static_cast<uint32_t>(P.n);
+  }
+};
+
+template <typename KeyT>
+struct BatchProbe {
+  static constexpr bool kOneTable = false;  // one count per pair
+  const BatchPairDev* pairs;
+  const uint32_t* part_pair;
+  uint64_t n_parts;
+  const KeyT* qkeys;
+  const uint32_t* qidx;
+  uint64_t capq;
+  const uint32_t* qstart;
+  uint32_t fine_log2;
+  __device__ __forceinline__ uint64_t count() const { return n_parts; }
+  __device__ __forceinline__ uint2 meta(uint64_t f) const { return make_uint2(qstart[f], qstart[f + 1]); }
+  __device__ __forceinline__ ProbePart<KeyT> at(uint64_t f) const {
+    const BatchPairDev& P = pairs[part_pair[f]];
+    const uint64_t b0 = (f - P.fq0) << fine_log2;
+    const uint32_t nb = static_cast<uint32_t>(umin64(1ull << fine_log2, P.n_buckets - b0));
+    return ProbePart<KeyT>{qkeys + f * capq, qidx + f * capq, b0, nb, P.bm, P.n_buckets, P.offsets,
+                           static_cast<const KeyT*>(P.keys_out), P.idx_out, P.n, P.a_bulk != 0, P.pairs,
+                           P.pair_cap, P.count};
+  }
+};
+
 // Host-side batch: the plan, the device workspace and the descriptors.
+constexpr uint64_t BATCH_PART_MIN = 1ull << 14;  // keys (queries) from which a pair is partitioned
+constexpr uint32_t BATCH_FINE_LOG2 = 11;          // fine width of the partitioned build
+
 struct BatchPlan {
   int n_pairs = 0;
   int key_bytes = 8;
   uint64_t n_ktiles = 0, n_stiles = 0, n_qtiles = 0;
+  // partitioned form
+  uint64_t n_mt = 0, n_mq = 0;      // pass-1 tiles of the keys / of the queries
+  uint64_t n_fb = 0, n_fq = 0;      // fine partitions of the tables / of the queries
+  uint64_t capf = 0, capq = 0;      // record slots per fine partition
+  uint32_t capa = 0;                // table records a probe CTA stages
+  uint32_t lq = 12;                 // probe fine width (log2)
+  uint32_t max_pb = 1, max_pq = 1;  // most fine partitions of one pair
+  bool wi_b = false, ai_q = false, bulk_b = true, bulk_q = true;
+  size_t smem1b = 0, smem1q = 0, smem3b = 0, smem3q = 0;
   size_t off_pairs = 0, off_kmap = 0, off_smap = 0, off_qmap = 0;
-  size_t off_zero = 0, off_sstat = 0, off_qstat = 0, off_ticket = 0, total = 0;
+  size_t off_mtmap = 0, off_mqmap = 0, off_fbmap = 0, off_fqmap = 0;
+  size_t off_fbkeys = 0, off_fbidx = 0, off_fqkeys = 0, off_fqidx = 0;
+  size_t off_zero = 0, off_sstat = 0, off_qstat = 0, off_ticket = 0, off_flags = 0;
+  size_t off_fbcount = 0, off_fbstat = 0, off_fqcount = 0, off_fqstat = 0, total = 0;
 };
 
 }  // namespace hg
@@ -298,7 +424,9 @@ namespace hg {
 
 static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_bytes, BatchPlan* plan,
                             std::vector<BatchPairDev>* dev, std::vector<uint32_t>* kmap,
-                            std::vector<uint32_t>* smap, std::vector<uint32_t>* qmap) {
+                            std::vector<uint32_t>* smap, std::vector<uint32_t>* qmap,
+                            std::vector<uint32_t>* mtmap, std::vector<uint32_t>* mqmap,
+                            std::vector<uint32_t>* fbmap, std::vector<uint32_t>* fqmap) {
   if (key_bytes != 4 && key_bytes != 8) return HG_ERR_KEY_WIDTH;
   if (n_pairs < 0 || (n_pairs > 0 && !pairs)) return HG_ERR_INVALID_ARGUMENT;
   BatchPlan p;
@@ -349,15 +477,119 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
     std::fill(smap->begin() + d.stile0, smap->begin() + d.stile0 + st, uint32_t(i));
     std::fill(qmap->begin() + d.qtile0, qmap->begin() + d.qtile0 + d.qtiles, uint32_t(i));
   }
+  // Partitioned form: large pairs whose buckets make at most PASS1_GOOD_PARTS
+  // fine partitions and whose partitions fit a CTA's shared memory.
+  const uint64_t wb = 1ull << BATCH_FINE_LOG2;
+  auto aligned = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+  for (int i = 0; i < n_pairs; i++) {
+    BatchPairDev& d = (*dev)[i];
+    const double per_b = double(d.n) * double(wb) / double(d.n_buckets);
+    d.pb = (d.n >= BATCH_PART_MIN && (d.n_buckets + wb - 1) / wb <= PASS1_GOOD_PARTS && per_b <= 4096.0) ? 1u : 0u;
+    if (d.pb) {
+      p.capf = std::max(p.capf, slack_capacity(per_b, 64));
+      p.wi_b = p.wi_b || d.idx_out != nullptr;
+      p.bulk_b = p.bulk_b && aligned(d.keys);
+    }
+    d.a_bulk = (aligned(d.offsets) && aligned(d.keys_out) && (!d.idx_out || aligned(d.idx_out))) ? 1u : 0u;
+  }
+  const size_t rec_b = key_bytes + (p.wi_b ? 4 : 0);
+  p.smem3b = align_up(8 * wb, 16) + p.capf * (2 * rec_b + 4);
+  if (p.smem3b > SMEM_BUDGET)
+    for (auto& d : *dev) d.pb = 0;
+  // the probe's fine width: the widest whose staging fits one CTA
+  for (uint32_t lq = 12; lq >= 10; lq--) {
+    const uint64_t wq = 1ull << lq;
+    uint64_t capq = 0, capa = 0;
+    bool ai = false, any = false;
+    for (auto& d : *dev) {
+      const double per_q = double(d.nq) * double(wq) / double(d.n_buckets);
+      const double per_a = double(d.n) * double(wq) / double(d.n_buckets);
+      d.pq = (d.nq >= BATCH_PART_MIN && d.n > 0 && (d.n_buckets + wq - 1) / wq <= PASS1_GOOD_PARTS &&
+              per_q <= 8192.0 && per_a <= 8192.0) ? 1u : 0u;
+      if (!d.pq) continue;
+      any = true;
+      capq = std::max(capq, slack_capacity(per_q, 64));
+      capa = std::max(capa, slack_capacity(per_a, 64, 4.0));
+      ai = ai || d.idx_out != nullptr;
+    }
+    if (!any) break;
+    const size_t smem = fine_probe_smem(lq, static_cast<uint32_t>(capa), capq, key_bytes, ai, true);
+    if (smem <= SMEM_BUDGET) {
+      p.lq = lq;
+      p.capq = capq;
+      p.capa = static_cast<uint32_t>(capa);
+      p.ai_q = ai;
+      p.smem3q = smem;
+      break;
+    }
+    if (lq == 10)
+      for (auto& d : *dev) d.pq = 0;
+  }
+  if (!p.smem3q)
+    for (auto& d : *dev) d.pq = 0;
+  // pass-1 tiles and fine partitions of the partitioned pairs
+  for (int i = 0; i < n_pairs; i++) {
+    BatchPairDev& d = (*dev)[i];
+    if (d.pb) {
+      d.nfb = static_cast<uint32_t>((d.n_buckets + wb - 1) / wb);
+      d.fb0 = p.n_fb;
+      d.mt0 = p.n_mt;
+      p.n_fb += d.nfb;
+      p.n_mt += (d.n + PASS1_TILE - 1) / PASS1_TILE;
+      p.max_pb = std::max(p.max_pb, d.nfb);
+    }
+    if (d.pq) {
+      d.nfq = static_cast<uint32_t>((d.n_buckets + (1ull << p.lq) - 1) >> p.lq);
+      d.fq0 = p.n_fq;
+      d.mq0 = p.n_mq;
+      p.n_fq += d.nfq;
+      p.n_mq += (d.nq + PASS1_TILE - 1) / PASS1_TILE;
+      p.max_pq = std::max(p.max_pq, d.nfq);
+      p.bulk_q = p.bulk_q && aligned(d.query);
+    }
+  }
+  if (p.n_mt >= (1ull << 32) || p.n_mq >= (1ull << 32) || p.n_fb >= (1ull << 32) || p.n_fq >= (1ull << 32))
+    return lib_fail(HG_ERR_TOO_LARGE, "hg_batch_create: more than 2^32 partition tiles");
+  p.smem1b = pass1_smem(p.max_pb, key_bytes);
+  p.smem1q = pass1_smem(p.max_pq, key_bytes);
+  mtmap->resize(p.n_mt);
+  mqmap->resize(p.n_mq);
+  fbmap->resize(p.n_fb);
+  fqmap->resize(p.n_fq);
+  for (int i = 0; i < n_pairs; i++) {
+    const BatchPairDev& d = (*dev)[i];
+    if (d.pb) {
+      std::fill(mtmap->begin() + d.mt0, mtmap->begin() + d.mt0 + (d.n + PASS1_TILE - 1) / PASS1_TILE, uint32_t(i));
+      std::fill(fbmap->begin() + d.fb0, fbmap->begin() + d.fb0 + d.nfb, uint32_t(i));
+    }
+    if (d.pq) {
+      std::fill(mqmap->begin() + d.mq0, mqmap->begin() + d.mq0 + (d.nq + PASS1_TILE - 1) / PASS1_TILE, uint32_t(i));
+      std::fill(fqmap->begin() + d.fq0, fqmap->begin() + d.fq0 + d.nfq, uint32_t(i));
+    }
+  }
+  auto tiles_of = [](uint64_t n) { return std::max<uint64_t>((n + SCAN_TILE - 1) / SCAN_TILE, 1); };
   size_t off = 0;
-  p.off_pairs = off;  off = align_up(off + sizeof(BatchPairDev) * std::max(n_pairs, 1));
-  p.off_kmap = off;   off = align_up(off + 4 * std::max<uint64_t>(p.n_ktiles, 1));
-  p.off_smap = off;   off = align_up(off + 4 * std::max<uint64_t>(p.n_stiles, 1));
-  p.off_qmap = off;   off = align_up(off + 4 * std::max<uint64_t>(p.n_qtiles, 1));
-  p.off_zero = off;   // zeroed by every run: look-back status words and tickets
-  p.off_sstat = off;  off = align_up(off + 8 * std::max<uint64_t>(p.n_stiles, 1));
-  p.off_qstat = off;  off = align_up(off + 8 * std::max<uint64_t>(p.n_qtiles, 1));
-  p.off_ticket = off; off = align_up(off + 4 * sizeof(unsigned));
+  p.off_pairs = off;   off = align_up(off + sizeof(BatchPairDev) * std::max(n_pairs, 1));
+  p.off_kmap = off;    off = align_up(off + 4 * std::max<uint64_t>(p.n_ktiles, 1));
+  p.off_smap = off;    off = align_up(off + 4 * std::max<uint64_t>(p.n_stiles, 1));
+  p.off_qmap = off;    off = align_up(off + 4 * std::max<uint64_t>(p.n_qtiles, 1));
+  p.off_mtmap = off;   off = align_up(off + 4 * std::max<uint64_t>(p.n_mt, 1));
+  p.off_mqmap = off;   off = align_up(off + 4 * std::max<uint64_t>(p.n_mq, 1));
+  p.off_fbmap = off;   off = align_up(off + 4 * std::max<uint64_t>(p.n_fb, 1));
+  p.off_fqmap = off;   off = align_up(off + 4 * std::max<uint64_t>(p.n_fq, 1));
+  p.off_fbkeys = off;  off = align_up(off + p.n_fb * p.capf * key_bytes);
+  p.off_fbidx = off;   off = align_up(off + (p.wi_b ? p.n_fb * p.capf * 4 : 0));
+  p.off_fqkeys = off;  off = align_up(off + p.n_fq * p.capq * key_bytes);
+  p.off_fqidx = off;   off = align_up(off + p.n_fq * p.capq * 4);
+  p.off_zero = off;    // zeroed by every run: look-back state, tickets, flags, partition counters
+  p.off_sstat = off;   off = align_up(off + 8 * std::max<uint64_t>(p.n_stiles, 1));
+  p.off_qstat = off;   off = align_up(off + 8 * std::max<uint64_t>(p.n_qtiles, 1));
+  p.off_ticket = off;  off = align_up(off + 8 * sizeof(unsigned));
+  p.off_flags = off;   off = align_up(off + 2 * sizeof(uint32_t));
+  p.off_fbcount = off; off = align_up(off + 4 * (p.n_fb + 1));
+  p.off_fbstat = off;  off = align_up(off + 8 * tiles_of(p.n_fb));
+  p.off_fqcount = off; off = align_up(off + 4 * (p.n_fq + 1));
+  p.off_fqstat = off;  off = align_up(off + 8 * tiles_of(p.n_fq));
   p.total = off;
   *plan = p;
   return HG_OK;
@@ -372,35 +604,122 @@ static hg_status batch_launch(const BatchPlan& p, char* ws, cudaStream_t s) {
   uint64_t* sstat = reinterpret_cast<uint64_t*>(ws + p.off_sstat);
   uint64_t* qstat = reinterpret_cast<uint64_t*>(ws + p.off_qstat);
   unsigned* ticket = reinterpret_cast<unsigned*>(ws + p.off_ticket);
+  uint32_t* flags = reinterpret_cast<uint32_t*>(ws + p.off_flags);
   HG_CUDA(cudaMemsetAsync(ws + p.off_zero, 0, p.total - p.off_zero, s), "hg_batch_run: state memset");
   if (p.n_pairs == 0) return HG_OK;
   const uint64_t resident = uint64_t(device_sm_count()) * 8;  // 256-thread CTAs, 8 per SM
   auto grid_for = [&](uint64_t tiles) { return static_cast<unsigned>(std::max<uint64_t>(1, std::min(tiles, resident))); };
+  hg_status st = HG_OK;
+  // partitioned pass 1 (keys or queries of the partitioned pairs), then the
+  // scan of their fine-partition counts
+  auto split_pass = [&](auto src, bool with_idx, bool bulk, size_t smem, uint32_t max_parts, uint32_t* fl,
+                        uint32_t* fcount, uint64_t n_f, uint64_t* fstat, unsigned* tk, const char* name,
+                        const char* scan_name) {
+    using Src = decltype(src);
+    auto go = [&](auto kern) {
+      const int bps = blocks_per_sm(kern, PASS1_BLOCK, smem);
+      if (bps <= 0) {
+        st = lib_fail(HG_ERR_CUDA, "batch multisplit kernel cannot be resident");
+        return;
+      }
+      const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(src.n_tiles, uint64_t(device_sm_count()) * bps));
+      Phase ph(s, name);
+      count_launch();
+      kern<<<std::max(grid, 1u), PASS1_BLOCK, smem, s>>>(src, max_parts, fl);
+    };
+    if (with_idx) {
+      if (bulk) go(k_multisplit<KeyT, true, PASS1_BLOCK, PASS1_KPT, true, Src>);
+      else go(k_multisplit<KeyT, true, PASS1_BLOCK, PASS1_KPT, false, Src>);
+    } else {
+      if (bulk) go(k_multisplit<KeyT, false, PASS1_BLOCK, PASS1_KPT, true, Src>);
+      else go(k_multisplit<KeyT, false, PASS1_BLOCK, PASS1_KPT, false, Src>);
+    }
+    launch_scan(fcount, n_f, fstat, tk, nullptr, fcount + n_f, nullptr, s, scan_name);
+  };
+  if (p.n_mt) {
+    using Src = BatchSplitTiles<KeyT, false>;
+    const Src src{pairs, reinterpret_cast<const uint32_t*>(ws + p.off_mtmap), p.n_mt, BATCH_FINE_LOG2, p.capf,
+                  reinterpret_cast<uint32_t*>(ws + p.off_fbcount), reinterpret_cast<KeyT*>(ws + p.off_fbkeys),
+                  p.wi_b ? reinterpret_cast<uint32_t*>(ws + p.off_fbidx) : nullptr};
+    split_pass(src, p.wi_b, p.bulk_b, p.smem1b, p.max_pb, flags, reinterpret_cast<uint32_t*>(ws + p.off_fbcount),
+               p.n_fb, reinterpret_cast<uint64_t*>(ws + p.off_fbstat), ticket + 2, "batch_multisplit",
+               "batch_part_scan");
+    if (st != HG_OK) return st;
+    using FSrc = BatchFine<KeyT>;
+    const FSrc fsrc{pairs, reinterpret_cast<const uint32_t*>(ws + p.off_fbmap), p.n_fb,
+                    reinterpret_cast<const KeyT*>(ws + p.off_fbkeys),
+                    p.wi_b ? reinterpret_cast<const uint32_t*>(ws + p.off_fbidx) : nullptr, p.capf,
+                    reinterpret_cast<const uint32_t*>(ws + p.off_fbcount), BATCH_FINE_LOG2};
+    auto go = [&](auto kern) {
+      const int bps = blocks_per_sm(kern, FINE_BLOCK, p.smem3b);
+      if (bps <= 0) {
+        st = lib_fail(HG_ERR_CUDA, "batch fine-build kernel cannot be resident");
+        return;
+      }
+      const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(p.n_fb, uint64_t(device_sm_count()) * bps));
+      Phase ph(s, "batch_fine_build");
+      count_launch();
+      kern<<<std::max(grid, 1u), FINE_BLOCK, p.smem3b, s>>>(fsrc, p.capf, BATCH_FINE_LOG2, flags);
+    };
+    if (p.wi_b) go(k_fine_build<KeyT, true, FINE_BLOCK, FSrc>);
+    else go(k_fine_build<KeyT, false, FINE_BLOCK, FSrc>);
+    if (st != HG_OK) return st;
+  }
+  // direct form: every pair not partitioned, and partitioned ones if their
+  // pass overflowed (the kernels read the flags)
   {
     Phase ph(s, "batch_clear");
     count_launch();
     k_batch_clear<<<grid_for(std::max<uint64_t>(p.n_stiles, (p.n_pairs + BATCH_BLOCK - 1) / BATCH_BLOCK)), BATCH_BLOCK, 0, s>>>(
-        pairs, p.n_pairs, smap, p.n_stiles);
+        pairs, p.n_pairs, smap, p.n_stiles, flags);
   }
   if (p.n_ktiles) {
     Phase ph(s, "batch_count");
     count_launch();
-    k_batch_count<KeyT><<<grid_for(p.n_ktiles), BATCH_BLOCK, 0, s>>>(pairs, kmap, p.n_ktiles);
+    k_batch_count<KeyT><<<grid_for(p.n_ktiles), BATCH_BLOCK, 0, s>>>(pairs, kmap, p.n_ktiles, flags);
   }
   {
     Phase ph(s, "batch_scan");
     count_launch();
-    k_batch_scan<SCAN_ITEMS><<<grid_for(p.n_stiles), BATCH_BLOCK, 0, s>>>(pairs, smap, p.n_stiles, sstat, ticket);
+    k_batch_scan<SCAN_ITEMS><<<grid_for(p.n_stiles), BATCH_BLOCK, 0, s>>>(pairs, smap, p.n_stiles, sstat, ticket, flags);
   }
   if (p.n_ktiles) {
     Phase ph(s, "batch_scatter");
     count_launch();
-    k_batch_scatter<KeyT><<<grid_for(p.n_ktiles), BATCH_BLOCK, 0, s>>>(pairs, kmap, p.n_ktiles);
+    k_batch_scatter<KeyT><<<grid_for(p.n_ktiles), BATCH_BLOCK, 0, s>>>(pairs, kmap, p.n_ktiles, flags);
+  }
+  if (p.n_mq) {
+    using Src = BatchSplitTiles<KeyT, true>;
+    const Src src{pairs, reinterpret_cast<const uint32_t*>(ws + p.off_mqmap), p.n_mq, p.lq, p.capq,
+                  reinterpret_cast<uint32_t*>(ws + p.off_fqcount), reinterpret_cast<KeyT*>(ws + p.off_fqkeys),
+                  reinterpret_cast<uint32_t*>(ws + p.off_fqidx)};
+    split_pass(src, true, p.bulk_q, p.smem1q, p.max_pq, flags + 1, reinterpret_cast<uint32_t*>(ws + p.off_fqcount),
+               p.n_fq, reinterpret_cast<uint64_t*>(ws + p.off_fqstat), ticket + 3, "batch_probe_multisplit",
+               "batch_probe_part_scan");
+    if (st != HG_OK) return st;
+    using PSrc = BatchProbe<KeyT>;
+    const PSrc psrc{pairs, reinterpret_cast<const uint32_t*>(ws + p.off_fqmap), p.n_fq,
+                    reinterpret_cast<const KeyT*>(ws + p.off_fqkeys), reinterpret_cast<const uint32_t*>(ws + p.off_fqidx),
+                    p.capq, reinterpret_cast<const uint32_t*>(ws + p.off_fqcount), p.lq};
+    auto go = [&](auto kern) {
+      const int bps = blocks_per_sm(kern, FINE_PROBE_BLOCK, p.smem3q);
+      if (bps <= 0) {
+        st = lib_fail(HG_ERR_CUDA, "batch fine-probe kernel cannot be resident");
+        return;
+      }
+      const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(p.n_fq, uint64_t(device_sm_count()) * bps));
+      Phase ph(s, "batch_fine_probe");
+      count_launch();
+      kern<<<std::max(grid, 1u), FINE_PROBE_BLOCK, p.smem3q, s>>>(psrc, p.capq, p.lq, p.capa, flags + 1);
+    };
+    if (p.ai_q) go(k_fine_probe<KeyT, true, true, FINE_PROBE_BLOCK, PSrc>);
+    else go(k_fine_probe<KeyT, false, true, FINE_PROBE_BLOCK, PSrc>);
+    if (st != HG_OK) return st;
   }
   if (p.n_qtiles) {
     Phase ph(s, "batch_probe");
     count_launch();
-    k_batch_probe<KeyT><<<grid_for(p.n_qtiles), BATCH_BLOCK, 0, s>>>(pairs, qmap, p.n_qtiles, qstat, ticket + 1);
+    k_batch_probe<KeyT><<<grid_for(p.n_qtiles), BATCH_BLOCK, 0, s>>>(pairs, qmap, p.n_qtiles, qstat, ticket + 1, flags);
   }
   HG_CUDA(cudaPeekAtLastError(), "hg_batch_run: kernel launch");
   return HG_OK;
@@ -416,8 +735,9 @@ extern "C" hg_status hg_batch_create(const hg_batch_pair* pairs, int n_pairs, in
   *out = nullptr;
   BatchPlan plan;
   std::vector<BatchPairDev> dev;
-  std::vector<uint32_t> kmap, smap, qmap;
-  hg_status st = batch_plan(pairs, n_pairs, key_bytes, &plan, &dev, &kmap, &smap, &qmap);
+  std::vector<uint32_t> kmap, smap, qmap, mtmap, mqmap, fbmap, fqmap;
+  hg_status st = batch_plan(pairs, n_pairs, key_bytes, &plan, &dev, &kmap, &smap, &qmap, &mtmap, &mqmap, &fbmap,
+                            &fqmap);
   if (st != HG_OK) return st;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   hg_batch* b = new hg_batch();
@@ -438,6 +758,10 @@ extern "C" hg_status hg_batch_create(const hg_batch_pair* pairs, int n_pairs, in
       (e = up(plan.off_kmap, kmap.data(), kmap.size() * 4)) != cudaSuccess ||
       (e = up(plan.off_smap, smap.data(), smap.size() * 4)) != cudaSuccess ||
       (e = up(plan.off_qmap, qmap.data(), qmap.size() * 4)) != cudaSuccess ||
+      (e = up(plan.off_mtmap, mtmap.data(), mtmap.size() * 4)) != cudaSuccess ||
+      (e = up(plan.off_mqmap, mqmap.data(), mqmap.size() * 4)) != cudaSuccess ||
+      (e = up(plan.off_fbmap, fbmap.data(), fbmap.size() * 4)) != cudaSuccess ||
+      (e = up(plan.off_fqmap, fqmap.data(), fqmap.size() * 4)) != cudaSuccess ||
       (e = cudaStreamSynchronize(s)) != cudaSuccess) {  // the host vectors go out of scope
     cudaFreeAsync(b->d_mem, s);
     delete b;

@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(BLOCK)
             uint64_t base = 0;
             if (lane == 0 && tot) {
               base = atomicAdd(d_count, static_cast<unsigned long long>(tot));
-              if (base + tot > pair_cap) record_error(HG_ERR_PAIR_CAPACITY);
+              if (pairs && base + tot > pair_cap) record_error(HG_ERR_PAIR_CAPACITY);
             }
             base = __shfl_sync(FULL_MASK, base, 0);
             if (lane < NW) red[lane] = base + wi - w;

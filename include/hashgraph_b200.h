@@ -229,10 +229,12 @@ hg_status hg_intersect_tables(const hg_table* a, const hg_table* b, uint32_t* d_
  * launch sequence.  No counterpart in the reference, which builds and
  * intersects one MultiHashGraph at a time (test/MultiHashGraphTest.cu:288-338,
  * src/MultiHashGraph.cu:408-740); each pair's result equals the one
- * hg_build_into + hg_intersect_into (direct path) would give it: the same
- * offsets, the same buckets, the same count and the same pairs in the same
- * query order (keys inside one bucket in unspecified order, as for every
- * build).
+ * hg_build_into + hg_intersect_into would give it: the same offsets, the
+ * same buckets, the same count and the same pairs (keys inside one bucket in
+ * unspecified order, as for every build).  Pairs of 2^14 or more keys
+ * (queries) whose buckets form at most 512 partitions of 2048 (4096)
+ * buckets run in a partitioned form and emit their pairs grouped by
+ * partition; the others emit them in query order.
  *
  * For each pair i: build table i from d_keys[0..n) into d_offsets
  * [n_buckets + 1], d_keys_out [n] and, when d_idx_out is not NULL, d_idx_out
@@ -265,8 +267,8 @@ typedef struct hg_batch hg_batch;
  * descriptors are copied: `pairs` may be reused after the call returns. */
 hg_status hg_batch_create(const hg_batch_pair* pairs, int n_pairs, int key_bytes, hg_stream_t stream,
                           hg_batch** out);
-/* Launches the batch's kernels on `stream` (five launches and one memset,
- * whatever the number of pairs).  Issues no allocation, no host copy and no
+/* Launches the batch's kernels on `stream` (a fixed sequence of at most
+ * eleven launches and one memset, whatever the number of pairs).  Issues no allocation, no host copy and no
  * synchronisation, so it can be captured into a CUDA graph and the graph
  * replayed after the callers' input buffers are refilled. */
 hg_status hg_batch_run(const hg_batch* batch, hg_stream_t stream);

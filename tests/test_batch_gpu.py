@@ -1,10 +1,11 @@
 """GPU parity of the batched build + intersect (hg_batch_*) against the oracle
 and against one plain call per pair, and its replay from a captured CUDA graph.
 
-Each pair's result must equal the single-pair direct path's: offsets
-bit-exact, canonical buckets equal, the exact match count, and the pairs in
-the same query order (a_ref compared through the key it names when the table
-has no index, since positions inside a bucket are in atomic order)."""
+Each pair's result must equal the single-pair path's: offsets bit-exact,
+canonical buckets equal, the exact match count, and the same pairs (in the
+same query order for pairs the batch runs in the direct form; a_ref compared
+through the key it names when the table has no index, since positions inside
+a bucket are in atomic order)."""
 import numpy as np
 import pytest
 
@@ -81,12 +82,44 @@ def test_batch_matches_oracle(hg, kb):
     b.free()
 
 
+def test_batch_partitioned_matches_oracle(hg):
+    """Pairs of 2^14 .. 2^17 keys take the partitioned form (pass 1 straight
+    into fine partitions, then the fine build and fine probe); one with heavy
+    duplicates overflows its partitions and is redone by the direct kernels."""
+    import torch
+    rng = np.random.default_rng(77)
+    keys, queries, buckets, wi = [], [], [], []
+    for i in range(12):
+        n = int(2 ** rng.uniform(14, 17))
+        nq = int(2 ** rng.uniform(14, 17)) if i % 5 else 100  # a small query set stays direct
+        a = oracle.gen_uniform(n, 8, 300 + i)
+        if i == 4:  # all copies of a few keys: the partitions overflow
+            a = (a % np.uint64(37)).astype(np.uint64)
+        q = oracle.gen_overlap(nq, a, float(rng.uniform(0.1, 0.9)), 400 + i)
+        keys.append(a)
+        queries.append(q)
+        buckets.append(n if i % 3 else int(rng.integers(n // 2, 2 * n)))
+        wi.append(bool(i % 2))
+    caps = [max(_oracle_pair(keys[i], queries[i], buckets[i], wi[i])[3], 1) for i in range(len(keys))]
+    b = hg.Batch([from_np_u(a) for a in keys], [from_np_u(q) for q in queries], buckets, wi, caps).run()
+    torch.cuda.synchronize()
+    assert hg.device_error() == 0
+    for i in range(len(keys)):
+        _check_pair(hg, b, i, keys[i], queries[i], buckets[i], wi[i], 8)
+    # a second run over the same buffers gives the same results
+    b.run()
+    torch.cuda.synchronize()
+    for i in range(len(keys)):
+        _check_pair(hg, b, i, keys[i], queries[i], buckets[i], wi[i], 8)
+
+
 def test_batch_equals_plain_calls(hg):
-    """Same offsets and, with an index, the same pairs in the same order as
-    one direct-path build + intersect per pair."""
+    """Same offsets and, with an index, the same pairs as one direct-path
+    build + intersect per pair: in the same order for the pairs the batch
+    runs in the direct form, as the same set for the partitioned ones."""
     import torch
     kb = 8
-    keys, queries, buckets, _ = _make_batch_inputs(kb, 24, 99, max_log2=14, dups=False)
+    keys, queries, buckets, _ = _make_batch_inputs(kb, 24, 99, max_log2=16, dups=False)
     wi = [True] * len(keys)
     dk = [from_np_u(a) for a in keys]
     dq = [from_np_u(q) for q in queries]
@@ -98,7 +131,11 @@ def test_batch_equals_plain_calls(hg):
         np.testing.assert_array_equal(to_np_u(b.offsets[i], 4), to_np_u(t.offsets, 4))
         c = int(count.item())
         assert int(b.counts[i].item()) == c
-        np.testing.assert_array_equal(to_np_u(b.pairs[i][:c], 4), to_np_u(pairs[:c], 4))
+        if keys[i].size < (1 << 14) or queries[i].size < (1 << 14):
+            np.testing.assert_array_equal(to_np_u(b.pairs[i][:c], 4), to_np_u(pairs[:c], 4))
+        else:
+            np.testing.assert_array_equal(_sorted_pairs(to_np_u(b.pairs[i][:c], 4)),
+                                          _sorted_pairs(to_np_u(pairs[:c], 4)))
     assert hg.device_error() == 0
 
 

@@ -268,9 +268,10 @@ typedef struct hg_batch hg_batch;
 hg_status hg_batch_create(const hg_batch_pair* pairs, int n_pairs, int key_bytes, hg_stream_t stream,
                           hg_batch** out);
 /* Launches the batch's kernels on `stream` (a fixed sequence of at most
- * eleven launches and one memset, whatever the number of pairs).  Issues no allocation, no host copy and no
- * synchronisation, so it can be captured into a CUDA graph and the graph
- * replayed after the callers' input buffers are refilled. */
+ * eleven launches and one memset, whatever the number of pairs).  Issues no
+ * allocation, no host copy and no synchronisation, so it can be captured
+ * into a CUDA graph and the graph replayed after the callers' input buffers
+ * are refilled. */
 hg_status hg_batch_run(const hg_batch* batch, hg_stream_t stream);
 /* Device bytes the batch holds (workspace and descriptors). */
 hg_status hg_batch_device_bytes(const hg_batch* batch, size_t* bytes);

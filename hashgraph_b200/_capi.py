@@ -48,6 +48,12 @@ class BatchPair(ctypes.Structure):
     ]
 
 
+class ServerDone(ctypes.Structure):
+    """hg_server_done of include/hashgraph_b200.h."""
+    _fields_ = [("ticket", ctypes.c_uint64), ("kind", ctypes.c_int), ("missed", ctypes.c_int),
+                ("count", ctypes.c_ulonglong), ("latency_s", ctypes.c_double)]
+
+
 SIGNATURES = {
     "hg_status_str": (ctypes.c_char_p, [_i32]),
     "hg_version": (ctypes.c_char_p, []),
@@ -93,6 +99,15 @@ SIGNATURES = {
     "hg_table_file_info": (_i32, [ctypes.c_char_p, ctypes.POINTER(_u64), ctypes.POINTER(_u64),
                                   ctypes.POINTER(_int), ctypes.POINTER(_int)]),
     "hg_table_load_arrays": (_i32, [ctypes.c_char_p, _p, _p, _p, _u64, _u64, _int, _p]),
+    "hg_server_now": (ctypes.c_double, []),
+    "hg_server_create": (_i32, [_sz, _int, _int, _u64, _int, _pp]),
+    "hg_server_reserve": (_i32, [_p, _sz]),
+    "hg_server_build": (_i32, [_p, _u64, _p, _u64, _u64, _int, ctypes.c_double, ctypes.POINTER(_u64)]),
+    "hg_server_intersect": (_i32, [_p, _u64, _p, _u64, _p, _u64, ctypes.c_double, ctypes.POINTER(_u64)]),
+    "hg_server_poll": (_i32, [_p, _int, ctypes.POINTER(ServerDone), _int, ctypes.POINTER(_int)]),
+    "hg_server_stats": (_i32, [_p, ctypes.POINTER(_u64), ctypes.POINTER(_sz), ctypes.POINTER(_u64),
+                               ctypes.POINTER(_u64)]),
+    "hg_server_free": (None, [_p]),
     "hg_profile_enable": (_i32, [_int]),
     "hg_profile_read": (_i32, [_int, ctypes.POINTER(_int), ctypes.POINTER(ctypes.c_char_p),
                                ctypes.POINTER(ctypes.c_float)]),

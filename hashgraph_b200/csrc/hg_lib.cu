@@ -8,3 +8,4 @@
 #include "hg_noalloc.cu"
 #include "hg_batch.cu"
 #include "hg_io.cu"
+#include "hg_server.cu"

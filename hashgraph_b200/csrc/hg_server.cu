@@ -1,0 +1,404 @@
+// hg_server.cu -- a native serving engine: resident tables under a device
+// memory budget with least-recently-used eviction, build and intersect
+// requests spread over a pool of CUDA streams, and per-request latency.
+//
+// The reference has no serving component (its tables are built and
+// intersected once per process, test/MultiHashGraphTest.cu:288-338).  A
+// request costs one library call here, a few microseconds of host time, so
+// the host keeps up with tens of thousands of requests per second.
+//
+// Ordering between streams:
+//   * an intersect waits (cudaStreamWaitEvent) for its table's build;
+//   * a table's memory is freed stream-ordered on the stream that built it,
+//     after that stream has waited for everything already queued on every
+//     stream, so no kernel still reading an evicted table loses its memory.
+// Tables come from the server's own stream-ordered memory pool, whose
+// release threshold is the budget: memory freed by an eviction is reused by
+// the next build instead of being unmapped at the next synchronisation.
+// Latency = arrival time (the caller's CLOCK_MONOTONIC stamp) to the device
+// completion of the request's last operation, mapped onto the host clock by
+// one reference event recorded when the server starts.
+#include <time.h>
+
+#include <deque>
+#include <list>
+#include <unordered_map>
+#include <vector>
+
+#include "hg_device.cuh"
+#include "hg_plan.h"
+
+namespace hg {
+
+struct ServerTable {
+  uint64_t n = 0, n_buckets = 0;
+  bool with_index = false;
+  uint32_t* offsets = nullptr;
+  void* keys = nullptr;
+  uint32_t* idx = nullptr;
+  size_t bytes = 0;
+  int stream = 0;             // the stream that built it (its memory is freed there)
+  cudaEvent_t ready = nullptr;
+  std::list<uint64_t>::iterator lru;
+};
+
+struct ServerReq {
+  uint64_t ticket;
+  int kind;                   // 0 build, 1 intersect
+  int missed;
+  double arrival;
+  cudaEvent_t done;
+  uint32_t slot;              // count slot (intersect)
+};
+
+static double monotonic_s() {
+  timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return double(ts.tv_sec) + 1e-9 * double(ts.tv_nsec);
+}
+
+}  // namespace hg
+
+struct hg_server {
+  int device = 0, key_bytes = 8, max_tables = 0;
+  size_t budget = 0, bytes = 0, ws_bytes = 0;
+  uint64_t max_keys = 0, evictions = 0, next_ticket = 1;
+  std::vector<cudaStream_t> streams;
+  std::vector<void*> ws;
+  std::vector<uint32_t*> pair_buf;
+  std::vector<double> busy_until;
+  std::unordered_map<uint64_t, hg::ServerTable> tables;
+  std::list<uint64_t> lru;    // least recently used first
+  std::deque<hg::ServerReq> inflight;
+  unsigned long long* d_counts = nullptr;
+  unsigned long long* h_counts = nullptr;  // pinned
+  uint32_t n_slots = 0, next_slot = 0;
+  std::vector<uint8_t> slot_busy;
+  std::vector<cudaEvent_t> free_events;
+  cudaMemPool_t pool = nullptr;
+  cudaEvent_t ref = nullptr;
+  double ref_host = 0;
+};
+
+namespace hg {
+
+static cudaEvent_t take_event(hg_server* s) {
+  if (!s->free_events.empty()) {
+    cudaEvent_t e = s->free_events.back();
+    s->free_events.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Frees a table's memory stream-ordered after everything queued so far.
+static void release_table(hg_server* s, ServerTable& t) {
+  cudaStream_t home = s->streams[t.stream];
+  for (size_t i = 0; i < s->streams.size(); i++) {
+    if (int(i) == t.stream) continue;
+    cudaEvent_t e = take_event(s);
+    cudaEventRecord(e, s->streams[i]);
+    cudaStreamWaitEvent(home, e, 0);
+    s->free_events.push_back(e);  // reusable: the wait is already queued
+  }
+  if (t.offsets) cudaFreeAsync(t.offsets, home);
+  if (t.keys) cudaFreeAsync(t.keys, home);
+  if (t.idx) cudaFreeAsync(t.idx, home);
+  if (t.ready) cudaEventDestroy(t.ready);
+  s->bytes -= t.bytes;
+}
+
+static void evict(hg_server* s, uint64_t id) {
+  auto it = s->tables.find(id);
+  if (it == s->tables.end()) return;
+  release_table(s, it->second);
+  s->lru.erase(it->second.lru);
+  s->tables.erase(it);
+}
+
+static void make_room(hg_server* s, size_t need) {
+  while (!s->lru.empty() && (s->bytes + need > s->budget || s->tables.size() >= size_t(s->max_tables))) {
+    evict(s, s->lru.front());
+    s->evictions++;
+  }
+}
+
+static int pick_stream(hg_server* s, double est) {
+  const double now = monotonic_s();
+  int best = 0;
+  for (size_t i = 1; i < s->streams.size(); i++)
+    if (std::max(s->busy_until[i], now) < std::max(s->busy_until[best], now)) best = int(i);
+  s->busy_until[best] = std::max(s->busy_until[best], now) + est;
+  return best;
+}
+
+// Count slots: the next free one after the last handed out; a slot is busy
+// from its intersect's submission until poll has read its count.
+static hg_status reserve_slot(hg_server* s, uint32_t* slot) {
+  for (uint32_t k = 0; k < s->n_slots; k++) {
+    const uint32_t c = (s->next_slot + k) % s->n_slots;
+    if (!s->slot_busy[c]) {
+      s->slot_busy[c] = 1;
+      s->next_slot = (c + 1) % s->n_slots;
+      *slot = c;
+      return HG_OK;
+    }
+  }
+  return lib_fail(HG_ERR_TOO_LARGE, "hg_server: 65536 intersects in flight; poll before submitting more");
+}
+
+// The latency clock: event times are taken relative to `ref`, a float count
+// of milliseconds, so `ref` is moved forward whenever nothing is in flight
+// and it is more than a minute old (keeping the float's resolution in
+// microseconds).
+static cudaError_t rebase_clock(hg_server* s) {
+  cudaError_t e = cudaEventRecord(s->ref, s->streams[0]);
+  if (e == cudaSuccess) e = cudaEventSynchronize(s->ref);
+  if (e == cudaSuccess) s->ref_host = monotonic_s();
+  return e;
+}
+
+}  // namespace hg
+
+using namespace hg;
+
+extern "C" double hg_server_now(void) { return monotonic_s(); }
+
+extern "C" void hg_server_free(hg_server* s) {
+  if (!s) return;
+  for (auto& st : s->streams) cudaStreamSynchronize(st);
+  if (!s->streams.empty()) {
+    cudaStream_t st = s->streams[0];
+    for (auto& kv : s->tables) {
+      if (kv.second.offsets) cudaFreeAsync(kv.second.offsets, st);
+      if (kv.second.keys) cudaFreeAsync(kv.second.keys, st);
+      if (kv.second.idx) cudaFreeAsync(kv.second.idx, st);
+      if (kv.second.ready) cudaEventDestroy(kv.second.ready);
+    }
+    cudaStreamSynchronize(st);
+  }
+  for (auto& r : s->inflight) cudaEventDestroy(r.done);
+  for (auto e : s->free_events) cudaEventDestroy(e);
+  if (s->pool) cudaMemPoolDestroy(s->pool);
+  for (auto p : s->ws) cudaFree(p);
+  for (auto p : s->pair_buf) cudaFree(p);
+  if (s->d_counts) cudaFree(s->d_counts);
+  if (s->h_counts) cudaFreeHost(s->h_counts);
+  if (s->ref) cudaEventDestroy(s->ref);
+  for (auto& st : s->streams) cudaStreamDestroy(st);
+  delete s;
+}
+
+extern "C" hg_status hg_server_create(size_t budget_bytes, int max_tables, int n_streams, uint64_t max_keys,
+                                      int key_bytes, hg_server** out) {
+  if (!out) return HG_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (key_bytes != 4 && key_bytes != 8) return HG_ERR_KEY_WIDTH;
+  if (max_tables <= 0 || n_streams <= 0 || n_streams > 64 || max_keys == 0 || budget_bytes == 0)
+    return lib_fail(HG_ERR_INVALID_ARGUMENT, "hg_server_create: tables, streams, keys and budget must be positive");
+  if (max_keys >= (1ull << 32)) return lib_fail(HG_ERR_TOO_LARGE, "hg_server_create: max_keys must be below 2^32");
+  size_t wb = 0, wq = 0;
+  BuildPlan bp;
+  ProbePlan pp;
+  hg_status st = plan_build(max_keys, key_bytes, max_keys, true, &bp);
+  if (st != HG_OK) return st;
+  st = plan_probe(max_keys, true, max_keys, max_keys, key_bytes, true, &pp);
+  if (st != HG_OK) return st;
+  wb = bp.total;
+  wq = pp.total;
+  hg_server* s = new hg_server();
+  cudaGetDevice(&s->device);
+  s->key_bytes = key_bytes;
+  s->max_tables = max_tables;
+  s->budget = budget_bytes;
+  s->max_keys = max_keys;
+  s->ws_bytes = std::max(wb, wq);
+  s->n_slots = 1u << 16;
+  s->slot_busy.assign(s->n_slots, 0);
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = s->device;
+  cudaError_t e = cudaMemPoolCreate(&s->pool, &props);
+  if (e == cudaSuccess) {
+    uint64_t keep = budget_bytes;
+    e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  for (int i = 0; i < n_streams && e == cudaSuccess; i++) {
+    cudaStream_t x = nullptr;
+    e = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
+    if (e != cudaSuccess) break;
+    s->streams.push_back(x);
+    void* w = nullptr;
+    e = cudaMalloc(&w, s->ws_bytes);
+    if (e != cudaSuccess) break;
+    s->ws.push_back(w);
+    uint32_t* pb = nullptr;
+    e = cudaMalloc(&pb, max_keys * 8);
+    if (e != cudaSuccess) break;
+    s->pair_buf.push_back(pb);
+    s->busy_until.push_back(0.0);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&s->d_counts, sizeof(unsigned long long) * s->n_slots);
+  if (e == cudaSuccess) e = cudaMallocHost(&s->h_counts, sizeof(unsigned long long) * s->n_slots);
+  if (e == cudaSuccess) e = cudaEventCreate(&s->ref);
+  if (e == cudaSuccess) e = rebase_clock(s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    hg_server_free(s);
+    return cuda_fail(e, "hg_server_create");
+  }
+  *out = s;
+  return HG_OK;
+}
+
+extern "C" hg_status hg_server_reserve(hg_server* s, size_t bytes) {
+  if (!s) return HG_ERR_INVALID_ARGUMENT;
+  bytes = std::min(bytes, s->budget);
+  // 1 GiB blocks taken from the pool and handed back at once: the pool maps
+  // them and, its release threshold being the budget, keeps them mapped.
+  cudaStream_t st = s->streams[0];
+  std::vector<void*> blocks;
+  cudaError_t e = cudaSuccess;
+  for (size_t done = 0; done < bytes;) {
+    const size_t b = std::min(size_t(1) << 30, bytes - done);
+    void* p = nullptr;
+    e = cudaMallocFromPoolAsync(&p, b, s->pool, st);
+    if (e != cudaSuccess) break;
+    blocks.push_back(p);
+    done += b;
+  }
+  if (e != cudaSuccess) cudaGetLastError();
+  for (void* p : blocks) cudaFreeAsync(p, st);
+  const cudaError_t e2 = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "hg_server_reserve");
+  return e2 == cudaSuccess ? HG_OK : cuda_fail(e2, "hg_server_reserve: sync");
+}
+
+extern "C" hg_status hg_server_build(hg_server* s, uint64_t table_id, const void* d_keys, uint64_t n,
+                                     uint64_t n_buckets, int with_index, double arrival_s, uint64_t* ticket) {
+  if (!s || !ticket || (n > 0 && !d_keys) || n_buckets == 0) return HG_ERR_INVALID_ARGUMENT;
+  if (n > s->max_keys || n_buckets > s->max_keys)
+    return lib_fail(HG_ERR_TOO_LARGE, "hg_server_build: more keys or buckets than the server's max_keys");
+  const size_t bytes = (n_buckets + 1) * 4 + n * (s->key_bytes + (with_index ? 4 : 0));
+  if (s->tables.count(table_id)) evict(s, table_id);  // replaced
+  make_room(s, bytes);
+  const int si = pick_stream(s, 20e-6 + double(n) * 4e-11);
+  cudaStream_t st = s->streams[si];
+  ServerTable t;
+  t.n = n;
+  t.n_buckets = n_buckets;
+  t.with_index = with_index != 0;
+  t.bytes = bytes;
+  t.stream = si;
+  cudaError_t e = cudaMallocFromPoolAsync(&t.offsets, (n_buckets + 1) * 4, s->pool, st);
+  if (e == cudaSuccess && n) e = cudaMallocFromPoolAsync(&t.keys, n * s->key_bytes, s->pool, st);
+  if (e == cudaSuccess && n && with_index)
+    e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&t.idx), n * 4, s->pool, st);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t.ready, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (t.offsets) cudaFreeAsync(t.offsets, st);
+    if (t.keys) cudaFreeAsync(t.keys, st);
+    if (t.idx) cudaFreeAsync(t.idx, st);
+    return cuda_fail(e, "hg_server_build: table allocation");
+  }
+  hg_status hs = hg_build_into(d_keys, n, s->key_bytes, n_buckets, t.offsets, t.keys, t.idx,
+                               s->ws[si], s->ws_bytes, reinterpret_cast<hg_stream_t>(st));
+  if (hs != HG_OK) {
+    cudaFreeAsync(t.offsets, st);
+    if (t.keys) cudaFreeAsync(t.keys, st);
+    if (t.idx) cudaFreeAsync(t.idx, st);
+    cudaEventDestroy(t.ready);
+    return hs;
+  }
+  cudaEventRecord(t.ready, st);
+  s->lru.push_back(table_id);
+  t.lru = std::prev(s->lru.end());
+  s->bytes += bytes;
+  s->tables.emplace(table_id, t);
+  ServerReq r{s->next_ticket++, 0, 0, arrival_s, take_event(s), 0};
+  cudaEventRecord(r.done, st);
+  s->inflight.push_back(r);
+  *ticket = r.ticket;
+  return HG_OK;
+}
+
+extern "C" hg_status hg_server_intersect(hg_server* s, uint64_t table_id, const void* d_query, uint64_t nq,
+                                         uint32_t* d_pairs, uint64_t pair_cap, double arrival_s, uint64_t* ticket) {
+  if (!s || !ticket || (nq > 0 && !d_query)) return HG_ERR_INVALID_ARGUMENT;
+  if (nq > s->max_keys) return lib_fail(HG_ERR_TOO_LARGE, "hg_server_intersect: more queries than max_keys");
+  uint32_t slot = 0;
+  hg_status hs = reserve_slot(s, &slot);
+  if (hs != HG_OK) return hs;
+  auto it = s->tables.find(table_id);
+  const int si = pick_stream(s, 20e-6 + double(nq) * 4e-11);
+  cudaStream_t st = s->streams[si];
+  ServerReq r{s->next_ticket++, 1, 0, arrival_s, take_event(s), slot};
+  if (it == s->tables.end()) {
+    r.missed = 1;
+  } else {
+    ServerTable& t = it->second;
+    s->lru.splice(s->lru.end(), s->lru, t.lru);  // most recently used
+    cudaStreamWaitEvent(st, t.ready, 0);
+    uint32_t* pairs = d_pairs ? d_pairs : s->pair_buf[si];
+    const uint64_t cap = d_pairs ? pair_cap : std::min<uint64_t>(pair_cap, s->max_keys);
+    hs = hg_intersect_into(t.offsets, t.keys, t.idx, t.n, t.n_buckets, s->key_bytes, d_query, nq, nullptr, pairs, cap,
+                           s->d_counts + slot, s->ws[si], s->ws_bytes, reinterpret_cast<hg_stream_t>(st));
+    if (hs != HG_OK) {
+      s->free_events.push_back(r.done);
+      s->slot_busy[slot] = 0;
+      return hs;
+    }
+    cudaMemcpyAsync(s->h_counts + slot, s->d_counts + slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+  }
+  cudaEventRecord(r.done, st);
+  s->inflight.push_back(r);
+  *ticket = r.ticket;
+  return HG_OK;
+}
+
+extern "C" hg_status hg_server_poll(hg_server* s, int block, hg_server_done* out, int max_out, int* n_out) {
+  if (!s || !n_out || (max_out > 0 && !out)) return HG_ERR_INVALID_ARGUMENT;
+  *n_out = 0;
+  if (block && !s->inflight.empty() && max_out > 0) {
+    const cudaError_t e = cudaEventSynchronize(s->inflight.front().done);
+    if (e != cudaSuccess) return cuda_fail(e, "hg_server_poll: wait");
+  }
+  for (auto it = s->inflight.begin(); it != s->inflight.end() && *n_out < max_out;) {
+    const cudaError_t q = cudaEventQuery(it->done);
+    if (q == cudaErrorNotReady) {
+      ++it;
+      continue;
+    }
+    if (q != cudaSuccess) return cuda_fail(q, "hg_server_poll: query");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, s->ref, it->done);
+    hg_server_done& d = out[(*n_out)++];
+    d.ticket = it->ticket;
+    d.kind = it->kind;
+    d.missed = it->missed;
+    d.count = it->kind == 1 && !it->missed ? s->h_counts[it->slot] : 0ull;
+    d.latency_s = std::max(0.0, s->ref_host + 1e-3 * double(ms) - it->arrival);
+    if (it->kind == 1) s->slot_busy[it->slot] = 0;
+    s->free_events.push_back(it->done);
+    it = s->inflight.erase(it);
+  }
+  if (s->inflight.empty() && monotonic_s() - s->ref_host > 60.0) {
+    const cudaError_t e = rebase_clock(s);
+    if (e != cudaSuccess) return cuda_fail(e, "hg_server_poll: clock");
+  }
+  return HG_OK;
+}
+
+extern "C" hg_status hg_server_stats(const hg_server* s, uint64_t* resident_tables, size_t* resident_bytes,
+                                     uint64_t* evictions, uint64_t* inflight) {
+  if (!s) return HG_ERR_INVALID_ARGUMENT;
+  if (resident_tables) *resident_tables = s->tables.size();
+  if (resident_bytes) *resident_bytes = s->bytes;
+  if (evictions) *evictions = s->evictions;
+  if (inflight) *inflight = s->inflight.size();
+  return HG_OK;
+}

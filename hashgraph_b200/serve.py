@@ -1,198 +1,148 @@
-"""Serving loop: resident tables, a device-memory budget with LRU eviction,
-and build / intersect requests executed concurrently on a pool of CUDA
-streams, with per-request latency.
+"""Serving loop over the native serving engine (hg_server_* of the C ABI).
+
+The engine keeps resident tables under a device-memory budget and a table
+limit (least recently used out first), spreads build and intersect requests
+over a pool of CUDA streams, orders an intersect after its table's build, and
+measures each request's latency from its arrival stamp to the device
+completion of its last operation.  This module adds the request objects, an
+open-loop driver (requests are submitted at their arrival times whatever the
+completions) and latency percentiles.
 
 The reference has no serving component (its tables are built and
-intersected once per process, test/MultiHashGraphTest.cu:288-338).  This is
-the host-side scheduler around the C ABI; all device work goes through the
-library's kernels.
-
-A request's latency is measured from its arrival time to the completion of
-its last kernel on the device: the end event's time is mapped onto the host
-clock through one reference event recorded when the server starts.
+intersected once per process, test/MultiHashGraphTest.cu:288-338).
 """
 from __future__ import annotations
 
-import collections
 import ctypes
 import time
 from dataclasses import dataclass, field
 
-from . import Table, _ptr, _stream, check, lib
+from . import _ptr, check, lib
+from ._capi import ServerDone
 
 
 @dataclass
 class Request:
     kind: str                      # "build" or "intersect"
     table_id: int
-    arrival: float                 # host seconds (time.perf_counter) when the request arrives
-    keys: object = None            # build: device key tensor
+    arrival: float                 # seconds on hg_server_now()'s clock (CLOCK_MONOTONIC)
+    keys: object = None            # build: device key tensor (valid until completion)
     n_buckets: int = 0
     with_index: bool = False
     queries: object = None         # intersect: device query tensor
     pair_cap: int = 0
-    # filled by the server
+    # filled when the request completes
     count: int | None = None
     latency_s: float | None = None
     missed: bool = False           # intersect against a table no longer resident
-    _end: object = field(default=None, repr=False)
-    _count_dev: object = field(default=None, repr=False)
-    _stream_i: int = field(default=-1, repr=False)
+    ticket: int = field(default=0, repr=False)
 
 
-class TableStore:
-    """Resident tables keyed by id, least recently used first out, within a
-    device-byte budget and a table-count limit."""
-
-    def __init__(self, budget_bytes: int, max_tables: int):
-        self.budget = int(budget_bytes)
-        self.max_tables = int(max_tables)
-        self.tables: collections.OrderedDict[int, Table] = collections.OrderedDict()
-        self.bytes = 0
-        self.evictions = 0
-
-    @staticmethod
-    def table_bytes(t: Table) -> int:
-        b = t.offsets.numel() * 4 + t.keys.numel() * t.keys.element_size()
-        if t.idx is not None:
-            b += t.idx.numel() * 4
-        return b
-
-    def get(self, table_id: int) -> Table | None:
-        t = self.tables.get(table_id)
-        if t is not None:
-            self.tables.move_to_end(table_id)
-        return t
-
-    def make_room(self, need_bytes: int, keep: int | None = None) -> None:
-        while self.tables and (self.bytes + need_bytes > self.budget or len(self.tables) >= self.max_tables):
-            victim = next(iter(self.tables))
-            if victim == keep:
-                break
-            t = self.tables.pop(victim)
-            self.bytes -= self.table_bytes(t)
-            self.evictions += 1
-
-    def put(self, table_id: int, t: Table) -> None:
-        old = self.tables.pop(table_id, None)
-        if old is not None:
-            self.bytes -= self.table_bytes(old)
-        self.tables[table_id] = t
-        self.bytes += self.table_bytes(t)
+def now() -> float:
+    """The clock arrival stamps use (the engine's CLOCK_MONOTONIC seconds)."""
+    return float(lib().hg_server_now())
 
 
 class Server:
-    """Runs requests on `n_streams` CUDA streams.  Each stream owns a build /
-    intersect workspace and a pair buffer sized for `max_keys`."""
+    """A native serving engine on the current device: `budget_bytes` of
+    resident tables at most, `max_tables` tables at most, `n_streams` CUDA
+    streams, tables of up to `max_keys` keys and buckets."""
 
     def __init__(self, budget_bytes: int, max_tables: int = 512, n_streams: int = 4, max_keys: int = 1 << 24,
                  key_bytes: int = 8, device=None):
         import torch
-        self.torch = torch
-        self.device = torch.device(device or "cuda")
-        self.store = TableStore(budget_bytes, max_tables)
+        if device is not None:
+            torch.cuda.set_device(torch.device(device))
         self.key_bytes = key_bytes
-        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(n_streams)]
-        L = lib()
-        wb, wq = ctypes.c_size_t(0), ctypes.c_size_t(0)
-        check(L.hg_build_workspace_size(max_keys, key_bytes, max_keys, 1, ctypes.byref(wb)), "workspace")
-        check(L.hg_intersect_workspace_size(max_keys, 1, max_keys, max_keys, key_bytes, 1, ctypes.byref(wq)),
-              "workspace")
-        ws = max(wb.value, wq.value, 1)
-        self.ws = [torch.empty(ws, dtype=torch.uint8, device=self.device) for _ in self.streams]
-        self.pairs = [torch.empty((max_keys, 2), dtype=torch.int32, device=self.device) for _ in self.streams]
-        self.busy_until = [0.0] * n_streams     # host estimate of each stream's queued work
-        self.inflight: list[Request] = []
-        torch.cuda.synchronize(self.device)
-        self.ref_event = torch.cuda.Event(enable_timing=True)
-        self.ref_event.record(torch.cuda.current_stream(self.device))
-        self.ref_event.synchronize()
-        self.ref_host = time.perf_counter()
+        self._h = ctypes.c_void_p()
+        check(lib().hg_server_create(int(budget_bytes), int(max_tables), int(n_streams), int(max_keys), key_bytes,
+                                     ctypes.byref(self._h)), "hg_server_create")
+        self._pending: dict[int, Request] = {}
+        self._done = (ServerDone * 1024)()
 
-    def _pick_stream(self, now: float) -> int:
-        return min(range(len(self.streams)), key=lambda i: max(self.busy_until[i], now))
+    def reserve(self, nbytes: int) -> None:
+        """Maps `nbytes` (at most the budget) into the table pool up front."""
+        check(lib().hg_server_reserve(self._h, int(nbytes)), "hg_server_reserve")
 
-    def submit(self, r: Request, est_s: float = 0.0) -> None:
-        torch = self.torch
-        now = time.perf_counter()
-        i = self._pick_stream(now)
-        self.busy_until[i] = max(self.busy_until[i], now) + est_s
-        s = self.streams[i]
-        r._stream_i = i
+    def submit(self, r: Request) -> None:
         L = lib()
-        with torch.cuda.stream(s):
-            if r.kind == "build":
-                n = r.keys.numel()
-                self.store.make_room((r.n_buckets + 1) * 4 + n * (self.key_bytes + (4 if r.with_index else 0)),
-                                     keep=None)
-                t = Table(r.n_buckets, self.key_bytes, r.with_index, n, self.device, workspace=False)
-                check(L.hg_build_into(_ptr(r.keys), n, self.key_bytes, r.n_buckets, _ptr(t.offsets), _ptr(t.keys),
-                                      _ptr(t.idx), _ptr(self.ws[i]), self.ws[i].numel(), _stream(s)),
-                      "serve build")
-                t.n = n
-                # intersects on other streams wait for the build to finish
-                t.ready = torch.cuda.Event()
-                t.ready.record(s)
-                self.store.put(r.table_id, t)
-            else:
-                t = self.store.get(r.table_id)
-                r._count_dev = torch.zeros(1, dtype=torch.int64, device=self.device)
-                if t is None:
-                    r.missed = True
-                else:
-                    s.wait_event(t.ready)
-                    # the table's memory is not reused while this stream reads it,
-                    # even if the table is evicted or replaced meanwhile
-                    for a in (t.offsets, t.keys, t.idx):
-                        if a is not None:
-                            a.record_stream(s)
-                    nq = r.queries.numel()
-                    check(L.hg_intersect_into(_ptr(t.offsets), _ptr(t.keys), _ptr(t.idx), t.n, t.n_buckets,
-                                              self.key_bytes, _ptr(r.queries), nq, None, _ptr(self.pairs[i]),
-                                              min(r.pair_cap, self.pairs[i].shape[0]), _ptr(r._count_dev),
-                                              _ptr(self.ws[i]), self.ws[i].numel(), _stream(s)),
-                          "serve intersect")
-            r._end = torch.cuda.Event(enable_timing=True)
-            r._end.record(s)
-        self.inflight.append(r)
+        t = ctypes.c_uint64(0)
+        if r.kind == "build":
+            check(L.hg_server_build(self._h, r.table_id, _ptr(r.keys), r.keys.numel(), r.n_buckets, int(r.with_index),
+                                    r.arrival, ctypes.byref(t)), "hg_server_build")
+        else:
+            check(L.hg_server_intersect(self._h, r.table_id, _ptr(r.queries), r.queries.numel(), None, r.pair_cap,
+                                        r.arrival, ctypes.byref(t)), "hg_server_intersect")
+        r.ticket = t.value
+        self._pending[r.ticket] = r
 
     def poll(self, block: bool = False) -> list[Request]:
-        done, rest = [], []
-        for r in self.inflight:
-            if block:
-                r._end.synchronize()
-            if block or r._end.query():
-                gpu_t = self.ref_host + self.ref_event.elapsed_time(r._end) * 1e-3
-                r.latency_s = max(gpu_t - r.arrival, 0.0)
-                if r.kind == "intersect":
-                    r.count = int(r._count_dev.item())
-                done.append(r)
-            else:
-                rest.append(r)
-        self.inflight = rest
-        return done
+        """Completed requests (block: wait until at least the oldest one is)."""
+        out = []
+        n = ctypes.c_int(0)
+        while True:
+            check(lib().hg_server_poll(self._h, int(block and not out), self._done, len(self._done), ctypes.byref(n)),
+                  "hg_server_poll")
+            for i in range(n.value):
+                d = self._done[i]
+                r = self._pending.pop(d.ticket)
+                r.latency_s = d.latency_s
+                r.missed = bool(d.missed)
+                if d.kind == 1:
+                    r.count = int(d.count)
+                out.append(r)
+            if n.value < len(self._done):
+                return out
+
+    def drain(self) -> list[Request]:
+        out = []
+        while self._pending:
+            out += self.poll(block=True)
+        return out
+
+    def stats(self) -> dict:
+        t, e, f = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_uint64(0)
+        b = ctypes.c_size_t(0)
+        check(lib().hg_server_stats(self._h, ctypes.byref(t), ctypes.byref(b), ctypes.byref(e), ctypes.byref(f)),
+              "hg_server_stats")
+        return {"resident_tables": t.value, "resident_bytes": b.value, "evictions": e.value, "inflight": f.value}
+
+    def free(self) -> None:
+        if self._h:
+            lib().hg_server_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
-def run_open_loop(server: Server, requests: list[Request], est=lambda r: 0.0) -> float:
-    """Submits every request at its arrival time (open loop; arrivals do not
-    wait for completions) and returns the makespan in seconds."""
-    t0 = time.perf_counter()
-    base = requests[0].arrival if requests else 0.0
+def run_open_loop(server, requests: list[Request], clock=now, sleep=time.sleep) -> float:
+    """Submits every request at its arrival time (open loop: arrivals do not
+    wait for completions), collects completions meanwhile, and returns the
+    makespan in seconds.  Arrival times are taken relative to the first
+    request and re-stamped on `clock`."""
+    if not requests:
+        return 0.0
+    t0 = clock()
+    base = requests[0].arrival
     for r in requests:
         r.arrival = t0 + (r.arrival - base)
     k = 0
     while k < len(requests):
-        now = time.perf_counter()
-        while k < len(requests) and requests[k].arrival <= now:
-            server.submit(requests[k], est(requests[k]))
+        t = clock()
+        while k < len(requests) and requests[k].arrival <= t:
+            server.submit(requests[k])
             k += 1
         server.poll()
         if k < len(requests):
-            wait = requests[k].arrival - time.perf_counter()
+            wait = requests[k].arrival - clock()
             if wait > 0:
-                time.sleep(min(wait, 0.0005))
-    server.poll(block=True)
-    return time.perf_counter() - t0
+                sleep(min(wait, 0.0005))
+    server.drain()
+    return clock() - t0
 
 
 def latency_summary(requests: list[Request]) -> dict:

@@ -281,6 +281,50 @@ void hg_batch_free(hg_batch* batch, hg_stream_t stream);
 hg_status hg_batch_build_intersect(const hg_batch_pair* pairs, int n_pairs, int key_bytes, hg_stream_t stream);
 
 /* ------------------------------------------------------------------------
+ * Serving engine (no counterpart in the reference, whose tables are built
+ * and intersected once per process): resident tables under a device-memory
+ * budget and a table limit, evicted least recently used first; requests
+ * spread over a pool of CUDA streams; each request's latency from its
+ * arrival stamp to the device completion of its last operation.  One host
+ * thread drives a server.  Tables hold up to max_keys keys and buckets.
+ * ---------------------------------------------------------------------- */
+typedef struct hg_server hg_server;
+
+/* A completed request, as hg_server_poll reports it. */
+typedef struct hg_server_done {
+  uint64_t ticket;
+  int kind;                  /* 0 build, 1 intersect */
+  int missed;                /* intersect: the table was not resident */
+  unsigned long long count;  /* intersect: exact match count */
+  double latency_s;          /* arrival to device completion */
+} hg_server_done;
+
+/* The clock arrival stamps use (CLOCK_MONOTONIC, seconds). */
+double hg_server_now(void);
+hg_status hg_server_create(size_t budget_bytes, int max_tables, int n_streams, uint64_t max_keys,
+                           int key_bytes, hg_server** out);
+/* Maps `bytes` (at most the budget) of device memory into the server's table
+ * pool up front, so that builds do not wait on the host while the pool
+ * grows.  The pool keeps up to the budget mapped for reuse. */
+hg_status hg_server_reserve(hg_server* server, size_t bytes);
+/* Builds (or replaces) table `table_id` from d_keys[0..n); the keys must be
+ * written before the call (the server's streams do not wait on the caller's)
+ * and stay valid until the request completes.  Evicts tables to make room. */
+hg_status hg_server_build(hg_server* server, uint64_t table_id, const void* d_keys, uint64_t n,
+                          uint64_t n_buckets, int with_index, double arrival_s, uint64_t* ticket);
+/* Probes d_query[0..nq) (the same rules as the keys of a build) against
+ * table `table_id`; pairs go to d_pairs (or,
+ * when NULL, to a per-stream buffer the next request overwrites). */
+hg_status hg_server_intersect(hg_server* server, uint64_t table_id, const void* d_query, uint64_t nq,
+                              uint32_t* d_pairs, uint64_t pair_cap, double arrival_s, uint64_t* ticket);
+/* Reports up to max_out completed requests (block: wait for the oldest). */
+hg_status hg_server_poll(hg_server* server, int block, hg_server_done* out, int max_out, int* n_out);
+hg_status hg_server_stats(const hg_server* server, uint64_t* resident_tables, size_t* resident_bytes,
+                          uint64_t* evictions, uint64_t* inflight);
+/* Waits for all work, frees every table and the server. */
+void hg_server_free(hg_server* server);
+
+/* ------------------------------------------------------------------------
  * Instrumentation (no counterpart in the reference, which prints host wall
  * times under HOST_PROFILE, src/MultiHashGraph.cu:55-57,431-615).
  * ---------------------------------------------------------------------- */

@@ -138,3 +138,27 @@ def test_table_file_header_checks_without_device(capi, tmp_path):
     wide = b"HGB2TBL\0" + struct.pack("<4I3Q2Q", 1, 5, 1, 1, 3, 2, 0, 0, 0)
     (tmp_path / "width.hgt").write_bytes(wide + bytes(48))
     assert L.hg_table_file_info(str(tmp_path / "width.hgt").encode(), *args) == -8
+
+
+def test_server_argument_checks_without_device(capi):
+    """hg_server_* check their arguments before any device call."""
+    L = capi.lib()
+    h = ctypes.c_void_p()
+    assert L.hg_server_create(1 << 30, 8, 2, 1 << 20, 3, ctypes.byref(h)) == -8
+    assert L.hg_server_create(1 << 30, 0, 2, 1 << 20, 8, ctypes.byref(h)) == -1
+    assert L.hg_server_create(1 << 30, 8, 0, 1 << 20, 8, ctypes.byref(h)) == -1
+    assert L.hg_server_create(1 << 30, 8, 65, 1 << 20, 8, ctypes.byref(h)) == -1
+    assert L.hg_server_create(0, 8, 2, 1 << 20, 8, ctypes.byref(h)) == -1
+    assert L.hg_server_create(1 << 30, 8, 2, 1 << 32, 8, ctypes.byref(h)) == -6
+    assert L.hg_server_create(1 << 30, 8, 2, 1 << 20, 8, None) == -1
+    assert not h.value
+    t = ctypes.c_uint64(0)
+    n = ctypes.c_int(0)
+    assert L.hg_server_build(None, 0, None, 0, 1, 0, 0.0, ctypes.byref(t)) == -1
+    assert L.hg_server_intersect(None, 0, None, 0, None, 0, 0.0, ctypes.byref(t)) == -1
+    assert L.hg_server_poll(None, 0, None, 0, ctypes.byref(n)) == -1
+    assert L.hg_server_stats(None, None, None, None, None) == -1
+    assert L.hg_server_reserve(None, 1 << 20) == -1
+    L.hg_server_free(None)
+    t0 = L.hg_server_now()
+    assert t0 > 0 and L.hg_server_now() >= t0

@@ -1,47 +1,65 @@
-"""Host logic of the serving loop: the table store's LRU order, byte budget
-and table-count limit (CPU tensors stand in for device arrays)."""
-import torch
-
-from hashgraph_b200.serve import TableStore
-
-
-class _T:
-    def __init__(self, nbytes):
-        self.offsets = torch.empty(1, dtype=torch.int32)
-        self.keys = torch.empty(nbytes // 8, dtype=torch.int64)
-        self.idx = None
+"""Host logic of the serving loop: the open-loop driver submits every request
+at its arrival time whatever the completions, and latency percentiles.  A
+fake clock and a fake server stand in for the native engine."""
+from hashgraph_b200.serve import Request, latency_summary, run_open_loop
 
 
-def _bytes(t):
-    return TableStore.table_bytes(t)
+class _Clock:
+    def __init__(self):
+        self.t = 100.0
+
+    def __call__(self):
+        return self.t
+
+    def sleep(self, dt):
+        self.t += dt
 
 
-def test_lru_order_and_count_limit():
-    s = TableStore(budget_bytes=1 << 40, max_tables=3)
-    for i in range(3):
-        s.make_room(80)
-        s.put(i, _T(80))
-    s.get(0)                       # 0 is now the most recent
-    s.make_room(80)
-    s.put(3, _T(80))
-    assert list(s.tables) == [2, 0, 3]  # 1 was least recently used and went first
-    assert s.evictions == 1
+class _FakeServer:
+    """Completes each request 5 ms after its submission."""
+
+    def __init__(self, clock):
+        self.clock = clock
+        self.pending = []
+        self.submitted = []
+
+    def submit(self, r):
+        self.submitted.append((r, self.clock()))
+        self.pending.append((r, self.clock() + 0.005))
+
+    def poll(self, block=False):
+        done = [r for r, t in self.pending if t <= self.clock()]
+        self.pending = [(r, t) for r, t in self.pending if t > self.clock()]
+        for r in done:
+            r.latency_s = 0.005
+        return done
+
+    def drain(self):
+        out = [r for r, _ in self.pending]
+        for r in out:
+            r.latency_s = 0.005
+        self.pending = []
+        return out
 
 
-def test_byte_budget():
-    t = _T(800)
-    s = TableStore(budget_bytes=3 * _bytes(t), max_tables=100)
-    for i in range(5):
-        s.make_room(_bytes(t))
-        s.put(i, _T(800))
-        assert s.bytes <= s.budget
-    assert set(s.tables) == {2, 3, 4}
-    assert s.evictions == 2
+def test_open_loop_submits_at_arrival_times():
+    clock = _Clock()
+    srv = _FakeServer(clock)
+    reqs = [Request("intersect", 0, 10.0 + 0.001 * k) for k in range(20)]
+    makespan = run_open_loop(srv, reqs, clock=clock, sleep=clock.sleep)
+    assert len(srv.submitted) == 20
+    # each request goes in no earlier than its arrival, and not long after it
+    for r, t in srv.submitted:
+        assert r.arrival - 1e-12 <= t <= r.arrival + 0.0006
+    # arrivals were re-stamped relative to the first one
+    assert abs(reqs[0].arrival - 100.0) < 1e-9 and abs(reqs[-1].arrival - reqs[0].arrival - 0.019) < 1e-9
+    assert makespan >= 0.019
+    assert all(r.latency_s == 0.005 for r in reqs)
 
 
-def test_replacing_a_table_keeps_the_byte_count():
-    s = TableStore(budget_bytes=1 << 40, max_tables=10)
-    s.put(7, _T(800))
-    b = s.bytes
-    s.put(7, _T(800))
-    assert s.bytes == b and len(s.tables) == 1
+def test_latency_percentiles():
+    reqs = [Request("build", 0, 0.0, latency_s=k / 1000.0) for k in range(1, 101)]
+    s = latency_summary(reqs)
+    assert abs(s["p50_ms"] - 51.0) < 1e-9 and abs(s["p99_ms"] - 100.0) < 1e-9
+    assert abs(s["mean_ms"] - 50.5) < 1e-9 and s["max_ms"] == 100.0
+    assert latency_summary([]) == {}

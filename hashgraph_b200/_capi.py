@@ -34,6 +34,7 @@ ERR_DEVICE_TIMEOUT = -5
 # Every symbol include/hashgraph_b200.h declares: (restype, argtypes).
 _p = ctypes.c_void_p
 _u64 = ctypes.c_uint64
+_u32 = ctypes.c_uint32
 _i32 = ctypes.c_int32
 _int = ctypes.c_int
 _sz = ctypes.c_size_t
@@ -108,6 +109,16 @@ SIGNATURES = {
     "hg_server_stats": (_i32, [_p, ctypes.POINTER(_u64), ctypes.POINTER(_sz), ctypes.POINTER(_u64),
                                ctypes.POINTER(_u64)]),
     "hg_server_free": (None, [_p]),
+    "hg_shard_histogram": (_i32, [_p, _u64, _int, _u64, _u32, _p, _p]),
+    "hg_shard_splits": (_i32, [_p, _u32, _u64, _int, _p]),
+    "hg_shard_route_workspace_size": (_i32, [_u64, _int, ctypes.POINTER(_sz)]),
+    "hg_shard_route": (_i32, [_p, _u64, _int, _u64, _p, _int, _u32, _p, _p, _p, _p, _sz, _p]),
+    "hg_shard_build_into": (_i32, [_p, _p, _u64, _int, _u64, _u64, _u64, _p, _p, _p, _p, _sz, _p]),
+    "hg_shard_build_into_path": (_i32, [_p, _p, _u64, _int, _u64, _u64, _u64, _p, _p, _p, _p, _sz, _int, _p]),
+    "hg_shard_intersect_into": (_i32, [_p, _p, _p, _u64, _u64, _u64, _u64, _int, _p, _u64, _p, _p, _u64, _p, _p,
+                                       _sz, _p]),
+    "hg_shard_intersect_into_path": (_i32, [_p, _p, _p, _u64, _u64, _u64, _u64, _int, _p, _u64, _p, _p, _u64, _p,
+                                            _p, _sz, _int, _p]),
     "hg_profile_enable": (_i32, [_int]),
     "hg_profile_read": (_i32, [_int, ctypes.POINTER(_int), ctypes.POINTER(ctypes.c_char_p),
                                ctypes.POINTER(ctypes.c_float)]),

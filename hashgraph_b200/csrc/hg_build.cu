@@ -788,7 +788,7 @@ static void launch_scan(uint32_t* data, uint64_t count, uint64_t* status, unsign
 template <typename KeyT, int V, bool WI>
 static hg_status run_direct(const BuildPlan& p, const KeyT* keys, uint32_t* offsets, KeyT* keys_out, uint32_t* idx_out,
                             char* ws, const uint32_t* gate, cudaStream_t s) {
-  const BucketMap bm = BucketMap::make(p.n_buckets);
+  const BucketMap bm = p.bucket_map();
   uint64_t* status = reinterpret_cast<uint64_t*>(ws + p.off_status);
   unsigned* ticket = reinterpret_cast<unsigned*>(ws + p.off_ticket);
   if (gate) {
@@ -1040,7 +1040,7 @@ static hg_status run_partition_passes(const PartGeometry& g, uint64_t n, const K
 template <typename KeyT, int V, bool WI>
 static hg_status run_partitioned(const BuildPlan& p, const KeyT* keys, uint32_t* offsets, KeyT* keys_out,
                                  uint32_t* idx_out, char* ws, cudaStream_t s) {
-  const BucketMap bm = BucketMap::make(p.n_buckets);
+  const BucketMap bm = p.bucket_map();
   const PartGeometry& g = p.g;
   uint32_t* flags = reinterpret_cast<uint32_t*>(ws + p.off_flags);
   // status words, tickets, flags, partition counts and their scan states

@@ -43,10 +43,12 @@ struct BucketMap {
   uint32_t d;
   uint32_t mask;  // d - 1 when d is a power of two (0xffffffff for d = 2^32)
   uint32_t pow2;  // 1 when d is a power of two
+  uint32_t base;  // first bucket of a shard's range (fastmod form only)
 
   static BucketMap make(uint64_t n_buckets) {
     BucketMap m;
     m.pow2 = (n_buckets & (n_buckets - 1)) == 0 ? 1u : 0u;
+    m.base = 0;
     if (n_buckets >= (1ull << 32)) {
       m.magic = 0; m.d = 0; m.mask = 0xffffffffu;
     } else {
@@ -54,6 +56,21 @@ struct BucketMap {
       m.magic = UINT64_MAX / m.d + 1;
       m.mask = m.pow2 ? m.d - 1 : 0u;
     }
+    return m;
+  }
+  // The shard [lo, lo + local) of a table of `total` buckets: a key's bucket
+  // in the shard is (hash % total) - lo, for keys whose bucket lies in the
+  // range.  An aligned power-of-two range of a power-of-two table is itself a
+  // power-of-two table (the hash's low bits), so it keeps the mask form.
+  // total < 2^32 otherwise.
+  static BucketMap make_range(uint64_t total, uint64_t lo, uint64_t local) {
+    const bool p2 = (total & (total - 1)) == 0 && (local & (local - 1)) == 0;
+    if (lo == 0 && local == total) return make(total);
+    if (p2 && local > 0 && lo % local == 0) return make(local);
+    BucketMap m = make(total);
+    m.pow2 = 0;
+    m.mask = 0;
+    m.base = static_cast<uint32_t>(lo);
     return m;
   }
   // high 64 bits of x * d for a 32-bit d, from 32x32 products: with
@@ -69,7 +86,7 @@ struct BucketMap {
 #else
     const uint32_t c = static_cast<uint32_t>((static_cast<uint64_t>(xl) * d) >> 32);
 #endif
-    return static_cast<uint32_t>((static_cast<uint64_t>(xh) * d + c) >> 32);
+    return static_cast<uint32_t>((static_cast<uint64_t>(xh) * d + c) >> 32) - base;
   }
   __host__ __device__ __forceinline__ uint32_t of_key(uint64_t key) const {
     return of_hash(murmur3_low32(key));

@@ -9,3 +9,4 @@
 #include "hg_batch.cu"
 #include "hg_io.cu"
 #include "hg_server.cu"
+#include "hg_shard.cu"

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "hashgraph_b200.h"
+#include "hg_device.cuh"
 
 namespace hg {
 
@@ -51,6 +52,12 @@ struct PartGeometry {
 struct BuildPlan {
   int path = BUILD_DIRECT;
   uint64_t n = 0, n_buckets = 0;
+  // a shard of a larger table: buckets [range_lo, range_lo + n_buckets) of
+  // range_total (0: the table is whole)
+  uint64_t range_total = 0, range_lo = 0;
+  BucketMap bucket_map() const {
+    return range_total ? BucketMap::make_range(range_total, range_lo, n_buckets) : BucketMap::make(n_buckets);
+  }
   int key_bytes = 8;
   bool with_index = false;
   uint64_t scan_tiles = 0;  // direct path: in-place scan over offsets[1..B]
@@ -72,6 +79,10 @@ enum ProbePath : int { PROBE_DIRECT = 0, PROBE_PARTITIONED = 1 };
 struct ProbePlan {
   int path = PROBE_DIRECT;
   uint64_t n_a = 0, nq = 0, n_buckets = 0;
+  uint64_t range_total = 0, range_lo = 0;  // as in BuildPlan
+  BucketMap bucket_map() const {
+    return range_total ? BucketMap::make_range(range_total, range_lo, n_buckets) : BucketMap::make(n_buckets);
+  }
   int key_bytes = 8;
   bool a_idx = false;
   bool emit = false;

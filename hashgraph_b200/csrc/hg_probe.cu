@@ -545,7 +545,7 @@ static void launch_probe_direct(const ProbePlan& p, const uint32_t* a_off, const
                                 const KeyT* q, const uint32_t* q_idx, uint32_t* pairs, uint64_t cap,
                                 unsigned long long* d_count, uint64_t* status, unsigned* ticket, const uint32_t* gate,
                                 cudaStream_t s) {
-  const BucketMap bm = BucketMap::make(p.n_buckets);
+  const BucketMap bm = p.bucket_map();
   const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(p.tiles, uint64_t(device_sm_count()) * 8));
   Phase ph(s, gate ? (EMIT ? "fallback_probe_emit" : "fallback_probe_count") : (EMIT ? "probe_emit" : "probe_count"));
   count_launch();
@@ -564,7 +564,7 @@ template <typename KeyT, bool EMIT>
 static hg_status run_probe_partitioned(const ProbePlan& p, const uint32_t* a_off, const KeyT* a_keys,
                                        const uint32_t* a_idx, const KeyT* q, const uint32_t* q_idx, uint32_t* pairs,
                                        uint64_t cap, unsigned long long* d_count, char* ws, cudaStream_t s) {
-  const BucketMap bm = BucketMap::make(p.n_buckets);
+  const BucketMap bm = p.bucket_map();
   const PartGeometry& g = p.g;
   uint32_t* flags = reinterpret_cast<uint32_t*>(ws + p.off_flags);
   unsigned* ticket = reinterpret_cast<unsigned*>(ws + p.off_ticket);

@@ -281,6 +281,70 @@ void hg_batch_free(hg_batch* batch, hg_stream_t stream);
 hg_status hg_batch_build_intersect(const hg_batch_pair* pairs, int n_pairs, int key_bytes, hg_stream_t stream);
 
 /* ------------------------------------------------------------------------
+ * One table sharded over several devices by bucket range: MultiHashGraph
+ * with gpuCount > 1 (src/MultiHashGraph.cu:408-629 build, :631-740
+ * intersect).  Shard r holds buckets [splits[r], splits[r+1]) of a table of
+ * n_buckets; one process drives each device and the caller moves the routed
+ * keys between devices with its own collective (an NCCL all-to-all).  A
+ * shard's table is the global table's CSR restricted to its range:
+ * offsets[b - lo] for b in [lo, hi], rebased to start at 0.
+ * ---------------------------------------------------------------------- */
+#define HG_MAX_SHARDS 64
+
+/* Adds the bucket-id histogram of d_keys into d_bins[n_bins] (uint64):
+ * bin = bucket / ceil(n_buckets / n_bins) -- countBinSizes,
+ * include/MultiHashGraphDeviceOperators.cuh:153-163.  n_bins <= 32768. */
+hg_status hg_shard_histogram(const void* d_keys, uint64_t n, int key_bytes, uint64_t n_buckets,
+                             uint32_t n_bins, unsigned long long* d_bins, hg_stream_t stream);
+/* Host only: splits[0..n_shards] from the summed histogram of every
+ * device's keys -- the reference's rule, include/MultiHashGraphHostOperators.cuh:80-88
+ * (about n/n_shards keys per shard; splits[0] = 0, splits[n_shards] = n_buckets). */
+hg_status hg_shard_splits(const unsigned long long* h_bins, uint32_t n_bins, uint64_t n_buckets,
+                          int n_shards, uint64_t* h_splits);
+/* Groups d_keys by destination shard (countKeyBuffSizes + binKeyValues,
+ * include/MultiHashGraphDeviceOperators.cuh:220-246): d_keys_out holds
+ * shard 0's keys, then shard 1's, ..., each group in input order;
+ * d_idx_out (optional) the keys' global indices index_base + position;
+ * d_shard_offsets[n_shards + 1] (uint64, device) the group boundaries.
+ * `splits` is a host array. */
+hg_status hg_shard_route_workspace_size(uint64_t n, int n_shards, size_t* bytes);
+hg_status hg_shard_route(const void* d_keys, uint64_t n, int key_bytes, uint64_t n_buckets,
+                         const uint64_t* splits, int n_shards, uint32_t index_base, void* d_keys_out,
+                         uint32_t* d_idx_out, unsigned long long* d_shard_offsets, void* d_workspace,
+                         size_t workspace_bytes, hg_stream_t stream);
+/* Builds the shard [bucket_lo, bucket_hi) of a table of n_buckets from keys
+ * whose buckets all lie in that range (a shard's routed keys); d_offsets
+ * holds bucket_hi - bucket_lo + 1 entries.  With d_idx_out, the index holds
+ * d_key_idx[position] (the keys' global indices) when d_key_idx is given,
+ * else the position.  Workspace: hg_build_workspace_size(n, key_bytes,
+ * bucket_hi - bucket_lo, with_index). */
+hg_status hg_shard_build_into(const void* d_keys, const uint32_t* d_key_idx, uint64_t n, int key_bytes,
+                              uint64_t n_buckets, uint64_t bucket_lo, uint64_t bucket_hi,
+                              uint32_t* d_offsets, void* d_keys_out, uint32_t* d_idx_out,
+                              void* d_workspace, size_t workspace_bytes, hg_stream_t stream);
+/* Probes queries whose buckets lie in the shard's range against the shard
+ * (as hg_intersect_into; q_ref = d_query_idx[i] when given).  Workspace:
+ * hg_intersect_workspace_size(n_a, a_has_index, bucket_hi - bucket_lo, nq,
+ * key_bytes, emit_pairs). */
+hg_status hg_shard_intersect_into(const uint32_t* d_a_offsets, const void* d_a_keys, const uint32_t* d_a_idx,
+                                  uint64_t n_a, uint64_t n_buckets, uint64_t bucket_lo, uint64_t bucket_hi,
+                                  int key_bytes, const void* d_query, uint64_t nq, const uint32_t* d_query_idx,
+                                  uint32_t* d_pairs, uint64_t pair_cap, unsigned long long* d_count,
+                                  void* d_workspace, size_t workspace_bytes, hg_stream_t stream);
+/* Internal: the same with an explicit path (-1 = planner's choice). */
+hg_status hg_shard_build_into_path(const void* d_keys, const uint32_t* d_key_idx, uint64_t n, int key_bytes,
+                                   uint64_t n_buckets, uint64_t bucket_lo, uint64_t bucket_hi,
+                                   uint32_t* d_offsets, void* d_keys_out, uint32_t* d_idx_out,
+                                   void* d_workspace, size_t workspace_bytes, int path, hg_stream_t stream);
+hg_status hg_shard_intersect_into_path(const uint32_t* d_a_offsets, const void* d_a_keys,
+                                       const uint32_t* d_a_idx, uint64_t n_a, uint64_t n_buckets,
+                                       uint64_t bucket_lo, uint64_t bucket_hi, int key_bytes,
+                                       const void* d_query, uint64_t nq, const uint32_t* d_query_idx,
+                                       uint32_t* d_pairs, uint64_t pair_cap, unsigned long long* d_count,
+                                       void* d_workspace, size_t workspace_bytes, int path,
+                                       hg_stream_t stream);
+
+/* ------------------------------------------------------------------------
  * Serving engine (no counterpart in the reference, whose tables are built
  * and intersected once per process): resident tables under a device-memory
  * budget and a table limit, evicted least recently used first; requests

@@ -162,3 +162,30 @@ def test_server_argument_checks_without_device(capi):
     L.hg_server_free(None)
     t0 = L.hg_server_now()
     assert t0 > 0 and L.hg_server_now() >= t0
+
+
+def test_shard_argument_checks_without_device(capi):
+    """hg_shard_* check ranges and splits before any device call."""
+    L = capi.lib()
+    f = 16  # a stand-in device pointer: no call below reaches the device
+    out = ctypes.c_size_t(0)
+    # lo >= hi, hi > B, an unaligned range of a 2^32-bucket table, key width
+    assert L.hg_shard_build_into(f, None, 4, 8, 100, 50, 50, f, f, None, f, 1 << 20, None) == -1
+    assert L.hg_shard_build_into(f, None, 4, 8, 100, 50, 101, f, f, None, f, 1 << 20, None) == -1
+    assert L.hg_shard_build_into(f, None, 4, 8, 1 << 32, 3, 1 << 20, f, f, None, f, 1 << 20, None) == -6
+    assert L.hg_shard_build_into(f, None, 4, 5, 100, 0, 50, f, f, None, f, 1 << 20, None) == -8
+    assert L.hg_shard_intersect_into(f, f, None, 4, 100, 60, 40, 8, f, 4, None, None, 0, f, f, 1 << 20, None) == -1
+    # splits that do not start at 0 / end at B, or that decrease
+    for bad in ([0, 60, 50, 100], [1, 50, 70, 100], [0, 50, 70, 99]):
+        sp = np.array(bad, dtype=np.uint64)
+        assert L.hg_shard_route(f, 4, 8, 100, sp.ctypes.data_as(ctypes.c_void_p), 3, 0, f, None, f, f,
+                                1 << 20, None) == -1
+    sp = np.array([0, 100], dtype=np.uint64)
+    assert L.hg_shard_route(f, 4, 8, 100, sp.ctypes.data_as(ctypes.c_void_p), 0, 0, f, None, f, f, 1 << 20, None) == -1
+    # global indices past 2^32
+    assert L.hg_shard_route(f, 4, 8, 100, sp.ctypes.data_as(ctypes.c_void_p), 1, (1 << 32) - 2, f, f, f, f,
+                            1 << 20, None) == -6
+    assert L.hg_shard_route_workspace_size(1000, 65, ctypes.byref(out)) == -1
+    assert L.hg_shard_route_workspace_size(1000, 8, ctypes.byref(out)) == 0 and out.value > 0
+    assert L.hg_shard_histogram(f, 10, 8, 100, 40000, f, None) == -6
+    assert L.hg_shard_histogram(f, 10, 8, 0, 16, f, None) == -1

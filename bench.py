@@ -673,6 +673,94 @@ def run_serving(args, rank, world, local):
 
 
 # ---------------------------------------------------------------------------
+# sharded: one table over all ranks by bucket range (hashgraph_b200.shard)
+# ---------------------------------------------------------------------------
+def run_sharded(args, rank, world, local):
+    """Each rank holds n u64 keys and n queries (25% drawn from its keys); one
+    step = ShardedTable.build over all ranks' keys into n * world buckets
+    (histogram, all-reduce, splits, route, all-to-all, shard build) + the
+    intersect of all ranks' queries (route, all-to-all, shard probe with
+    pairs, all-reduce of the count).  With one rank the all-to-alls move the
+    routed keys to the rank itself; the collectives are NCCL."""
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    import hashgraph_b200 as hg
+    from hashgraph_b200.shard import ShardedTable
+
+    dev = torch.device("cuda", local)
+    own_group = False
+    if not dist.is_initialized():
+        sk = socket.socket()
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+        sk.close()
+        dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                                device_id=dev)
+        own_group = True
+    try:
+        kb = 8
+        n = args.n or (1 << 28)
+        B = n * world
+        a = hg.gen_uniform(n, kb, 3 + 1000 * rank, device=dev)
+        q = hg.gen_overlap(n, a, 0.25, 4 + 1000 * rank)
+        torch.cuda.synchronize(dev)
+
+        def step():
+            t = ShardedTable.build(a, B, with_index=True)
+            return t, t.intersect(q)
+
+        for _ in range(args.warmup):
+            t, r = step()
+        torch.cuda.synchronize(dev)
+        matches = r.count
+        if world == 1:  # the one-shard table against the plain path
+            plain = hg.Table.build(a, B, with_index=True)
+            c, _ = plain.intersect(q, emit=False)
+            if int(c.item()) != matches:
+                raise RuntimeError(f"sharded count {matches} != plain count {int(c.item())}")
+            del plain
+        del t, r
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        clocks = ClockSampler(local)
+        launches0 = hg.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clocks.start()
+        e0.record()
+        for _ in range(args.steps):
+            t, r = step()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        clk = clocks.stop()
+        launches = hg.launch_count() - launches0
+        barrier(world)
+        ms = max_over_ranks(e0.elapsed_time(e1), world) / args.steps
+        value = sum_over_ranks(n, world) / (ms * 1e-3)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded splitmix64 keys generated on each rank's device)",
+            "config": {"workload": f"sharded: {n} u64 keys + {n} queries (25% overlap) per rank, one table of "
+                                   f"{B} buckets over {world} rank(s) by bucket range, index + pairs",
+                       "keys_per_rank": n, "n_buckets": B, "matches": matches, "splits": t.splits,
+                       "parallelism": f"{world} shard(s), NCCL all-to-all",
+                       "l2": "inputs larger than L2; no flush"},
+            "clocks": clk, "e2e": None, "gpu_launches": launches, "cpu_baseline": None,
+            "note": "device time of whole steps (CUDA events), max over ranks; includes the host reads of the "
+                    "route and exchange sizes each step",
+        }
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+    finally:
+        if own_group:
+            dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
 # CPU baseline / reference arm
 # ---------------------------------------------------------------------------
 def cpu_run(workload, n_sample, repeats=3):
@@ -800,6 +888,8 @@ def run_reference(args, rank, world):
     if args.workload == "serving":
         run_reference_serving(args)
         return
+    if args.workload == "sharded":  # the same per-rank work on one host: build + probe of 2^28 u64
+        args.workload = "large"
     import oracle
     kb, n, bfn, kind, seed_a, seed_q, overlap, with_index = WORKLOADS[args.workload]
     n = args.n or n
@@ -835,7 +925,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "serving"], default="large")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "serving", "sharded"], default="large")
     ap.add_argument("--requests", type=int, default=3000, help="requests of the serving workload")
     ap.add_argument("--rate", type=float, default=20000.0, help="serving arrivals per second")
     ap.add_argument("--streams", type=int, default=4, help="serving CUDA streams")
@@ -859,6 +949,8 @@ def main():
             run_batched(args, rank, world, local)
         elif args.workload == "serving":
             run_serving(args, rank, world, local)
+        elif args.workload == "sharded":
+            run_sharded(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

@@ -2,12 +2,17 @@
 // (alokpathy/hashgraph test/MultiHashGraphTest.cu:130-427) rewritten over the
 // drop-in classes: same positional arguments
 //   multi-hash size maxkey binCount gpuCount lrbBins check|nocheck countSizeB build|intersect
-// same inputs (sequential keys A = 0..size-1, B = 0..countSizeB-1), same
-// timed regions (CUDA events around build, and around build A + build B +
+// same inputs (sequential keys A = 0..size-1, B = 0..countSizeB-1, each cut
+// into gpuCount contiguous chunks of ceil(size / gpuCount), chunk t on GPU t),
+// the same OpenMP team of gpuCount threads calling build(true, tid), B's
+// build(false, tid) on A's splits and intersect(..., tid), the same timed
+// regions (CUDA events around build, and around build A + build B +
 // intersect) and the same "multi ... time:" lines.  With `check` the build is
-// cross-checked by buildSingle() and the intersect output against a CPU
-// multiset join; unlike the reference, a mismatch exits with status 1.
+// cross-checked by buildSingle() and the intersect output (every GPU's)
+// against a CPU multiset join; unlike the reference, a mismatch exits with
+// status 1.  With fewer devices than gpuCount, GPU t is device t % count.
 #include <cuda_runtime.h>
+#include <omp.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -17,13 +22,35 @@
 
 #include "hashgraph_b200/MultiHashGraph.h"
 
-static void generate_input(inputData* d, index_t count) {
-  std::vector<hkey_t> h(static_cast<size_t>(count));
-  for (index_t j = 0; j < count; j++) h[j] = static_cast<hkey_t>(j);
-  cudaMalloc(&d->d_keys, (count ? count : 1) * sizeof(hkey_t));
-  cudaMalloc(&d->d_hash, (count ? count : 1) * sizeof(HashKey));
-  cudaMemcpy(d->d_keys, h.data(), count * sizeof(hkey_t), cudaMemcpyHostToDevice);
-  d->len = count;
+static int device_of(index_t t) {
+  int nd = 1;
+  cudaGetDeviceCount(&nd);
+  return static_cast<int>(t % nd);
+}
+
+// keys 0..count-1, chunk t = [ceil(count/G) * t, ...) on GPU t
+static void generate_input(inputData* d, index_t count, index_t gpuCount) {
+  const index_t avg = (count + gpuCount - 1) / gpuCount;
+  for (index_t t = 0; t < gpuCount; t++) {
+    const index_t lo = std::min(avg * t, count), hi = std::min(avg * (t + 1), count);
+    std::vector<hkey_t> h(static_cast<size_t>(hi - lo));
+    for (index_t j = lo; j < hi; j++) h[j - lo] = static_cast<hkey_t>(j);
+    cudaSetDevice(device_of(t));
+    cudaMalloc(&d[t].d_keys, (hi > lo ? hi - lo : 1) * sizeof(hkey_t));
+    cudaMalloc(&d[t].d_hash, (hi > lo ? hi - lo : 1) * sizeof(HashKey));
+    cudaMemcpy(d[t].d_keys, h.data(), (hi - lo) * sizeof(hkey_t), cudaMemcpyHostToDevice);
+    d[t].len = hi - lo;
+  }
+  cudaSetDevice(0);
+}
+
+static void free_input(inputData* d, index_t gpuCount) {
+  for (index_t t = 0; t < gpuCount; t++) {
+    cudaSetDevice(device_of(t));
+    cudaFree(d[t].d_keys);
+    cudaFree(d[t].d_hash);
+  }
+  cudaSetDevice(0);
 }
 
 int main(int argc, char** argv) {
@@ -49,31 +76,50 @@ int main(int argc, char** argv) {
   cudaEventCreate(&start);
   cudaEventCreate(&stop);
   float ms = 0.f;
+  if (gpuCount < 1 || gpuCount > HG_MAX_SHARDS) {
+    std::fprintf(stderr, "gpuCount must be 1..64\n");
+    return 1;
+  }
   try {
     if (buildTest) {
-      inputData in[1];
-      generate_input(in, countSizeA);
-      MultiHashGraph mhg(in, countSizeA, maxkey, tableSize, binCount, lrbBins, gpuCount);
+      std::vector<inputData> in(gpuCount);
+      generate_input(in.data(), countSizeA, gpuCount);
+      MultiHashGraph mhg(in.data(), countSizeA, maxkey, tableSize, binCount, lrbBins, gpuCount);
       cudaEventRecord(start);
-      mhg.build(true, 0);
+#pragma omp parallel num_threads(gpuCount)
+      {
+        const index_t tid = omp_get_thread_num();
+        mhg.build(true, tid);
+      }
+      cudaSetDevice(0);
       cudaEventRecord(stop);
       cudaEventSynchronize(stop);
       cudaEventElapsedTime(&ms, start, stop);
       std::printf("multi buildTable() time: %g\n", ms / 1000.0);
       if (check) mhg.buildSingle();
+      free_input(in.data(), gpuCount);
       return 0;
     }
-    inputData inA[1], inB[1];
-    generate_input(inA, countSizeA);
-    generate_input(inB, countSizeB);
-    MultiHashGraph mhgA(inA, countSizeA, maxkey, tableSize, binCount, lrbBins, gpuCount);
-    MultiHashGraph mhgB(inB, countSizeB, maxkey, tableSize, binCount, lrbBins, gpuCount);
-    keypair* h_dOutput[1] = {nullptr};
-    index_t h_Common[1] = {0};
+    std::vector<inputData> inA(gpuCount), inB(gpuCount);
+    generate_input(inA.data(), countSizeA, gpuCount);
+    generate_input(inB.data(), countSizeB, gpuCount);
+    MultiHashGraph mhgA(inA.data(), countSizeA, maxkey, tableSize, binCount, lrbBins, gpuCount);
+    MultiHashGraph mhgB(inB.data(), countSizeB, maxkey, tableSize, binCount, lrbBins, gpuCount);
+    std::vector<keypair*> h_dOutput(gpuCount, nullptr);
+    std::vector<index_t> h_Common(gpuCount, 0);
     cudaEventRecord(start);
-    mhgA.build(true, 0);
-    mhgB.build(false, 0);
-    MultiHashGraph::intersect(mhgA, mhgB, h_Common, h_dOutput, 0);
+#pragma omp parallel num_threads(gpuCount)
+    {
+      const index_t tid = omp_get_thread_num();
+      mhgA.build(true, tid);
+#pragma omp master
+      mhgB.h_binSplits = mhgA.h_binSplits;  // B on A's splits
+#pragma omp barrier
+      mhgB.build(false, tid);
+#pragma omp barrier
+      MultiHashGraph::intersect(mhgA, mhgB, h_Common.data(), h_dOutput.data(), tid);
+    }
+    cudaSetDevice(0);
     cudaEventRecord(stop);
     cudaEventSynchronize(stop);
     cudaEventElapsedTime(&ms, start, stop);
@@ -81,10 +127,16 @@ int main(int argc, char** argv) {
     if (check) {
       mhgA.buildSingle();
       mhgB.buildSingle();
-      std::vector<keypair> out(static_cast<size_t>(h_Common[0]));
-      if (h_Common[0]) cudaMemcpy(out.data(), h_dOutput[0], out.size() * sizeof(keypair), cudaMemcpyDeviceToHost);
       std::vector<hkey_t> result;
-      for (const keypair& p : out) result.push_back(static_cast<hkey_t>(p.right));
+      index_t total = 0;
+      for (index_t t = 0; t < gpuCount; t++) {
+        std::vector<keypair> out(static_cast<size_t>(h_Common[t]));
+        cudaSetDevice(device_of(t));
+        if (h_Common[t]) cudaMemcpy(out.data(), h_dOutput[t], out.size() * sizeof(keypair), cudaMemcpyDeviceToHost);
+        for (const keypair& p : out) result.push_back(static_cast<hkey_t>(p.right));
+        total += h_Common[t];
+      }
+      cudaSetDevice(0);
       std::vector<hkey_t> a(mhgA.h_vals, mhgA.h_vals + countSizeA), b(mhgB.h_vals, mhgB.h_vals + countSizeB);
       std::sort(a.begin(), a.end());
       std::sort(b.begin(), b.end());
@@ -110,9 +162,15 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "ERROR: INTERSECT OUTPUT HAS INCORRECT CONTENT\n");
         return 1;
       }
-      std::printf("intersect check ok: %lld matches\n", static_cast<long long>(h_Common[0]));
+      std::printf("intersect check ok: %lld matches\n", static_cast<long long>(total));
     }
-    cudaFree(h_dOutput[0]);
+    for (index_t t = 0; t < gpuCount; t++) {
+      cudaSetDevice(device_of(t));
+      cudaFree(h_dOutput[t]);
+    }
+    cudaSetDevice(0);
+    free_input(inA.data(), gpuCount);
+    free_input(inB.data(), gpuCount);
   } catch (const hg::Error& e) {
     std::fprintf(stderr, "%s\n", e.what());
     return 2;

@@ -319,40 +319,36 @@ def run_ours(args, rank, world, local):
     step_s = total_ms / args.steps * 1e-3
     value = sum_over_ranks(n * args.steps, world) / (total_ms_max * 1e-3)
 
-    # ---- end to end through the public API from pinned host buffers
+    # ---- end to end through the public API from pinned host buffers: every
+    # step uploads its keys and queries, builds, probes and downloads the count
+    # and the pairs; HostPipeline overlaps step k+1's upload with step k's
+    # build + probe and step k-1's download
     e2e = None
     if not args.skip_e2e:
+        from hashgraph_b200.pipeline import HostPipeline
         h_a = torch.empty(a_keys.shape, dtype=a_keys.dtype, pin_memory=True)
         h_q = torch.empty(q_keys.shape, dtype=q_keys.dtype, pin_memory=True)
         h_a.copy_(a_keys)
         h_q.copy_(q_keys)
-        h_count = torch.empty(1, dtype=torch.int64, pin_memory=True)
         h_pairs = torch.empty((max(pair_cap, 1), 2), dtype=torch.int32, pin_memory=True) if emit else None
-        d_a = torch.empty_like(a_keys)
-        d_q = torch.empty_like(q_keys)
-        d2h = 0
+        del table, ws, pairs
+        pipe = HostPipeline(n, nq, B, key_bytes=kb, with_index=with_index, emit=emit, pair_cap=pair_cap,
+                            device=dev, build_path=build_path, probe_path=probe_path)
+        pipe.run([(h_a, h_q)], [h_pairs])  # warm-up
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier(world)
         torch.cuda.synchronize(dev)
-        e0.record(stream)
-        for _ in range(args.steps):
-            d_a.copy_(h_a, non_blocking=True)
-            d_q.copy_(h_q, non_blocking=True)
-            step(d_a, d_q)
-            h_count.copy_(count, non_blocking=True)
-            stream.synchronize()
-            c = int(h_count.item())
-            d2h += 8
-            if emit and c:
-                h_pairs[:c].copy_(pairs[:c], non_blocking=True)
-                d2h += c * 8
-        e1.record(stream)
+        counts = pipe.run([(h_a, h_q)] * args.steps, [h_pairs] * args.steps, start_event=e0, end_event=e1)
         torch.cuda.synchronize(dev)
+        if any(c != n_matches for c in counts):
+            raise RuntimeError(f"end-to-end counts {set(counts)} != {n_matches}")
+        d2h = sum(8 + (8 * min(c, pair_cap) if emit else 0) for c in counts)
         e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
         e2e = {"value": sum_over_ranks(n * args.steps, world) / (e2e_ms * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": int(a_keys.numel() * kb + q_keys.numel() * kb),
-               "d2h_bytes_per_step": int(d2h // args.steps)}
-        del h_a, h_q, h_pairs, d_a, d_q
+               "d2h_bytes_per_step": int(d2h // args.steps),
+               "api": "hashgraph_b200.pipeline.HostPipeline (hg_build_into + hg_intersect_into on its streams)"}
+        del h_a, h_q, h_pairs, pipe
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:

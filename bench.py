@@ -724,6 +724,8 @@ def run_sharded(args, rank, world, local):
         clocks = ClockSampler(local)
         launches0 = hg.launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        hg.profile_enable(True)
+        hg.profile_read()
         clocks.start()
         e0.record()
         for _ in range(args.steps):
@@ -731,6 +733,10 @@ def run_sharded(args, rank, world, local):
         e1.record()
         torch.cuda.synchronize(dev)
         clk = clocks.stop()
+        phases = {}
+        for name, pms in hg.profile_read():
+            phases[name] = phases.get(name, 0.0) + pms / args.steps
+        hg.profile_enable(False)
         launches = hg.launch_count() - launches0
         barrier(world)
         ms = max_over_ranks(e0.elapsed_time(e1), world) / args.steps
@@ -745,9 +751,11 @@ def run_sharded(args, rank, world, local):
                        "keys_per_rank": n, "n_buckets": B, "matches": matches, "splits": t.splits,
                        "parallelism": f"{world} shard(s), NCCL all-to-all",
                        "l2": "inputs larger than L2; no flush"},
+            "phases_ms": phases, "library_ms": sum(phases.values()),
             "clocks": clk, "e2e": None, "gpu_launches": launches, "cpu_baseline": None,
             "note": "device time of whole steps (CUDA events), max over ranks; includes the host reads of the "
-                    "route and exchange sizes each step",
+                    "route and exchange sizes each step; phases_ms: the library's kernels per step (the rest "
+                    "is the collectives and the host round trips)",
         }
         if rank == 0:
             print(json.dumps(out), flush=True)

@@ -100,7 +100,8 @@ __global__ void __launch_bounds__(256) k_count(const KeyT* __restrict__ keys, ui
 template <typename KeyT, int V, bool WITH_IDX>
 __global__ void __launch_bounds__(256) k_scatter(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
                                                  uint32_t* __restrict__ cursor, KeyT* __restrict__ keys_out,
-                                                 uint32_t* __restrict__ idx_out, const uint32_t* gate) {
+                                                 uint32_t* __restrict__ idx_out, const uint32_t* __restrict__ key_idx,
+                                                 const uint32_t* gate) {
   if (gated_off(gate)) return;
   const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
   const uint64_t nchunks = (n + 32ull * V - 1) / (32ull * V);
@@ -115,7 +116,10 @@ __global__ void __launch_bounds__(256) k_scatter(const KeyT* __restrict__ keys, 
       const uint32_t pos = warp_aggregated_inc(cursor, bm.of_key(k[j]), ok[j]);
       if (ok[j]) {
         keys_out[pos] = k[j];
-        if constexpr (WITH_IDX) idx_out[pos] = static_cast<uint32_t>(base + lane_id() * V + j);
+        if constexpr (WITH_IDX) {
+          const uint64_t i = base + lane_id() * V + j;
+          idx_out[pos] = key_idx ? key_idx[i] : static_cast<uint32_t>(i);
+        }
       }
     }
   }
@@ -765,13 +769,13 @@ static void launch_direct_count(const KeyT* keys, uint64_t n, BucketMap bm, uint
 
 template <typename KeyT, int V, bool WI>
 static void launch_direct_scatter(const KeyT* keys, uint64_t n, BucketMap bm, uint32_t* cursor, KeyT* out,
-                                  uint32_t* idx, const uint32_t* gate, cudaStream_t s) {
+                                  uint32_t* idx, const uint32_t* key_idx, const uint32_t* gate, cudaStream_t s) {
   const uint64_t chunks = (n + 32ull * V - 1) / (32ull * V);
   const uint64_t want = (chunks + 7) / 8;
   const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(want, uint64_t(device_sm_count()) * 8)));
   Phase ph(s, gate ? "fallback_scatter" : "scatter");
   count_launch();
-  k_scatter<KeyT, V, WI><<<grid, 256, 0, s>>>(keys, n, bm, cursor, out, idx, gate);
+  k_scatter<KeyT, V, WI><<<grid, 256, 0, s>>>(keys, n, bm, cursor, out, idx, key_idx, gate);
 }
 
 static void launch_scan(uint32_t* data, uint64_t count, uint64_t* status, unsigned* ticket, uint32_t* first_slot,
@@ -802,7 +806,7 @@ static hg_status run_direct(const BuildPlan& p, const KeyT* keys, uint32_t* offs
   HG_CUDA(cudaMemsetAsync(ws + p.off_status, 0, p.off_flags - p.off_status, s), "build: scan state memset");
   if (p.n > 0) launch_direct_count<KeyT, V>(keys, p.n, bm, offsets + 1, gate, s);
   launch_scan(offsets + 1, p.n_buckets, status, ticket, offsets, nullptr, gate, s);
-  if (p.n > 0) launch_direct_scatter<KeyT, V, WI>(keys, p.n, bm, offsets + 1, keys_out, idx_out, gate, s);
+  if (p.n > 0) launch_direct_scatter<KeyT, V, WI>(keys, p.n, bm, offsets + 1, keys_out, idx_out, p.key_idx, gate, s);
   return HG_OK;
 }
 
@@ -1045,7 +1049,7 @@ static hg_status run_partitioned(const BuildPlan& p, const KeyT* keys, uint32_t*
   uint32_t* flags = reinterpret_cast<uint32_t*>(ws + p.off_flags);
   // status words, tickets, flags, partition counts and their scan states
   HG_CUDA(cudaMemsetAsync(ws + p.off_status, 0, p.off_pkeys - p.off_status, s), "build: workspace memset");
-  hg_status st = run_partition_passes<KeyT, V, WI>(g, p.n, keys, nullptr, bm, ws, p.off_flags, p.off_ticket,
+  hg_status st = run_partition_passes<KeyT, V, WI>(g, p.n, keys, p.key_idx, bm, ws, p.off_flags, p.off_ticket,
                                                    p.off_pcount, p.off_pstatus, p.off_fcount, p.off_fstatus,
                                                    p.off_pkeys, p.off_pidx, p.off_fkeys, p.off_fidx, "build", s);
   if (st != HG_OK) return st;

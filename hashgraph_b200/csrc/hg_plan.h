@@ -60,6 +60,9 @@ struct BuildPlan {
   }
   int key_bytes = 8;
   bool with_index = false;
+  // with an index: the indices to store for the input keys (input key i gets
+  // key_idx[i]); NULL stores the input position i
+  const uint32_t* key_idx = nullptr;
   uint64_t scan_tiles = 0;  // direct path: in-place scan over offsets[1..B]
   PartGeometry g;           // partitioned path
   // workspace byte offsets

@@ -21,8 +21,8 @@
 //                        inside each group, each with its global index
 //                        (index_base + position) -- deterministic.
 //   hg_shard_build_into  the ordinary build under the range's bucket map
-//                        (no hash array, no decrHash pass), then the carried
-//                        global indices gathered into the table's index.
+//                        (no hash array, no decrHash pass), storing the
+//                        carried global indices as the table's index.
 //   hg_shard_intersect_into  the ordinary probe under the range's bucket map.
 #include <algorithm>
 #include <vector>
@@ -55,18 +55,38 @@ __device__ __forceinline__ int shard_of(uint32_t b, const uint64_t* s, int G) {
   return lo;
 }
 
+// Bin of a bucket: bucket / width with c = ceil(2^64 / width), exact for
+// 32-bit buckets and widths (Lemire, Kaser & Kurz, "Faster remainder by
+// direct computation", 2019: 64 fraction bits cover 32-bit operands);
+// width 1 (c would not fit) is the bucket itself.
+__device__ __forceinline__ uint32_t bin_of(uint32_t bucket, uint64_t c) {
+  return c ? static_cast<uint32_t>(__umul64hi(c, bucket)) : bucket;
+}
+
+constexpr int HIST_BLOCK = 256, HIST_V = 8;
+
 template <typename KeyT>
-__global__ void __launch_bounds__(256) k_shard_hist(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
-                                                    uint32_t bin_width, uint32_t n_bins,
-                                                    unsigned long long* __restrict__ bins) {
+__global__ void __launch_bounds__(HIST_BLOCK) k_shard_hist(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
+                                                           uint64_t bin_magic, uint32_t n_bins,
+                                                           unsigned long long* __restrict__ bins) {
   extern __shared__ uint32_t s_bin[];
-  for (uint32_t i = threadIdx.x; i < n_bins; i += blockDim.x) s_bin[i] = 0;
+  for (uint32_t i = threadIdx.x; i < n_bins; i += HIST_BLOCK) s_bin[i] = 0;
   __syncthreads();
-  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
-    atomicAdd(&s_bin[bm.of_key(keys[i]) / bin_width], 1u);
+  // HIST_V keys per thread per round, each load coalesced across the block
+  constexpr uint64_t CH = uint64_t(HIST_BLOCK) * HIST_V;
+  for (uint64_t base = uint64_t(blockIdx.x) * CH; base < n; base += uint64_t(gridDim.x) * CH) {
+    KeyT k[HIST_V];
+#pragma unroll
+    for (int j = 0; j < HIST_V; j++) {
+      const uint64_t i = base + uint64_t(j) * HIST_BLOCK + threadIdx.x;
+      k[j] = i < n ? __ldcs(keys + i) : KeyT(0);
+    }
+#pragma unroll
+    for (int j = 0; j < HIST_V; j++)
+      if (base + uint64_t(j) * HIST_BLOCK + threadIdx.x < n) atomicAdd(&s_bin[bin_of(bm.of_key(k[j]), bin_magic)], 1u);
+  }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < n_bins; i += blockDim.x)
+  for (uint32_t i = threadIdx.x; i < n_bins; i += HIST_BLOCK)
     if (s_bin[i]) atomicAdd(bins + i, static_cast<unsigned long long>(s_bin[i]));
 }
 
@@ -97,7 +117,7 @@ __device__ __forceinline__ void route_count_warp(const int (&d)[ROUTE_V], uint32
 
 // tile_counts[r * tiles + t] = keys of tile t bound for shard r.
 template <typename KeyT>
-__global__ void __launch_bounds__(ROUTE_BLOCK) k_route_count(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
+__global__ void __launch_bounds__(ROUTE_BLOCK, 4) k_route_count(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
                                                              ShardSplits splits, int G,
                                                              uint32_t* __restrict__ tile_counts, uint64_t tiles) {
   __shared__ uint64_t s_split[SHARD_MAX + 1];
@@ -124,7 +144,7 @@ __global__ void __launch_bounds__(ROUTE_BLOCK) k_route_count(const KeyT* __restr
 // knows where its keys start; each warp adds the counts of the warps before
 // it and writes its keys in order.
 template <typename KeyT, bool WITH_IDX>
-__global__ void __launch_bounds__(ROUTE_BLOCK) k_route_scatter(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
+__global__ void __launch_bounds__(ROUTE_BLOCK, 4) k_route_scatter(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
                                                                ShardSplits splits, int G,
                                                                const uint32_t* __restrict__ tile_start, uint64_t tiles,
                                                                KeyT* __restrict__ keys_out,
@@ -174,13 +194,6 @@ __global__ void k_route_offsets(const uint32_t* __restrict__ tile_start, uint64_
   const int r = threadIdx.x;
   if (r < G) offsets[r] = tiles ? tile_start[uint64_t(r) * tiles] : 0ull;
   if (r == G) offsets[r] = n;
-}
-
-// idx[j] = carried[idx[j]]: the table's index held positions in the routed
-// array; the shard's index holds the keys' global positions.
-__global__ void k_gather_index(uint32_t* __restrict__ idx, const uint32_t* __restrict__ carried, uint64_t n) {
-  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) idx[i] = carried[idx[i]];
 }
 
 static int max_dyn_smem_set(const void* kern, size_t bytes) {
@@ -238,18 +251,22 @@ extern "C" hg_status hg_shard_histogram(const void* d_keys, uint64_t n, int key_
   if (n == 0) return HG_OK;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const BucketMap bm = BucketMap::make(n_buckets);
-  const uint32_t width = static_cast<uint32_t>((n_buckets + n_bins - 1) / n_bins);
+  const uint64_t width = (n_buckets + n_bins - 1) / n_bins;
+  // ceil(2^64 / width) for width >= 2; 0 marks width 1
+  const uint64_t magic = width == 1 ? 0ull : UINT64_MAX / width + 1;
   const size_t smem = size_t(n_bins) * 4;
-  const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((n + 4095) / 4096,
-                                                                            uint64_t(device_sm_count()) * 4)));
+  const uint64_t chunks = (n + uint64_t(HIST_BLOCK) * HIST_V - 1) / (uint64_t(HIST_BLOCK) * HIST_V);
+  const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(chunks, uint64_t(device_sm_count()) * 8)));
   Phase ph(s, "shard_histogram");
   count_launch();
   if (key_bytes == 8) {
     if (smem > 48 * 1024) max_dyn_smem_set(reinterpret_cast<const void*>(k_shard_hist<uint64_t>), smem);
-    k_shard_hist<uint64_t><<<grid, 256, smem, s>>>(static_cast<const uint64_t*>(d_keys), n, bm, width, n_bins, d_bins);
+    k_shard_hist<uint64_t><<<grid, HIST_BLOCK, smem, s>>>(static_cast<const uint64_t*>(d_keys), n, bm, magic, n_bins,
+                                                         d_bins);
   } else {
     if (smem > 48 * 1024) max_dyn_smem_set(reinterpret_cast<const void*>(k_shard_hist<uint32_t>), smem);
-    k_shard_hist<uint32_t><<<grid, 256, smem, s>>>(static_cast<const uint32_t*>(d_keys), n, bm, width, n_bins, d_bins);
+    k_shard_hist<uint32_t><<<grid, HIST_BLOCK, smem, s>>>(static_cast<const uint32_t*>(d_keys), n, bm, magic, n_bins,
+                                                         d_bins);
   }
   HG_CUDA(cudaPeekAtLastError(), "hg_shard_histogram");
   return HG_OK;
@@ -370,15 +387,9 @@ extern "C" hg_status hg_shard_build_into_path(const void* d_keys, const uint32_t
   if (workspace_bytes < plan.total) return HG_ERR_TOO_LARGE;
   plan.range_total = n_buckets;
   plan.range_lo = bucket_lo;
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  st = launch_build(plan, d_keys, d_offsets, d_keys_out, d_idx_out, d_workspace, s);
-  if (st != HG_OK || !d_idx_out || !d_key_idx || n == 0) return st;
-  Phase ph(s, "shard_gather_index");
-  count_launch();
-  const int grid = static_cast<int>(std::min<uint64_t>((n + 255) / 256, uint64_t(device_sm_count()) * 8));
-  k_gather_index<<<grid, 256, 0, s>>>(d_idx_out, d_key_idx, n);
-  HG_CUDA(cudaPeekAtLastError(), "hg_shard_build_into: gather");
-  return HG_OK;
+  plan.key_idx = d_key_idx;  // the partition passes (or the direct scatter) store the carried indices
+  return launch_build(plan, d_keys, d_offsets, d_keys_out, d_idx_out, d_workspace,
+                      reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" hg_status hg_shard_build_into(const void* d_keys, const uint32_t* d_key_idx, uint64_t n, int key_bytes,

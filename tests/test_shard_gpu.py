@@ -54,7 +54,7 @@ def test_route_matches_stable_partition(hg, kb, n, G):
 def test_histogram_matches_bincount(hg, n_bins):
     from hashgraph_b200.shard import DeviceShardOps
     k = oracle.gen_uniform(300_000, 8, 77)
-    for B in (1 << 22, 999_983):
+    for B in (1 << 22, 999_983, 1000):  # 1000 < n_bins: bin width 1
         got = DeviceShardOps().histogram(from_np_u(k), B, n_bins).cpu().numpy()
         ref = CpuShardOps().histogram(_from_np(k), B, n_bins).numpy()
         np.testing.assert_array_equal(got, ref)

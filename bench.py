@@ -118,7 +118,8 @@ class ClockSampler:
 # processed, so a full launch's traffic is this figure times its keys.
 MEASURED_TRAFFIC_PER_KEY = {
     (8, False): {"multisplit": 14.5, "split": 14.4, "fine_build": 18.5,
-                 "probe_multisplit": 18.3, "probe_split": 22.4, "fine_probe_emit": 25.8},
+                 "probe_multisplit": 18.3, "probe_split": 22.4, "fine_probe_emit": 25.8,
+                 "coarse_probe_emit": 25.8},
 }
 
 
@@ -213,6 +214,10 @@ def algorithmic_bytes(phase, kb, n, nq, B, with_index, pairs):
         "probe_split": 2 * nq * qrec,
         "fine_probe_emit": nq * qrec + n * rec + 4 * (B + 1) + 8 * pairs,
         "fine_probe_count": nq * qrec + n * rec + 4 * (B + 1),
+        # the coarse probe reads every query record once, the table once (each
+        # bucket range's slice comes from HBM into L2 once) and writes the pairs
+        "coarse_probe_emit": nq * qrec + n * rec + 4 * (B + 1) + 8 * pairs,
+        "coarse_probe_count": nq * qrec + n * rec + 4 * (B + 1),
         "probe_emit": nq * kb + n * rec + 4 * (B + 1) + 8 * pairs,
         "probe_count": nq * kb + n * rec + 4 * (B + 1),
     }.get(phase)

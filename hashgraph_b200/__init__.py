@@ -18,11 +18,12 @@ from ._capi import (ERR_DEVICE_TIMEOUT, ERR_PAIR_CAPACITY, BatchPair, HGError, b
 __all__ = [
     "HGError", "Table", "build_library", "lib", "hash_keys", "intersect", "device_error",
     "gen_uniform", "gen_overlap", "gen_zipf", "zipf_cdf", "PATH_AUTO", "PATH_DIRECT",
-    "PATH_PARTITIONED", "ERR_PAIR_CAPACITY", "ERR_DEVICE_TIMEOUT", "status_str",
+    "PATH_PARTITIONED", "PATH_COARSE", "ERR_PAIR_CAPACITY", "ERR_DEVICE_TIMEOUT", "status_str",
     "profile_enable", "profile_read", "launch_count", "Batch",
 ]
 
 PATH_AUTO, PATH_DIRECT, PATH_PARTITIONED = -1, 0, 1
+PATH_COARSE = 2  # probes only: queries grouped by L2-sized bucket ranges, probed from L2
 
 
 def _torch():

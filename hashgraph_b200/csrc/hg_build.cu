@@ -988,6 +988,28 @@ static int blocks_per_sm(Kern kern, unsigned block, size_t smem) {
   return n;
 }
 
+// Pass 1 over `n` streamed keys (with their input positions when WI): the
+// per-CTA multisplit into g.n_parts coarse partitions of 2^g.coarse_log2
+// buckets, record slots p * g.part_cap, counts in pcount[p].
+template <typename KeyT, int V, bool WI>
+static hg_status launch_pass1(const PartGeometry& g, uint64_t n, const KeyT* keys, const uint32_t* key_idx,
+                              BucketMap bm, uint32_t* pcount, KeyT* pkeys, uint32_t* pidx, uint32_t* flags,
+                              const char* name, cudaStream_t s) {
+  if (n == 0) return HG_OK;
+  auto kern = k_multisplit<KeyT, WI, PASS1_BLOCK, PASS1_KPT, (V > 1), TableTiles<KeyT, PASS1_TILE>>;
+  const int bps = blocks_per_sm(kern, PASS1_BLOCK, g.smem1);
+  if (bps <= 0) return lib_fail(HG_ERR_CUDA, "multisplit kernel cannot be resident");
+  const uint64_t ntiles = (n + PASS1_TILE - 1) / PASS1_TILE;
+  const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ntiles, uint64_t(device_sm_count()) * bps));
+  Phase ph(s, name);
+  count_launch();
+  using Src = TableTiles<KeyT, PASS1_TILE>;
+  const Src src{keys, key_idx, n, bm, g.coarse_log2, static_cast<uint32_t>(g.n_parts), g.part_cap, pcount, pkeys, pidx};
+  kern<<<grid, PASS1_BLOCK, g.smem1, s>>>(src, static_cast<uint32_t>(g.n_parts), flags);
+  HG_CUDA(cudaPeekAtLastError(), "multisplit launch");
+  return HG_OK;
+}
+
 // Passes 1 and 2 of a partitioned path over `n` streamed keys (with their
 // input positions when WI): cluster multisplit into coarse partitions, scan,
 // split into fine partitions, scan.  Shared by the build and the probe.
@@ -1007,19 +1029,9 @@ static hg_status run_partition_passes(const PartGeometry& g, uint64_t n, const K
   uint32_t* pidx = WI ? reinterpret_cast<uint32_t*>(ws + off_pidx) : nullptr;
   KeyT* fkeys = reinterpret_cast<KeyT*>(ws + off_fkeys);
   uint32_t* fidx = WI ? reinterpret_cast<uint32_t*>(ws + off_fidx) : nullptr;
-  if (n > 0) {
-    auto kern = k_multisplit<KeyT, WI, PASS1_BLOCK, PASS1_KPT, (V > 1), TableTiles<KeyT, PASS1_TILE>>;
-    const int bps = blocks_per_sm(kern, PASS1_BLOCK, g.smem1);
-    if (bps <= 0) return lib_fail(HG_ERR_CUDA, "multisplit kernel cannot be resident");
-    const uint64_t ntiles = (n + PASS1_TILE - 1) / PASS1_TILE;
-    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ntiles, uint64_t(device_sm_count()) * bps));
-    Phase ph(s, who[0] == 'b' ? "multisplit" : "probe_multisplit");
-    count_launch();
-    using Src = TableTiles<KeyT, PASS1_TILE>;
-    const Src src{keys, key_idx, n, bm, g.coarse_log2, static_cast<uint32_t>(g.n_parts), g.part_cap, pcount, pkeys, pidx};
-    kern<<<grid, PASS1_BLOCK, g.smem1, s>>>(src, static_cast<uint32_t>(g.n_parts), flags);
-    HG_CUDA(cudaPeekAtLastError(), "multisplit launch");
-  }
+  hg_status st = launch_pass1<KeyT, V, WI>(g, n, keys, key_idx, bm, pcount, pkeys, pidx, flags,
+                                          who[0] == 'b' ? "multisplit" : "probe_multisplit", s);
+  if (st != HG_OK) return st;
   launch_scan(pcount, g.n_parts, pstatus, ticket + 1, nullptr, pcount + g.n_parts, nullptr, s,
               who[0] == 'b' ? "part_scan" : "probe_part_scan");
   {

@@ -22,6 +22,8 @@ enum BuildPath : int { BUILD_DIRECT = 0, BUILD_PARTITIONED = 1 };
 constexpr size_t SMEM_BUDGET = 220 * 1024;  // dynamic shared memory per CTA (B200 opt-in max 227 KB)
 constexpr size_t FINE_SMEM_BUDGET = 100 * 1024;        // pass-3 build CTAs: two per SM (double-buffered)
 constexpr size_t FINE_PROBE_SMEM_BUDGET = 220 * 1024;  // pass-3 probe CTAs: one per SM (double-buffered)
+// coarse probe: bytes of the table per bucket range, read from L2 by every CTA at once
+constexpr size_t COARSE_SLICE_BUDGET = size_t(24) << 20;
 constexpr int PASS1_BLOCK = 512;
 constexpr int PASS1_KPT = 8;                     // pass-1 keys per thread per tile (registers)
 constexpr int PASS1_TILE = PASS1_BLOCK * PASS1_KPT;
@@ -77,7 +79,9 @@ struct BuildPlan {
 hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_index,
                      BuildPlan* plan, int force_path = -1);
 
-enum ProbePath : int { PROBE_DIRECT = 0, PROBE_PARTITIONED = 1 };
+// PROBE_COARSE: pass 1 into bucket ranges whose slice of the table stays in
+// L2, then every range probed from L2 (no split pass, no staging).
+enum ProbePath : int { PROBE_DIRECT = 0, PROBE_PARTITIONED = 1, PROBE_COARSE = 2 };
 
 struct ProbePlan {
   int path = PROBE_DIRECT;

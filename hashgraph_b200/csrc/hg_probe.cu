@@ -472,6 +472,147 @@ __global__ void __launch_bounds__(BLOCK)
   }
 }
 
+// The coarse probe: pass 1 has grouped the queries (with their positions) by
+// bucket range; CTAs take tiles of CPROBE_BLOCK * QPT queries in range order
+// from a ticket, so at any time they all read the table slices of two or
+// three ranges, which stay in L2 (each slice comes from HBM once).  Each
+// thread probes QPT queries side by side: bucket bounds, then the first
+// entries of all its buckets, then the rest of each bucket, keeping the count
+// and the first match in registers.  One block scan and ONE atomic on the
+// pair count reserve a tile's output; pairs come out grouped by tile (no
+// query order).  The kernel waits on L2 reads (bucket bounds and entries,
+// about two sectors per query), not on HBM.
+constexpr int CPROBE_BLOCK = 256;  // 512 and 1024 measured slower (3.50, 3.75 against 3.36 ms)
+
+template <typename KeyT, bool EMIT, bool A_IDX, int QPT>
+__global__ void __launch_bounds__(CPROBE_BLOCK)
+    k_coarse_probe(const KeyT* __restrict__ pkeys, const uint32_t* __restrict__ pidx,
+                   const uint32_t* __restrict__ pcount, uint32_t n_parts, uint64_t part_cap, uint32_t tiles_per_part,
+                   const uint32_t* __restrict__ a_off, const KeyT* __restrict__ a_keys,
+                   const uint32_t* __restrict__ a_idx, BucketMap bm, uint32_t* __restrict__ pairs, uint64_t pair_cap,
+                   unsigned long long* d_count, unsigned* ticket, const uint32_t* flags) {
+  if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
+  constexpr int NW = CPROBE_BLOCK / 32;
+  constexpr uint32_t TILE = uint32_t(CPROBE_BLOCK) * QPT;
+  __shared__ uint64_t red[NW + 1];
+  __shared__ unsigned s_vt[2];
+  const uint64_t vtiles = uint64_t(n_parts) * tiles_per_part;
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+  auto a_ref = [&](uint32_t x) -> uint32_t {
+    if constexpr (A_IDX) return a_idx[x];
+    else return x;
+  };
+  uint64_t counted = 0;
+  // the ticket of iteration i sits in s_vt[i & 1]; thread 0 takes the next
+  // one while the tile is probed, and the barrier that closes the tile
+  // publishes it
+  if (threadIdx.x == 0) s_vt[0] = atomicAdd(ticket, 1u);
+  __syncthreads();
+  for (uint32_t it = 0;; it++) {
+    const uint64_t vt = s_vt[it & 1];
+    if (vt >= vtiles) break;
+    if (threadIdx.x == 0) s_vt[(it + 1) & 1] = atomicAdd(ticket, 1u);
+    const uint64_t part = vt / tiles_per_part;
+    const uint32_t r0 = static_cast<uint32_t>(vt % tiles_per_part) * TILE;
+    const uint32_t m = pcount[part];
+    if (r0 >= m) {  // the same for the whole CTA
+      __syncthreads();
+      continue;
+    }
+    const KeyT* qk = pkeys + part * part_cap;
+    const uint32_t* qi = pidx + part * part_cap;
+    KeyT key[QPT];
+    uint32_t lo[QPT], hi[QPT];
+#pragma unroll
+    for (int j = 0; j < QPT; j++) {
+      const uint32_t r = r0 + j * CPROBE_BLOCK + threadIdx.x;
+      key[j] = r < m ? __ldcs(qk + r) : KeyT(0);
+    }
+#pragma unroll
+    for (int j = 0; j < QPT; j++) {
+      const uint32_t r = r0 + j * CPROBE_BLOCK + threadIdx.x;
+      lo[j] = hi[j] = 0;
+      if (r < m) {
+        const uint32_t b = bm.of_key(key[j]);
+        lo[j] = a_off[b];
+        hi[j] = a_off[b + 1];
+      }
+    }
+    KeyT first[QPT];
+#pragma unroll
+    for (int j = 0; j < QPT; j++) first[j] = lo[j] < hi[j] ? a_keys[lo[j]] : KeyT(0);
+    uint32_t cnt[QPT], ref[QPT];
+    uint64_t mine = 0;
+#pragma unroll
+    for (int j = 0; j < QPT; j++) {
+      cnt[j] = 0;
+      ref[j] = 0;
+      if (lo[j] < hi[j]) {
+        if (first[j] == key[j]) {
+          cnt[j] = 1;
+          if constexpr (EMIT) ref[j] = a_ref(lo[j]);
+        }
+        for (uint32_t x = lo[j] + 1; x < hi[j]; x++) {
+          if (a_keys[x] == key[j]) {
+            if constexpr (EMIT) {
+              if (cnt[j] == 0) ref[j] = a_ref(x);
+            }
+            cnt[j]++;
+          }
+        }
+      }
+      mine += cnt[j];
+    }
+    if constexpr (!EMIT) {
+      counted += mine;
+      __syncthreads();
+    } else {
+      const uint64_t inc = warp_inclusive_scan(mine);
+      if (lane == 31) red[warp] = inc;
+      __syncthreads();
+      if (warp == 0) {
+        const uint64_t w = lane < NW ? red[lane] : 0ull;
+        const uint64_t wi = warp_inclusive_scan(w);
+        const uint64_t tot = __shfl_sync(FULL_MASK, wi, NW - 1);
+        uint64_t base = 0;
+        if (lane == 0 && tot) {
+          base = atomicAdd(d_count, static_cast<unsigned long long>(tot));
+          if (base + tot > pair_cap) record_error(HG_ERR_PAIR_CAPACITY);
+        }
+        base = __shfl_sync(FULL_MASK, base, 0);
+        if (lane < NW) red[lane] = base + wi - w;
+      }
+      __syncthreads();
+      uint64_t pos = red[warp] + inc - mine;
+      __syncwarp();  // the warp's lane 31 rewrites red[warp] in the next tile
+      if (mine) {
+        uint2* out = reinterpret_cast<uint2*>(pairs);
+#pragma unroll
+        for (int j = 0; j < QPT; j++) {
+          if (cnt[j] == 0) continue;
+          const uint32_t qref = qi[r0 + j * CPROBE_BLOCK + threadIdx.x];
+          if (cnt[j] == 1) {
+            if (pos < pair_cap) out[pos] = make_uint2(ref[j], qref);
+            pos++;
+          } else {
+            for (uint32_t x = lo[j]; x < hi[j]; x++) {
+              if (a_keys[x] == key[j]) {
+                if (pos < pair_cap) out[pos] = make_uint2(a_ref(x), qref);
+                pos++;
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  if constexpr (!EMIT) {
+    uint64_t tot;
+    block_exclusive_scan<CPROBE_BLOCK>(counted, red, &tot);
+    if (threadIdx.x == 0 && tot) atomicAdd(d_count, static_cast<unsigned long long>(tot));
+  }
+}
+
 size_t fine_probe_smem(uint32_t fine_log2, uint32_t capa, uint64_t capq, int key_bytes, bool a_idx, bool emit) {
   return 2 * fine_probe_buf_bytes(fine_log2, capa, capq, key_bytes, a_idx, emit);
 }
@@ -483,6 +624,40 @@ static size_t probe_smem_budget() {
     if (kb >= 16 && kb <= 220) return size_t(kb) * 1024;
   }
   return FINE_PROBE_SMEM_BUDGET;
+}
+
+// Bucket ranges of the coarse probe: the widest power of two of buckets whose
+// slice of the table (4-byte offsets + records at the table's mean density)
+// fits the L2 budget, so the CTAs, which take the ranges in order, find the
+// slice they read in L2; at least 16 ranges, so small tables exercise the
+// form too.  The budget leaves room in the 126 MB L2 for the two or three
+// ranges in flight at once (tuning override HG_L2_SLICE_MB).
+static bool plan_coarse(uint64_t nq, uint64_t n_a, size_t a_rec, uint64_t n_buckets, int key_bytes,
+                        PartGeometry* out) {
+  double budget = double(COARSE_SLICE_BUDGET);
+  if (const char* e = std::getenv("HG_L2_SLICE_MB")) {
+    const int mb = std::atoi(e);
+    if (mb >= 1 && mb <= 120) budget = double(mb) * 1048576.0;
+  }
+  const double per_bucket = 4.0 + double(a_rec) * double(n_a) / double(n_buckets);
+  uint32_t c = 0;
+  while (c < 32 && double(1ull << (c + 1)) * per_bucket <= budget) c++;
+  while (c > 0 && ((n_buckets + (1ull << c) - 1) >> c) < 16) c--;
+  // pass 1 slows down sharply above PASS1_GOOD_PARTS ranges (2^31 buckets of
+  // u32 + index: 1024 ranges 14.1 ms, 512 ranges 8.4 ms); wider slices cost
+  // the probe little (3 to 48 MB within 4% at 2^28)
+  while (c < 32 && ((n_buckets + (1ull << c) - 1) >> c) > PASS1_GOOD_PARTS) c++;
+  PartGeometry g;
+  g.coarse_log2 = c;
+  g.n_parts = (n_buckets + (1ull << c) - 1) >> c;
+  if (g.n_parts > PASS1_MAX_PARTS) return false;
+  g.part_cap = slack_capacity(double(nq) * double(std::min<uint64_t>(1ull << c, n_buckets)) / double(n_buckets), 256);
+  if (g.part_cap >= (1ull << 32)) return false;
+  g.tile1 = PASS1_TILE;
+  g.smem1 = pass1_smem(g.n_parts, key_bytes);
+  if (g.smem1 > SMEM_BUDGET) return false;
+  *out = g;
+  return true;
 }
 
 hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, int key_bytes, bool emit,
@@ -510,12 +685,20 @@ hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, 
     p.g.smem3 = fine_probe_smem(p.g.fine_log2, p.g.smem_cap, p.g.fine_cap, key_bytes, a_idx, emit);
     part_ok = p.g.smem1 <= SMEM_BUDGET && p.g.smem2 <= SMEM_BUDGET && p.g.smem3 <= SMEM_BUDGET;
   }
+  PartGeometry cg;
+  const bool coarse_ok = plan_coarse(nq, n_a, a_rec, n_buckets, key_bytes, &cg);
   const uint64_t a_bytes = n_a * a_rec + 4 * n_buckets;
   int path = force_path;
-  if (path < 0) path = (part_ok && a_bytes > (64ull << 20) && nq >= (1ull << 20)) ? PROBE_PARTITIONED : PROBE_DIRECT;
+  if (path < 0) {
+    const bool big = a_bytes > (64ull << 20) && nq >= (1ull << 20);
+    path = !big ? PROBE_DIRECT : coarse_ok ? PROBE_COARSE : part_ok ? PROBE_PARTITIONED : PROBE_DIRECT;
+  }
   // Too few buckets to split the queries finely (everything in a handful of
   // buckets): the direct probe, even when the partitioned one is asked for.
   if (path == PROBE_PARTITIONED && !part_ok) path = PROBE_DIRECT;
+  if (path == PROBE_COARSE && !coarse_ok) path = PROBE_DIRECT;
+  if (path != PROBE_DIRECT && path != PROBE_PARTITIONED && path != PROBE_COARSE) return HG_ERR_INVALID_ARGUMENT;
+  if (path == PROBE_COARSE) p.g = cg;
   p.path = path;
   size_t off = 0;
   p.off_status = off;  off = align_up(off + (emit ? p.tiles * 8 : 0));
@@ -531,6 +714,13 @@ hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, 
     p.off_pidx = off;    off = align_up(off + g.n_parts * g.part_cap * 4);
     p.off_fkeys = off;   off = align_up(off + g.n_fine * g.fine_cap * key_bytes);
     p.off_fidx = off;    off = align_up(off + g.n_fine * g.fine_cap * 4);
+  } else if (path == PROBE_COARSE) {
+    const PartGeometry& g = p.g;
+    p.off_pcount = off;  off = align_up(off + (g.n_parts + 1) * 4);
+    p.off_pstatus = p.off_fcount = p.off_fstatus = off;
+    p.off_pkeys = off;   off = align_up(off + g.n_parts * g.part_cap * key_bytes);
+    p.off_pidx = off;    off = align_up(off + g.n_parts * g.part_cap * 4);
+    p.off_fkeys = p.off_fidx = off;
   } else {
     p.off_pcount = p.off_pstatus = p.off_fcount = p.off_fstatus = off;
     p.off_pkeys = p.off_pidx = p.off_fkeys = p.off_fidx = off;
@@ -618,6 +808,70 @@ static hg_status run_probe_partitioned(const ProbePlan& p, const uint32_t* a_off
   return HG_OK;
 }
 
+template <typename KeyT, bool EMIT>
+static hg_status run_probe_coarse(const ProbePlan& p, const uint32_t* a_off, const KeyT* a_keys, const uint32_t* a_idx,
+                                  const KeyT* q, const uint32_t* q_idx, uint32_t* pairs, uint64_t cap,
+                                  unsigned long long* d_count, char* ws, cudaStream_t s) {
+  const BucketMap bm = p.bucket_map();
+  const PartGeometry& g = p.g;
+  uint32_t* flags = reinterpret_cast<uint32_t*>(ws + p.off_flags);
+  unsigned* ticket = reinterpret_cast<unsigned*>(ws + p.off_ticket);
+  uint64_t* status = reinterpret_cast<uint64_t*>(ws + p.off_status);
+  uint32_t* pcount = reinterpret_cast<uint32_t*>(ws + p.off_pcount);
+  KeyT* pkeys = reinterpret_cast<KeyT*>(ws + p.off_pkeys);
+  uint32_t* pidx = reinterpret_cast<uint32_t*>(ws + p.off_pidx);
+  HG_CUDA(cudaMemsetAsync(ws, 0, p.off_pkeys, s), "intersect: workspace memset");
+  const bool aligned = (reinterpret_cast<uintptr_t>(q) & 15u) == 0;
+  hg_status st = aligned ? launch_pass1<KeyT, 16 / sizeof(KeyT), true>(g, p.nq, q, q_idx, bm, pcount, pkeys, pidx,
+                                                                       flags, "probe_multisplit", s)
+                         : launch_pass1<KeyT, 1, true>(g, p.nq, q, q_idx, bm, pcount, pkeys, pidx, flags,
+                                                       "probe_multisplit", s);
+  if (st != HG_OK) return st;
+  {
+    // queries per thread (tuning override HG_CPROBE_QPT = 1, 2 or 4): fewer
+    // queries per thread keep more warps resident, which hides the L2 latency
+    // of the bucket reads better (2^28 u64 with pairs: 8 -> 4.94 ms, 4 ->
+    // 3.85, 2 -> 3.36, 1 -> 3.84)
+    int qpt = 2;
+    const int block = CPROBE_BLOCK;
+    if (const char* e = std::getenv("HG_CPROBE_QPT")) {
+      const int v = std::atoi(e);
+      qpt = (v == 1 || v == 4) ? v : 2;
+    }
+    const uint32_t tiles_per_part =
+        static_cast<uint32_t>((g.part_cap + uint64_t(block) * qpt - 1) / (uint64_t(block) * qpt));
+    const uint64_t vtiles = g.n_parts * tiles_per_part;
+    auto go = [&](auto kern) {
+      const int bps = blocks_per_sm(kern, block, 0);
+      if (bps <= 0) {
+        st = lib_fail(HG_ERR_CUDA, "coarse-probe kernel cannot be resident");
+        return;
+      }
+      const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(vtiles, uint64_t(device_sm_count()) * bps));
+      Phase ph(s, EMIT ? "coarse_probe_emit" : "coarse_probe_count");
+      count_launch();
+      kern<<<std::max(grid, 1u), block, 0, s>>>(pkeys, pidx, pcount, static_cast<uint32_t>(g.n_parts),
+                                                       g.part_cap, tiles_per_part, a_off, a_keys, a_idx, bm, pairs,
+                                                       cap, d_count, ticket + 3, flags);
+      const cudaError_t e = cudaPeekAtLastError();
+      if (e != cudaSuccess) st = cuda_fail(e, "coarse-probe launch");
+    };
+    auto pick = [&](auto qpt_c) {
+      constexpr int Q = decltype(qpt_c)::value;
+      if (a_idx) go(k_coarse_probe<KeyT, EMIT, true, Q>);
+      else go(k_coarse_probe<KeyT, EMIT, false, Q>);
+    };
+    if (qpt == 1) pick(std::integral_constant<int, 1>{});
+    else if (qpt == 4) pick(std::integral_constant<int, 4>{});
+    else pick(std::integral_constant<int, 2>{});
+    if (st != HG_OK) return st;
+  }
+  // Fallback when a query range overflowed its slots (heavy duplicates): the
+  // direct probe, gated on the flag.
+  launch_probe_direct<KeyT, EMIT>(p, a_off, a_keys, a_idx, q, q_idx, pairs, cap, d_count, status, ticket, flags, s);
+  return HG_OK;
+}
+
 hg_status launch_probe(const ProbePlan& p, const uint32_t* a_off, const void* a_keys, const uint32_t* a_idx,
                        const void* q_keys, const uint32_t* q_idx, uint32_t* pairs, uint64_t pair_cap,
                        unsigned long long* d_count, void* d_ws, cudaStream_t s) {
@@ -635,6 +889,11 @@ hg_status launch_probe(const ProbePlan& p, const uint32_t* a_off, const void* a_
     if (p.path == PROBE_PARTITIONED) {
       st = emit ? run_probe_partitioned<KeyT, true>(p, a_off, ak, a_idx, qk, q_idx, pairs, pair_cap, d_count, ws, s)
                 : run_probe_partitioned<KeyT, false>(p, a_off, ak, a_idx, qk, q_idx, pairs, pair_cap, d_count, ws, s);
+      return;
+    }
+    if (p.path == PROBE_COARSE) {
+      st = emit ? run_probe_coarse<KeyT, true>(p, a_off, ak, a_idx, qk, q_idx, pairs, pair_cap, d_count, ws, s)
+                : run_probe_coarse<KeyT, false>(p, a_off, ak, a_idx, qk, q_idx, pairs, pair_cap, d_count, ws, s);
       return;
     }
     const cudaError_t e = cudaMemsetAsync(ws, 0, p.total, s);

@@ -201,9 +201,11 @@ hg_status hg_intersect_into(const uint32_t* d_a_offsets, const void* d_a_keys,
 
 /* Same with the probe path fixed: 0 = direct (every query reads its bucket
  * from A in HBM), 1 = partitioned (queries are split by bucket range, A's
- * slice of each range is staged in shared memory), -1 = planner's choice.
- * As for the build, path 1 falls back to the direct probe when the buckets
- * are too few to split the queries. */
+ * slice of each range is staged in shared memory), 2 = coarse (queries are
+ * grouped by bucket ranges whose slice of A fits in L2, and every range is
+ * probed from L2), -1 = planner's choice.  As for the build, paths 1 and 2
+ * fall back to the direct probe when the buckets are too few to split the
+ * queries; any other value is HG_ERR_INVALID_ARGUMENT. */
 hg_status hg_intersect_workspace_size_path(uint64_t n_a, int a_has_index, uint64_t n_buckets,
                                            uint64_t nq, int key_bytes, int emit_pairs, int path,
                                            size_t* bytes);

@@ -96,9 +96,15 @@ def test_workspace_plans(capi):
     # the planner picks the partitioned path for a 2^28 x u64 table
     assert L.hg_build_workspace_size(1 << 28, 8, 1 << 28, 0, ctypes.byref(out)) == 0
     assert out.value >= (1 << 28) * 8
-    # and for probing 2^28 queries against it (queries + their index staged)
+    # and the coarse probe for 2^28 queries against it: one pass of the queries
+    # (+ their positions) into L2-sized bucket ranges, no fine partitions
     assert L.hg_intersect_workspace_size(1 << 28, 0, 1 << 28, 1 << 28, 8, 1, ctypes.byref(out)) == 0
+    assert (1 << 28) * 12 <= out.value < (1 << 28) * 12 * 1.1
+    # the partitioned probe, asked for, stages coarse and fine partitions
+    assert L.hg_intersect_workspace_size_path(1 << 28, 0, 1 << 28, 1 << 28, 8, 1, 1, ctypes.byref(out)) == 0
     assert out.value >= 2 * (1 << 28) * 12
+    # an unknown path is an argument error
+    assert L.hg_intersect_workspace_size_path(1 << 20, 0, 1 << 20, 1 << 20, 8, 1, 3, ctypes.byref(out)) == -1
     # a single bucket: the partitioned probe still plans (A's slice is read in
     # place), the partitioned build cannot stage it and plans the direct one
     assert L.hg_intersect_workspace_size_path(1 << 15, 0, 1, 1 << 15, 4, 1, 1, ctypes.byref(out)) == 0

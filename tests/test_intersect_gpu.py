@@ -23,7 +23,7 @@ def _oracle_pairs(a_keys_np, B, with_index, q_np):
     return c, pairs
 
 
-@pytest.mark.parametrize("probe_path", [0, 1])
+@pytest.mark.parametrize("probe_path", [0, 1, 2])
 @pytest.mark.parametrize("path", [0, 1])
 @pytest.mark.parametrize("kb", [4, 8])
 @pytest.mark.parametrize("na,nq,B,frac", [(1 << 16, 1 << 16, 1 << 16, 0.5), (70_001, 30_000, 12_345, 0.25),
@@ -43,7 +43,7 @@ def test_intersect_pairs_with_index(hg, probe_path, path, kb, na, nq, B, frac):
     assert hg.device_error() == 0
 
 
-@pytest.mark.parametrize("probe_path", [0, 1])
+@pytest.mark.parametrize("probe_path", [0, 1, 2])
 def test_intersect_without_index_table(hg, probe_path):
     a = oracle.gen_uniform(200_000, 8, 41)
     q = oracle.gen_overlap(150_000, a, 0.3, 42)
@@ -74,7 +74,7 @@ def test_intersect_without_index_refers_to_csr_positions(hg, kb):
     np.testing.assert_array_equal(np.sort(q[p[:, 1]]), np.sort(q[op[:, 1]]))
 
 
-@pytest.mark.parametrize("probe_path", [0, 1])
+@pytest.mark.parametrize("probe_path", [0, 1, 2])
 def test_intersect_duplicates_multiply(hg, probe_path):
     """Multiset join: k copies in A and m in the queries give k*m matches.
     The partitioned probe overflows its query partitions / spills owners here."""
@@ -90,7 +90,7 @@ def test_intersect_duplicates_multiply(hg, probe_path):
     np.testing.assert_array_equal(_sorted_pairs(to_np_u(pairs, 4)), _sorted_pairs(op))
 
 
-@pytest.mark.parametrize("probe_path", [0, 1])
+@pytest.mark.parametrize("probe_path", [0, 1, 2])
 def test_intersect_pair_capacity(hg, probe_path):
     """Too small a pair buffer: exact count, pairs truncated, error recorded."""
     a = oracle.gen_uniform(1 << 15, 4, 10)

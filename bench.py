@@ -471,8 +471,14 @@ def run_batched(args, rank, world, local):
     dom = max(per_phase, key=lambda k: sum(per_phase[k]))
     peak, peak_kind = load_peaks()
     sum_b = n_total + args.pairs  # buckets + 1 per pair
+    # the L2 form of the probe takes the pairs of >= 2^14 queries (tables of at most 2^20 u64 keys fit its
+    # 24 MB budget): their queries once, their tables once, their pairs
+    large = sizes >= (1 << 14)
+    l2_n = int(sizes[large].sum())
+    l2_m = int(batch.counts[: args.pairs].cpu().numpy()[large].sum())
     alg = {"batch_count": n_total * kb, "batch_scan": 8 * sum_b, "batch_scatter": 2 * n_total * kb,
-           "batch_probe": n_total * kb * 2 + 4 * sum_b + 8 * matches, "batch_clear": 4 * sum_b}.get(dom)
+           "batch_probe": n_total * kb * 2 + 4 * sum_b + 8 * matches, "batch_clear": 4 * sum_b,
+           "batch_l2_probe": l2_n * kb * 2 + 4 * (l2_n + int(large.sum())) + 8 * l2_m}.get(dom)
     achieved = alg / (phase_avg[dom] * 1e-3) / 1e9 if alg else None
     compulsory = n_total * kb * 2 + 4 * sum_b + (n_total * kb * 2 + 4 * sum_b + 8 * matches)
     step_s = total_ms / args.steps * 1e-3

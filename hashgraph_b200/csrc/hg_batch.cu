@@ -22,6 +22,11 @@
 //   k_batch_probe    per query tile: count, per-pair look-back for the output
 //                    offset, pairs written in query order; the pair's last
 //                    tile stores its exact count
+// Large pairs take faster forms: the table through the partitioned build,
+// the queries of a pair whose table fits an L2 budget through
+// k_batch_l2probe (tiles in pair order, the pair's table read from L2, one
+// atomic per tile on the pair's count, pairs grouped by tile), those of a
+// larger table through the partitioned probe.
 // Each pair's result is the one the single-pair direct path
 // (k_count / k_scan_u32 / k_scatter / k_probe) gives.  The reference has no
 // batched form; per pair it replaces build + intersect of
@@ -64,6 +69,8 @@ struct BatchPairDev {
   uint64_t fb0, fq0;                // first fine partition in the batch's lists
   uint64_t mt0, mq0;                // first pass-1 tile of the keys / of the queries
   uint32_t a_bulk;                  // the table's arrays are 16-byte aligned
+  uint32_t pl;                      // L2 form of the probe: tiles [ltile0, ltile0 + ltiles)
+  uint64_t ltile0, ltiles;
 };
 
 // Flags of a batch run: [0] a table's partitioned build overflowed, [1] a
@@ -72,7 +79,7 @@ __device__ __forceinline__ bool batch_skip_build(const BatchPairDev& P, const ui
   return P.pb && !(*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW);
 }
 __device__ __forceinline__ bool batch_skip_probe(const BatchPairDev& P, const uint32_t* flags) {
-  return P.pq && !(*reinterpret_cast<const volatile uint32_t*>(flags + 1) & FLAG_OVERFLOW);
+  return P.pl || (P.pq && !(*reinterpret_cast<const volatile uint32_t*>(flags + 1) & FLAG_OVERFLOW));
 }
 
 // Every pair's offsets to zero (tile lt of a pair clears entries
@@ -308,6 +315,118 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_probe(const BatchPairDev*
   }
 }
 
+// L2 form of a large pair's probe: the pair's table (at most BATCH_L2_TABLE
+// bytes) was built just before and is read from L2 while the CTAs, which take
+// tiles in pair order from a ticket, work on it.  Per thread BATCH_LQPT
+// queries side by side (bucket bounds, first entries, the rest of each
+// bucket; count and first match in registers); one block scan and ONE atomic
+// on the pair's count reserve a tile's output.
+constexpr uint32_t BATCH_LQPT = 2;
+constexpr uint32_t BATCH_LTILE = BATCH_BLOCK * BATCH_LQPT;
+
+template <typename KeyT>
+__global__ void __launch_bounds__(BATCH_BLOCK) k_batch_l2probe(const BatchPairDev* __restrict__ pairs,
+                                                              const uint32_t* __restrict__ ltile_pair,
+                                                              uint64_t n_ltiles, unsigned* ticket) {
+  constexpr int NW = BATCH_BLOCK / 32;
+  __shared__ uint64_t red[NW + 1];
+  __shared__ unsigned s_t[2];
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+  // ticket of iteration i in s_t[i & 1]; the next one is taken during the
+  // tile and published by the tile's barriers
+  if (threadIdx.x == 0) s_t[0] = atomicAdd(ticket, 1u);
+  __syncthreads();
+  for (uint32_t it = 0;; it++) {
+    const uint64_t t = s_t[it & 1];
+    if (t >= n_ltiles) break;
+    if (threadIdx.x == 0) s_t[(it + 1) & 1] = atomicAdd(ticket, 1u);
+    const BatchPairDev& P = pairs[ltile_pair[t]];
+    const uint64_t r0 = (t - P.ltile0) * BATCH_LTILE;
+    const KeyT* q = static_cast<const KeyT*>(P.query);
+    const KeyT* a_keys = static_cast<const KeyT*>(P.keys_out);
+    const uint32_t* a_off = P.offsets;
+    const uint32_t* a_idx = P.idx_out;
+    const BucketMap bm = P.bm;
+    const uint64_t nq = P.nq;
+    KeyT key[BATCH_LQPT];
+    uint32_t lo[BATCH_LQPT], hi[BATCH_LQPT], cnt[BATCH_LQPT], ref[BATCH_LQPT];
+#pragma unroll
+    for (uint32_t j = 0; j < BATCH_LQPT; j++) {
+      const uint64_t r = r0 + j * BATCH_BLOCK + threadIdx.x;
+      key[j] = r < nq ? __ldcs(q + r) : KeyT(0);
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < BATCH_LQPT; j++) {
+      const uint64_t r = r0 + j * BATCH_BLOCK + threadIdx.x;
+      lo[j] = hi[j] = 0;
+      if (r < nq) {
+        const uint32_t b = bm.of_key(key[j]);
+        lo[j] = a_off[b];
+        hi[j] = a_off[b + 1];
+      }
+    }
+    KeyT first[BATCH_LQPT];
+#pragma unroll
+    for (uint32_t j = 0; j < BATCH_LQPT; j++) first[j] = lo[j] < hi[j] ? a_keys[lo[j]] : KeyT(0);
+    uint64_t mine = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < BATCH_LQPT; j++) {
+      cnt[j] = 0;
+      ref[j] = 0;
+      if (lo[j] < hi[j]) {
+        if (first[j] == key[j]) {
+          cnt[j] = 1;
+          ref[j] = a_idx ? a_idx[lo[j]] : lo[j];
+        }
+        for (uint32_t x = lo[j] + 1; x < hi[j]; x++) {
+          if (a_keys[x] == key[j]) {
+            if (cnt[j] == 0) ref[j] = a_idx ? a_idx[x] : x;
+            cnt[j]++;
+          }
+        }
+      }
+      mine += cnt[j];
+    }
+    const uint64_t inc = warp_inclusive_scan(mine);
+    if (lane == 31) red[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+      const uint64_t w = lane < NW ? red[lane] : 0ull;
+      const uint64_t wi = warp_inclusive_scan(w);
+      const uint64_t tot = __shfl_sync(FULL_MASK, wi, NW - 1);
+      uint64_t base = 0;
+      if (lane == 0 && tot) {
+        base = atomicAdd(P.count, static_cast<unsigned long long>(tot));
+        if (P.pairs && base + tot > P.pair_cap) record_error(HG_ERR_PAIR_CAPACITY);
+      }
+      base = __shfl_sync(FULL_MASK, base, 0);
+      if (lane < NW) red[lane] = base + wi - w;
+    }
+    __syncthreads();
+    uint64_t pos = red[warp] + inc - mine;
+    __syncwarp();  // the warp's lane 31 rewrites red[warp] in the next tile
+    if (P.pairs && mine) {
+      uint2* out = reinterpret_cast<uint2*>(P.pairs);
+#pragma unroll
+      for (uint32_t j = 0; j < BATCH_LQPT; j++) {
+        if (cnt[j] == 0) continue;
+        const uint32_t qref = static_cast<uint32_t>(r0 + j * BATCH_BLOCK + threadIdx.x);
+        if (cnt[j] == 1) {
+          if (pos < P.pair_cap) out[pos] = make_uint2(ref[j], qref);
+          pos++;
+        } else {
+          for (uint32_t x = lo[j]; x < hi[j]; x++) {
+            if (a_keys[x] == key[j]) {
+              if (pos < P.pair_cap) out[pos] = make_uint2(a_idx ? a_idx[x] : x, qref);
+              pos++;
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Partitioned form of large pairs: the pass-1 multisplit of each pair goes
 // straight to its fine partitions (at most PASS1_GOOD_PARTS of them: no split
@@ -391,11 +510,12 @@ struct BatchProbe {
 // Host-side batch: the plan, the device workspace and the descriptors.
 constexpr uint64_t BATCH_PART_MIN = 1ull << 14;  // keys (queries) from which a pair is partitioned
 constexpr uint32_t BATCH_FINE_LOG2 = 11;          // fine width of the partitioned build
+constexpr uint64_t BATCH_L2_TABLE = uint64_t(24) << 20;  // table bytes up to which a large pair's probe reads L2
 
 struct BatchPlan {
   int n_pairs = 0;
   int key_bytes = 8;
-  uint64_t n_ktiles = 0, n_stiles = 0, n_qtiles = 0;
+  uint64_t n_ktiles = 0, n_stiles = 0, n_qtiles = 0, n_ltiles = 0;
   // partitioned form
   uint64_t n_mt = 0, n_mq = 0;      // pass-1 tiles of the keys / of the queries
   uint64_t n_fb = 0, n_fq = 0;      // fine partitions of the tables / of the queries
@@ -405,7 +525,7 @@ struct BatchPlan {
   uint32_t max_pb = 1, max_pq = 1;  // most fine partitions of one pair
   bool wi_b = false, ai_q = false, bulk_b = true, bulk_q = true;
   size_t smem1b = 0, smem1q = 0, smem3b = 0, smem3q = 0;
-  size_t off_pairs = 0, off_kmap = 0, off_smap = 0, off_qmap = 0;
+  size_t off_pairs = 0, off_kmap = 0, off_smap = 0, off_qmap = 0, off_lmap = 0;
   size_t off_mtmap = 0, off_mqmap = 0, off_fbmap = 0, off_fqmap = 0;
   size_t off_fbkeys = 0, off_fbidx = 0, off_fqkeys = 0, off_fqidx = 0;
   size_t off_zero = 0, off_sstat = 0, off_qstat = 0, off_ticket = 0, off_flags = 0;
@@ -426,7 +546,8 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
                             std::vector<BatchPairDev>* dev, std::vector<uint32_t>* kmap,
                             std::vector<uint32_t>* smap, std::vector<uint32_t>* qmap,
                             std::vector<uint32_t>* mtmap, std::vector<uint32_t>* mqmap,
-                            std::vector<uint32_t>* fbmap, std::vector<uint32_t>* fqmap) {
+                            std::vector<uint32_t>* fbmap, std::vector<uint32_t>* fqmap,
+                            std::vector<uint32_t>* lmap) {
   if (key_bytes != 4 && key_bytes != 8) return HG_ERR_KEY_WIDTH;
   if (n_pairs < 0 || (n_pairs > 0 && !pairs)) return HG_ERR_INVALID_ARGUMENT;
   BatchPlan p;
@@ -496,6 +617,11 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
   p.smem3b = align_up(8 * wb, 16) + p.capf * (2 * rec_b + 4);
   if (p.smem3b > SMEM_BUDGET)
     for (auto& d : *dev) d.pb = 0;
+  // the L2 form for large pairs whose whole table fits the L2 budget
+  for (auto& d : *dev) {
+    const uint64_t table_bytes = 4 * (d.n_buckets + 1) + d.n * (key_bytes + (d.idx_out ? 4 : 0));
+    d.pl = (d.nq >= BATCH_PART_MIN && d.n > 0 && table_bytes <= BATCH_L2_TABLE) ? 1u : 0u;
+  }
   // the probe's fine width: the widest whose staging fits one CTA
   for (uint32_t lq = 12; lq >= 10; lq--) {
     const uint64_t wq = 1ull << lq;
@@ -504,7 +630,7 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
     for (auto& d : *dev) {
       const double per_q = double(d.nq) * double(wq) / double(d.n_buckets);
       const double per_a = double(d.n) * double(wq) / double(d.n_buckets);
-      d.pq = (d.nq >= BATCH_PART_MIN && d.n > 0 && (d.n_buckets + wq - 1) / wq <= PASS1_GOOD_PARTS &&
+      d.pq = (!d.pl && d.nq >= BATCH_PART_MIN && d.n > 0 && (d.n_buckets + wq - 1) / wq <= PASS1_GOOD_PARTS &&
               per_q <= 8192.0 && per_a <= 8192.0) ? 1u : 0u;
       if (!d.pq) continue;
       any = true;
@@ -548,8 +674,20 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
       p.bulk_q = p.bulk_q && aligned(d.query);
     }
   }
-  if (p.n_mt >= (1ull << 32) || p.n_mq >= (1ull << 32) || p.n_fb >= (1ull << 32) || p.n_fq >= (1ull << 32))
+  for (int i = 0; i < n_pairs; i++) {
+    BatchPairDev& d = (*dev)[i];
+    d.ltile0 = p.n_ltiles;
+    d.ltiles = d.pl ? (d.nq + BATCH_LTILE - 1) / BATCH_LTILE : 0;
+    p.n_ltiles += d.ltiles;
+  }
+  if (p.n_mt >= (1ull << 32) || p.n_mq >= (1ull << 32) || p.n_fb >= (1ull << 32) || p.n_fq >= (1ull << 32) ||
+      p.n_ltiles >= (1ull << 32))
     return lib_fail(HG_ERR_TOO_LARGE, "hg_batch_create: more than 2^32 partition tiles");
+  lmap->resize(p.n_ltiles);
+  for (int i = 0; i < n_pairs; i++) {
+    const BatchPairDev& d = (*dev)[i];
+    std::fill(lmap->begin() + d.ltile0, lmap->begin() + d.ltile0 + d.ltiles, uint32_t(i));
+  }
   p.smem1b = pass1_smem(p.max_pb, key_bytes);
   p.smem1q = pass1_smem(p.max_pq, key_bytes);
   mtmap->resize(p.n_mt);
@@ -573,6 +711,7 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
   p.off_kmap = off;    off = align_up(off + 4 * std::max<uint64_t>(p.n_ktiles, 1));
   p.off_smap = off;    off = align_up(off + 4 * std::max<uint64_t>(p.n_stiles, 1));
   p.off_qmap = off;    off = align_up(off + 4 * std::max<uint64_t>(p.n_qtiles, 1));
+  p.off_lmap = off;    off = align_up(off + 4 * std::max<uint64_t>(p.n_ltiles, 1));
   p.off_mtmap = off;   off = align_up(off + 4 * std::max<uint64_t>(p.n_mt, 1));
   p.off_mqmap = off;   off = align_up(off + 4 * std::max<uint64_t>(p.n_mq, 1));
   p.off_fbmap = off;   off = align_up(off + 4 * std::max<uint64_t>(p.n_fb, 1));
@@ -688,6 +827,12 @@ static hg_status batch_launch(const BatchPlan& p, char* ws, cudaStream_t s) {
     count_launch();
     k_batch_scatter<KeyT><<<grid_for(p.n_ktiles), BATCH_BLOCK, 0, s>>>(pairs, kmap, p.n_ktiles, flags);
   }
+  if (p.n_ltiles) {
+    Phase ph(s, "batch_l2_probe");
+    count_launch();
+    k_batch_l2probe<KeyT><<<grid_for(p.n_ltiles), BATCH_BLOCK, 0, s>>>(
+        pairs, reinterpret_cast<const uint32_t*>(ws + p.off_lmap), p.n_ltiles, ticket + 4);
+  }
   if (p.n_mq) {
     using Src = BatchSplitTiles<KeyT, true>;
     const Src src{pairs, reinterpret_cast<const uint32_t*>(ws + p.off_mqmap), p.n_mq, p.lq, p.capq,
@@ -735,9 +880,9 @@ extern "C" hg_status hg_batch_create(const hg_batch_pair* pairs, int n_pairs, in
   *out = nullptr;
   BatchPlan plan;
   std::vector<BatchPairDev> dev;
-  std::vector<uint32_t> kmap, smap, qmap, mtmap, mqmap, fbmap, fqmap;
+  std::vector<uint32_t> kmap, smap, qmap, mtmap, mqmap, fbmap, fqmap, lmap;
   hg_status st = batch_plan(pairs, n_pairs, key_bytes, &plan, &dev, &kmap, &smap, &qmap, &mtmap, &mqmap, &fbmap,
-                            &fqmap);
+                            &fqmap, &lmap);
   if (st != HG_OK) return st;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   hg_batch* b = new hg_batch();
@@ -762,6 +907,7 @@ extern "C" hg_status hg_batch_create(const hg_batch_pair* pairs, int n_pairs, in
       (e = up(plan.off_mqmap, mqmap.data(), mqmap.size() * 4)) != cudaSuccess ||
       (e = up(plan.off_fbmap, fbmap.data(), fbmap.size() * 4)) != cudaSuccess ||
       (e = up(plan.off_fqmap, fqmap.data(), fqmap.size() * 4)) != cudaSuccess ||
+      (e = up(plan.off_lmap, lmap.data(), lmap.size() * 4)) != cudaSuccess ||
       (e = cudaStreamSynchronize(s)) != cudaSuccess) {  // the host vectors go out of scope
     cudaFreeAsync(b->d_mem, s);
     delete b;

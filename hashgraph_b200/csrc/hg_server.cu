@@ -76,6 +76,7 @@ struct hg_server {
   std::vector<uint8_t> slot_busy;
   std::vector<cudaEvent_t> free_events;
   cudaMemPool_t pool = nullptr;
+  cudaStream_t clock_stream = nullptr;  // carries only `ref`, so `ref` completes at once
   cudaEvent_t ref = nullptr;
   double ref_host = 0;
 };
@@ -149,14 +150,20 @@ static hg_status reserve_slot(hg_server* s, uint32_t* slot) {
   return lib_fail(HG_ERR_TOO_LARGE, "hg_server: 65536 intersects in flight; poll before submitting more");
 }
 
-// The latency clock: event times are taken relative to `ref`, a float count
-// of milliseconds, so `ref` is moved forward whenever nothing is in flight
-// and it is more than a minute old (keeping the float's resolution in
-// microseconds).
+// The latency clock: a request's completion is its event's time after `ref`
+// (a float count of milliseconds) added to ref_host, the host time of `ref`.
+// The GPU's event timer and the host clock drift apart by tens of
+// microseconds over seconds, so `ref` is re-taken at a poll when it is more
+// than REF_MAX_AGE_S old.  It is recorded on a stream of its own that carries
+// no work, so it completes at once whatever the other streams hold; ref_host
+// is the midpoint of the record and the synchronisation that saw it.
+constexpr double REF_MAX_AGE_S = 0.1;
+
 static cudaError_t rebase_clock(hg_server* s) {
-  cudaError_t e = cudaEventRecord(s->ref, s->streams[0]);
+  const double t0 = monotonic_s();
+  cudaError_t e = cudaEventRecord(s->ref, s->clock_stream);
   if (e == cudaSuccess) e = cudaEventSynchronize(s->ref);
-  if (e == cudaSuccess) s->ref_host = monotonic_s();
+  if (e == cudaSuccess) s->ref_host = 0.5 * (t0 + monotonic_s());
   return e;
 }
 
@@ -187,6 +194,7 @@ extern "C" void hg_server_free(hg_server* s) {
   if (s->d_counts) cudaFree(s->d_counts);
   if (s->h_counts) cudaFreeHost(s->h_counts);
   if (s->ref) cudaEventDestroy(s->ref);
+  if (s->clock_stream) cudaStreamDestroy(s->clock_stream);
   for (auto& st : s->streams) cudaStreamDestroy(st);
   delete s;
 }
@@ -243,6 +251,7 @@ extern "C" hg_status hg_server_create(size_t budget_bytes, int max_tables, int n
   }
   if (e == cudaSuccess) e = cudaMalloc(&s->d_counts, sizeof(unsigned long long) * s->n_slots);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_counts, sizeof(unsigned long long) * s->n_slots);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->clock_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&s->ref);
   if (e == cudaSuccess) e = rebase_clock(s);
   if (e != cudaSuccess) {
@@ -386,7 +395,9 @@ extern "C" hg_status hg_server_poll(hg_server* s, int block, hg_server_done* out
     s->free_events.push_back(it->done);
     it = s->inflight.erase(it);
   }
-  if (s->inflight.empty() && monotonic_s() - s->ref_host > 60.0) {
+  // re-based only when every completed request has been reported against the
+  // old `ref` (the loop did not stop at max_out)
+  if (*n_out < max_out && monotonic_s() - s->ref_host > REF_MAX_AGE_S) {
     const cudaError_t e = rebase_clock(s);
     if (e != cudaSuccess) return cuda_fail(e, "hg_server_poll: clock");
   }

@@ -61,10 +61,11 @@ class DeviceShardOps:
     """The device steps of a sharded build / intersect on one GPU, through the
     C ABI (hg_shard_*)."""
 
-    def __init__(self, device=None, path: int = PATH_AUTO):
+    def __init__(self, device=None, path: int = PATH_AUTO, probe_path: int | None = None):
         import torch
         self.device = torch.device(device or "cuda")
-        self.path = path
+        self.path = path  # the build's path
+        self.probe_path = path if probe_path is None else probe_path
 
     def histogram(self, keys, n_buckets: int, n_bins: int):
         import torch
@@ -113,14 +114,15 @@ class DeviceShardOps:
         nq, kb = queries.numel(), _key_bytes(queries)
         out = ctypes.c_size_t(0)
         check(lib().hg_intersect_workspace_size_path(part.n, int(part.idx is not None), part.hi - part.lo, nq, kb,
-                                                     int(emit), self.path, ctypes.byref(out)), "intersect workspace")
+                                                     int(emit), self.probe_path, ctypes.byref(out)),
+              "intersect workspace")
         ws = torch.empty(max(out.value, 1), dtype=torch.uint8, device=self.device)
         count = torch.empty(1, dtype=torch.int64, device=self.device)
         pairs = torch.empty((max(int(pair_cap), 1), 2), dtype=torch.int32, device=self.device) if emit else None
         check(lib().hg_shard_intersect_into_path(
             _ptr(part.offsets), _ptr(part.keys), _ptr(part.idx), part.n, int(n_buckets), part.lo, part.hi, kb,
             _ptr(queries), nq, _ptr(query_idx), _ptr(pairs), int(pair_cap) if emit else 0, _ptr(count), _ptr(ws),
-            ws.numel(), self.path, _stream()), "hg_shard_intersect_into")
+            ws.numel(), self.probe_path, _stream()), "hg_shard_intersect_into")
         return count, pairs
 
     def empty_keys(self, n: int, like):

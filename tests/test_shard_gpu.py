@@ -70,8 +70,8 @@ def _check_shard(part, off, k, idx, lo, hi, kb):
 
 
 @pytest.mark.parametrize("case", ["pow2_aligned", "pow2_balanced", "odd_buckets"])
-@pytest.mark.parametrize("path", [0, 1])
-def test_emulated_shards_equal_global_table(hg, case, path):
+@pytest.mark.parametrize("path,probe_path", [(0, 0), (1, 1), (1, 2)])
+def test_emulated_shards_equal_global_table(hg, case, path, probe_path):
     import torch
     from hashgraph_b200.shard import DeviceShardOps, shard_splits
     kb, G = 8, 4
@@ -79,7 +79,7 @@ def test_emulated_shards_equal_global_table(hg, case, path):
     B = {"pow2_aligned": 1 << 21, "pow2_balanced": 1 << 21, "odd_buckets": 2_000_003}[case]
     A = oracle.gen_uniform(n, kb, 91)
     Q = oracle.gen_overlap(n // 2, A, 0.4, 92)
-    dev = DeviceShardOps(path=path)
+    dev = DeviceShardOps(path=path, probe_path=probe_path)
     dA, dQ = from_np_u(A), from_np_u(Q)
     if case == "pow2_aligned":
         splits = [r * (B // G) for r in range(G + 1)]

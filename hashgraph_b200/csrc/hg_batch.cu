@@ -614,7 +614,7 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
     d.a_bulk = (aligned(d.offsets) && aligned(d.keys_out) && (!d.idx_out || aligned(d.idx_out))) ? 1u : 0u;
   }
   const size_t rec_b = key_bytes + (p.wi_b ? 4 : 0);
-  p.smem3b = align_up(8 * wb, 16) + p.capf * (2 * rec_b + 4);
+  p.smem3b = align_up(8 * wb, 16) + p.capf * (2 * rec_b + 6);
   if (p.smem3b > SMEM_BUDGET)
     for (auto& d : *dev) d.pb = 0;
   // the L2 form for large pairs whose whole table fits the L2 budget

@@ -635,6 +635,7 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(Src src, uint64_t capf, ui
   KeyT* sk = reinterpret_cast<KeyT*>(smem_raw + align_up_dev(size_t(W) * 8, 16));
   uint32_t* si = reinterpret_cast<uint32_t*>(sk + 2 * capf);
   uint32_t* sr = si + (WITH_IDX ? 2 * capf : 0);
+  uint16_t* sperm = reinterpret_cast<uint16_t*>(sr + capf);  // record at each output position
   __shared__ uint32_t wsum[NW + 1];
   __shared__ uint64_t bar[2];
   __shared__ uint32_t s_base[2], s_m[2];
@@ -729,12 +730,19 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(Src src, uint64_t capf, ui
     } else {
       block_scan_segments<BLOCK>(ctr, nb, base, base, wsum, [&](uint32_t j, uint32_t g) { offsets[b0 + j] = g; });
     }
+    // the partition's output is the contiguous range [base, base + m): each
+    // record's position goes into shared memory, then the keys (and
+    // indices) leave in position order with coalesced stores
     for (uint32_t r = threadIdx.x; r < m; r += BLOCK) {
       const uint32_t v = sr[r];
-      const uint32_t pos = ctr[v >> 16] + (v & 0xffffu);
-      keys_out[pos] = ck[r];
+      sperm[ctr[v >> 16] + (v & 0xffffu) - base] = static_cast<uint16_t>(r);
+    }
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < m; q += BLOCK) {
+      const uint32_t r = sperm[q];
+      keys_out[base + q] = ck[r];
       if constexpr (WITH_IDX) {
-        if (idx_out) idx_out[pos] = ci[r];
+        if (idx_out) idx_out[base + q] = ci[r];
       }
     }
   }
@@ -912,13 +920,13 @@ hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_in
   const size_t rec = key_bytes + (with_index ? 4 : 0);
   // pass 3 double-buffers its partition's records (2 * rec per staged
   // record) and its bucket counters (8 bytes per bucket), and keeps a 4-byte
-  // (bucket, rank) word per record
+  // (bucket, rank) word and a 2-byte output-position entry per record
   size_t budget = FINE_SMEM_BUDGET;
   if (const char* e = std::getenv("HG_BUILD_SMEM_KB")) {  // tuning override of the fine-build CTA's budget
     const int kb = std::atoi(e);
     if (kb >= 16 && kb <= 220) budget = size_t(kb) * 1024;
   }
-  bool part_ok = plan_geometry(n, rec, n, 2 * rec + 4, 8, 0, n_buckets, false, &p.g, budget);
+  bool part_ok = plan_geometry(n, rec, n, 2 * rec + 6, 8, 0, n_buckets, false, &p.g, budget);
   // ranks within a bucket and local bucket numbers are packed in 16 bits
   if (part_ok && (p.g.fine_cap >= 65536 || p.g.fine_log2 > 16)) part_ok = false;
   if (part_ok) {

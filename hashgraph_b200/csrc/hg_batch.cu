@@ -69,7 +69,7 @@ struct BatchPairDev {
   uint64_t fb0, fq0;                // first fine partition in the batch's lists
   uint64_t mt0, mq0;                // first pass-1 tile of the keys / of the queries
   uint32_t a_bulk;                  // the table's arrays are 16-byte aligned
-  uint32_t pl;                      // L2 form of the probe: tiles [ltile0, ltile0 + ltiles)
+  uint32_t pl;                      // L2 form of the probe: chunks [ltile0, ltile0 + ltiles)
   uint64_t ltile0, ltiles;
 };
 
@@ -320,14 +320,17 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_probe(const BatchPairDev*
 // tiles in pair order from a ticket, work on it.  Per thread BATCH_LQPT
 // queries side by side (bucket bounds, first entries, the rest of each
 // bucket; count and first match in registers); one block scan and ONE atomic
-// on the pair's count reserve a tile's output.
+// on the pair's count reserve a tile's output.  A ticket hands out
+// BATCH_LCHUNK consecutive tiles of one pair ("chunk"): the pair's descriptor
+// is read once for them.
 constexpr uint32_t BATCH_LQPT = 2;
 constexpr uint32_t BATCH_LTILE = BATCH_BLOCK * BATCH_LQPT;
+constexpr uint32_t BATCH_LCHUNK = 4;  // tiles of one pair per ticket: the pair's descriptor is read once for them
 
 template <typename KeyT>
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_l2probe(const BatchPairDev* __restrict__ pairs,
-                                                              const uint32_t* __restrict__ ltile_pair,
-                                                              uint64_t n_ltiles, unsigned* ticket) {
+                                                              const uint32_t* __restrict__ lchunk_pair,
+                                                              uint64_t n_lchunks, unsigned* ticket) {
   constexpr int NW = BATCH_BLOCK / 32;
   __shared__ uint64_t red[NW + 1];
   __shared__ unsigned s_t[2];
@@ -337,17 +340,23 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_l2probe(const BatchPairDe
   if (threadIdx.x == 0) s_t[0] = atomicAdd(ticket, 1u);
   __syncthreads();
   for (uint32_t it = 0;; it++) {
-    const uint64_t t = s_t[it & 1];
-    if (t >= n_ltiles) break;
+    const uint64_t c = s_t[it & 1];
+    if (c >= n_lchunks) break;
     if (threadIdx.x == 0) s_t[(it + 1) & 1] = atomicAdd(ticket, 1u);
-    const BatchPairDev& P = pairs[ltile_pair[t]];
-    const uint64_t r0 = (t - P.ltile0) * BATCH_LTILE;
+    const BatchPairDev& P = pairs[lchunk_pair[c]];
     const KeyT* q = static_cast<const KeyT*>(P.query);
     const KeyT* a_keys = static_cast<const KeyT*>(P.keys_out);
     const uint32_t* a_off = P.offsets;
     const uint32_t* a_idx = P.idx_out;
     const BucketMap bm = P.bm;
     const uint64_t nq = P.nq;
+    uint32_t* pairs_out = P.pairs;
+    const uint64_t pair_cap = P.pair_cap;
+    unsigned long long* count = P.count;
+    const uint64_t t0 = (c - P.ltile0) * BATCH_LCHUNK;
+  for (uint32_t k = 0; k < BATCH_LCHUNK; k++) {
+    const uint64_t r0 = (t0 + k) * BATCH_LTILE;
+    if (r0 >= nq) break;  // the same for the whole CTA
     KeyT key[BATCH_LQPT];
     uint32_t lo[BATCH_LQPT], hi[BATCH_LQPT], cnt[BATCH_LQPT], ref[BATCH_LQPT];
 #pragma unroll
@@ -396,8 +405,8 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_l2probe(const BatchPairDe
       const uint64_t tot = __shfl_sync(FULL_MASK, wi, NW - 1);
       uint64_t base = 0;
       if (lane == 0 && tot) {
-        base = atomicAdd(P.count, static_cast<unsigned long long>(tot));
-        if (P.pairs && base + tot > P.pair_cap) record_error(HG_ERR_PAIR_CAPACITY);
+        base = atomicAdd(count, static_cast<unsigned long long>(tot));
+        if (pairs_out && base + tot > pair_cap) record_error(HG_ERR_PAIR_CAPACITY);
       }
       base = __shfl_sync(FULL_MASK, base, 0);
       if (lane < NW) red[lane] = base + wi - w;
@@ -405,25 +414,26 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_l2probe(const BatchPairDe
     __syncthreads();
     uint64_t pos = red[warp] + inc - mine;
     __syncwarp();  // the warp's lane 31 rewrites red[warp] in the next tile
-    if (P.pairs && mine) {
-      uint2* out = reinterpret_cast<uint2*>(P.pairs);
+    if (pairs_out && mine) {
+      uint2* out = reinterpret_cast<uint2*>(pairs_out);
 #pragma unroll
       for (uint32_t j = 0; j < BATCH_LQPT; j++) {
         if (cnt[j] == 0) continue;
         const uint32_t qref = static_cast<uint32_t>(r0 + j * BATCH_BLOCK + threadIdx.x);
         if (cnt[j] == 1) {
-          if (pos < P.pair_cap) out[pos] = make_uint2(ref[j], qref);
+          if (pos < pair_cap) out[pos] = make_uint2(ref[j], qref);
           pos++;
         } else {
           for (uint32_t x = lo[j]; x < hi[j]; x++) {
             if (a_keys[x] == key[j]) {
-              if (pos < P.pair_cap) out[pos] = make_uint2(a_idx ? a_idx[x] : x, qref);
+              if (pos < pair_cap) out[pos] = make_uint2(a_idx ? a_idx[x] : x, qref);
               pos++;
             }
           }
         }
       }
     }
+  }
   }
 }
 
@@ -676,8 +686,8 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
   }
   for (int i = 0; i < n_pairs; i++) {
     BatchPairDev& d = (*dev)[i];
-    d.ltile0 = p.n_ltiles;
-    d.ltiles = d.pl ? (d.nq + BATCH_LTILE - 1) / BATCH_LTILE : 0;
+    d.ltile0 = p.n_ltiles;  // counted in chunks of BATCH_LCHUNK tiles
+    d.ltiles = d.pl ? (d.nq + uint64_t(BATCH_LTILE) * BATCH_LCHUNK - 1) / (uint64_t(BATCH_LTILE) * BATCH_LCHUNK) : 0;
     p.n_ltiles += d.ltiles;
   }
   if (p.n_mt >= (1ull << 32) || p.n_mq >= (1ull << 32) || p.n_fb >= (1ull << 32) || p.n_fq >= (1ull << 32) ||

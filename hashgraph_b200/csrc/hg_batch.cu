@@ -85,12 +85,15 @@ __device__ __forceinline__ bool batch_skip_probe(const BatchPairDev& P, const ui
 // Every pair's offsets to zero (tile lt of a pair clears entries
 // [lt*STILE, ...) of offsets[1..B]; tile 0 also offsets[0]); every count to 0.
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_clear(const BatchPairDev* __restrict__ pairs, int n_pairs,
-                                                            const uint32_t* __restrict__ stile_pair, uint64_t n_stiles,
-                                                            const uint32_t* flags) {
-  for (uint64_t i = uint64_t(blockIdx.x) * BATCH_BLOCK + threadIdx.x; i < uint64_t(n_pairs);
-       i += uint64_t(gridDim.x) * BATCH_BLOCK)
-    *pairs[i].count = 0ull;
-  for (uint64_t t = blockIdx.x; t < n_stiles; t += gridDim.x) {
+                                                            const uint32_t* __restrict__ stile_pair, uint64_t s_begin,
+                                                            uint64_t s_end, const uint32_t* flags,
+                                                            const uint32_t* gate) {
+  if (gated_off(gate)) return;
+  if (!gate)  // the ungated launch zeroes every pair's count
+    for (uint64_t i = uint64_t(blockIdx.x) * BATCH_BLOCK + threadIdx.x; i < uint64_t(n_pairs);
+         i += uint64_t(gridDim.x) * BATCH_BLOCK)
+      *pairs[i].count = 0ull;
+  for (uint64_t t = s_begin + blockIdx.x; t < s_end; t += gridDim.x) {
     const BatchPairDev& P = pairs[stile_pair[t]];
     if (batch_skip_build(P, flags)) continue;
     const uint64_t lt = t - P.stile0;
@@ -104,9 +107,10 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_clear(const BatchPairDev*
 
 template <typename KeyT>
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_count(const BatchPairDev* __restrict__ pairs,
-                                                            const uint32_t* __restrict__ ktile_pair, uint64_t n_ktiles,
-                                                            const uint32_t* flags) {
-  for (uint64_t t = blockIdx.x; t < n_ktiles; t += gridDim.x) {
+                                                            const uint32_t* __restrict__ ktile_pair, uint64_t k_begin,
+                                                            uint64_t k_end, const uint32_t* flags, const uint32_t* gate) {
+  if (gated_off(gate)) return;
+  for (uint64_t t = k_begin + blockIdx.x; t < k_end; t += gridDim.x) {
     const BatchPairDev& P = pairs[ktile_pair[t]];
     if (batch_skip_build(P, flags)) continue;
     const KeyT* keys = static_cast<const KeyT*>(P.keys);
@@ -129,19 +133,20 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_count(const BatchPairDev*
 // every tile a look-back waits on is already held by a running CTA.
 template <int ITEMS>
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scan(const BatchPairDev* __restrict__ pairs,
-                                                           const uint32_t* __restrict__ stile_pair, uint64_t n_stiles,
-                                                           uint64_t* __restrict__ status, unsigned* ticket,
-                                                           const uint32_t* flags) {
+                                                           const uint32_t* __restrict__ stile_pair, uint64_t s_begin,
+                                                           uint64_t s_end, uint64_t* __restrict__ status, unsigned* ticket,
+                                                           const uint32_t* flags, const uint32_t* gate) {
+  if (gated_off(gate)) return;
   constexpr int TILE = BATCH_BLOCK * ITEMS;
   static_assert(TILE == BATCH_STILE, "scan tile");
   __shared__ uint32_t s[TILE + TILE / 32];
   __shared__ uint32_t red[BATCH_BLOCK / 32 + 1];
   __shared__ uint64_t s_tile, s_prefix;
   while (true) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    if (threadIdx.x == 0) s_tile = s_begin + atomicAdd(ticket, 1u);
     __syncthreads();
     const uint64_t t = s_tile;
-    if (t >= n_stiles) break;
+    if (t >= s_end) break;
     const BatchPairDev& P = pairs[stile_pair[t]];
     if (batch_skip_build(P, flags)) {
       __syncthreads();  // every thread read s_tile before thread 0 takes the next ticket
@@ -194,8 +199,10 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scan(const BatchPairDev* 
 template <typename KeyT>
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scatter(const BatchPairDev* __restrict__ pairs,
                                                               const uint32_t* __restrict__ ktile_pair,
-                                                              uint64_t n_ktiles, const uint32_t* flags) {
-  for (uint64_t t = blockIdx.x; t < n_ktiles; t += gridDim.x) {
+                                                              uint64_t k_begin, uint64_t k_end, const uint32_t* flags,
+                                                              const uint32_t* gate) {
+  if (gated_off(gate)) return;
+  for (uint64_t t = k_begin + blockIdx.x; t < k_end; t += gridDim.x) {
     const BatchPairDev& P = pairs[ktile_pair[t]];
     if (batch_skip_build(P, flags)) continue;
     const KeyT* keys = static_cast<const KeyT*>(P.keys);
@@ -236,16 +243,18 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scatter(const BatchPairDe
 // the pairs come out in the same order as the single-pair direct probe.
 template <typename KeyT>
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_probe(const BatchPairDev* __restrict__ pairs,
-                                                            const uint32_t* __restrict__ qtile_pair, uint64_t n_qtiles,
-                                                            uint64_t* __restrict__ status, unsigned* ticket,
-                                                            const uint32_t* flags) {
+                                                            const uint32_t* __restrict__ qtile_pair, uint64_t q_begin,
+                                                            uint64_t q_end, uint64_t* __restrict__ status,
+                                                            unsigned* ticket, const uint32_t* flags,
+                                                            const uint32_t* gate) {
+  if (gated_off(gate)) return;
   __shared__ uint64_t red[BATCH_BLOCK / 32 + 1];
   __shared__ uint64_t s_tile, s_prefix;
   while (true) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    if (threadIdx.x == 0) s_tile = q_begin + atomicAdd(ticket, 1u);
     __syncthreads();
     const uint64_t t = s_tile;
-    if (t >= n_qtiles) break;
+    if (t >= q_end) break;
     const BatchPairDev& P = pairs[qtile_pair[t]];
     if (batch_skip_probe(P, flags)) {
       __syncthreads();  // every thread read s_tile before thread 0 takes the next ticket
@@ -526,6 +535,7 @@ struct BatchPlan {
   int n_pairs = 0;
   int key_bytes = 8;
   uint64_t n_ktiles = 0, n_stiles = 0, n_qtiles = 0, n_ltiles = 0;
+  uint64_t n_kd = 0, n_sd = 0, n_qd = 0;  // tiles of the pairs in the direct form (the ungated launches)
   // partitioned form
   uint64_t n_mt = 0, n_mq = 0;      // pass-1 tiles of the keys / of the queries
   uint64_t n_fb = 0, n_fq = 0;      // fine partitions of the tables / of the queries
@@ -584,29 +594,6 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
     d.n_buckets = a.n_buckets;
     d.pair_cap = a.d_pairs ? a.pair_cap : 0;
     d.bm = BucketMap::make(a.n_buckets);
-    const uint64_t kt = (a.n + BATCH_KTILE - 1) / BATCH_KTILE;
-    const uint64_t st = (a.n_buckets + BATCH_STILE - 1) / BATCH_STILE;
-    const uint64_t qt = (a.nq + BATCH_QTILE - 1) / BATCH_QTILE;
-    d.ktile0 = p.n_ktiles;
-    d.stile0 = p.n_stiles;
-    d.qtile0 = p.n_qtiles;
-    d.qtiles = qt;
-    p.n_ktiles += kt;
-    p.n_stiles += st;
-    p.n_qtiles += qt;
-    if (p.n_ktiles >= (1ull << 32) || p.n_stiles >= (1ull << 32) || p.n_qtiles >= (1ull << 32))
-      return lib_fail(HG_ERR_TOO_LARGE, "hg_batch_create: more than 2^32 tiles");
-  }
-  kmap->resize(p.n_ktiles);
-  smap->resize(p.n_stiles);
-  qmap->resize(p.n_qtiles);
-  for (int i = 0; i < n_pairs; i++) {
-    const BatchPairDev& d = (*dev)[i];
-    const uint64_t kt = (d.n + BATCH_KTILE - 1) / BATCH_KTILE;
-    const uint64_t st = (d.n_buckets + BATCH_STILE - 1) / BATCH_STILE;
-    std::fill(kmap->begin() + d.ktile0, kmap->begin() + d.ktile0 + kt, uint32_t(i));
-    std::fill(smap->begin() + d.stile0, smap->begin() + d.stile0 + st, uint32_t(i));
-    std::fill(qmap->begin() + d.qtile0, qmap->begin() + d.qtile0 + d.qtiles, uint32_t(i));
   }
   // Partitioned form: large pairs whose buckets make at most PASS1_GOOD_PARTS
   // fine partitions and whose partitions fit a CTA's shared memory.
@@ -663,6 +650,50 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
   }
   if (!p.smem3q)
     for (auto& d : *dev) d.pq = 0;
+  // Tiles of the direct kernels, numbered pairs in the direct form first, then
+  // the partitioned ones: the ungated launches cover [0, n_kd) (keys),
+  // [0, n_sd) (scans) and [0, n_qd) (queries); the gated fallback launches
+  // the rest, which they redo only when a partitioned pass overflowed.  Pairs
+  // probed in the L2 form never need the direct probe (nothing can overflow)
+  // and get no query tiles.
+  auto assign = [&](bool partitioned_build, bool partitioned_probe) {
+    for (int i = 0; i < n_pairs; i++) {
+      BatchPairDev& d = (*dev)[i];
+      if ((d.pb != 0) == partitioned_build) {
+        d.ktile0 = p.n_ktiles;
+        d.stile0 = p.n_stiles;
+        p.n_ktiles += (d.n + BATCH_KTILE - 1) / BATCH_KTILE;
+        p.n_stiles += (d.n_buckets + BATCH_STILE - 1) / BATCH_STILE;
+      }
+      if (!d.pl && (d.pq != 0) == partitioned_probe) {
+        d.qtile0 = p.n_qtiles;
+        d.qtiles = (d.nq + BATCH_QTILE - 1) / BATCH_QTILE;
+        p.n_qtiles += d.qtiles;
+      }
+    }
+  };
+  for (auto& d : *dev) {
+    d.qtile0 = 0;
+    d.qtiles = 0;
+  }
+  assign(false, false);
+  p.n_kd = p.n_ktiles;
+  p.n_sd = p.n_stiles;
+  p.n_qd = p.n_qtiles;
+  assign(true, true);
+  if (p.n_ktiles >= (1ull << 32) || p.n_stiles >= (1ull << 32) || p.n_qtiles >= (1ull << 32))
+    return lib_fail(HG_ERR_TOO_LARGE, "hg_batch_create: more than 2^32 tiles");
+  kmap->resize(p.n_ktiles);
+  smap->resize(p.n_stiles);
+  qmap->resize(p.n_qtiles);
+  for (int i = 0; i < n_pairs; i++) {
+    const BatchPairDev& d = (*dev)[i];
+    const uint64_t kt = (d.n + BATCH_KTILE - 1) / BATCH_KTILE;
+    const uint64_t st = (d.n_buckets + BATCH_STILE - 1) / BATCH_STILE;
+    std::fill(kmap->begin() + d.ktile0, kmap->begin() + d.ktile0 + kt, uint32_t(i));
+    std::fill(smap->begin() + d.stile0, smap->begin() + d.stile0 + st, uint32_t(i));
+    std::fill(qmap->begin() + d.qtile0, qmap->begin() + d.qtile0 + d.qtiles, uint32_t(i));
+  }
   // pass-1 tiles and fine partitions of the partitioned pairs
   for (int i = 0; i < n_pairs; i++) {
     BatchPairDev& d = (*dev)[i];
@@ -816,26 +847,37 @@ static hg_status batch_launch(const BatchPlan& p, char* ws, cudaStream_t s) {
   }
   // direct form: every pair not partitioned, and partitioned ones if their
   // pass overflowed (the kernels read the flags)
+  // (each kind twice: the pairs in the direct form, then the partitioned
+  // pairs gated on the build's overflow flag, which return at once without it)
   {
     Phase ph(s, "batch_clear");
-    count_launch();
-    k_batch_clear<<<grid_for(std::max<uint64_t>(p.n_stiles, (p.n_pairs + BATCH_BLOCK - 1) / BATCH_BLOCK)), BATCH_BLOCK, 0, s>>>(
-        pairs, p.n_pairs, smap, p.n_stiles, flags);
+    count_launch(2);
+    k_batch_clear<<<grid_for(std::max<uint64_t>(p.n_sd, (p.n_pairs + BATCH_BLOCK - 1) / BATCH_BLOCK)), BATCH_BLOCK, 0, s>>>(
+        pairs, p.n_pairs, smap, 0, p.n_sd, flags, nullptr);
+    k_batch_clear<<<grid_for(p.n_stiles - p.n_sd), BATCH_BLOCK, 0, s>>>(pairs, p.n_pairs, smap, p.n_sd, p.n_stiles,
+                                                                       flags, flags);
   }
-  if (p.n_ktiles) {
+  {
     Phase ph(s, "batch_count");
-    count_launch();
-    k_batch_count<KeyT><<<grid_for(p.n_ktiles), BATCH_BLOCK, 0, s>>>(pairs, kmap, p.n_ktiles, flags);
+    count_launch(2);
+    k_batch_count<KeyT><<<grid_for(p.n_kd), BATCH_BLOCK, 0, s>>>(pairs, kmap, 0, p.n_kd, flags, nullptr);
+    k_batch_count<KeyT><<<grid_for(p.n_ktiles - p.n_kd), BATCH_BLOCK, 0, s>>>(pairs, kmap, p.n_kd, p.n_ktiles, flags,
+                                                                             flags);
   }
   {
     Phase ph(s, "batch_scan");
-    count_launch();
-    k_batch_scan<SCAN_ITEMS><<<grid_for(p.n_stiles), BATCH_BLOCK, 0, s>>>(pairs, smap, p.n_stiles, sstat, ticket, flags);
+    count_launch(2);
+    k_batch_scan<SCAN_ITEMS><<<grid_for(p.n_sd), BATCH_BLOCK, 0, s>>>(pairs, smap, 0, p.n_sd, sstat, ticket, flags,
+                                                                      nullptr);
+    k_batch_scan<SCAN_ITEMS><<<grid_for(p.n_stiles - p.n_sd), BATCH_BLOCK, 0, s>>>(pairs, smap, p.n_sd, p.n_stiles,
+                                                                                   sstat, ticket + 5, flags, flags);
   }
-  if (p.n_ktiles) {
+  {
     Phase ph(s, "batch_scatter");
-    count_launch();
-    k_batch_scatter<KeyT><<<grid_for(p.n_ktiles), BATCH_BLOCK, 0, s>>>(pairs, kmap, p.n_ktiles, flags);
+    count_launch(2);
+    k_batch_scatter<KeyT><<<grid_for(p.n_kd), BATCH_BLOCK, 0, s>>>(pairs, kmap, 0, p.n_kd, flags, nullptr);
+    k_batch_scatter<KeyT><<<grid_for(p.n_ktiles - p.n_kd), BATCH_BLOCK, 0, s>>>(pairs, kmap, p.n_kd, p.n_ktiles, flags,
+                                                                               flags);
   }
   if (p.n_ltiles) {
     Phase ph(s, "batch_l2_probe");
@@ -871,10 +913,13 @@ static hg_status batch_launch(const BatchPlan& p, char* ws, cudaStream_t s) {
     else go(k_fine_probe<KeyT, false, true, FINE_PROBE_BLOCK, PSrc>);
     if (st != HG_OK) return st;
   }
-  if (p.n_qtiles) {
+  {
     Phase ph(s, "batch_probe");
-    count_launch();
-    k_batch_probe<KeyT><<<grid_for(p.n_qtiles), BATCH_BLOCK, 0, s>>>(pairs, qmap, p.n_qtiles, qstat, ticket + 1, flags);
+    count_launch(2);
+    k_batch_probe<KeyT><<<grid_for(p.n_qd), BATCH_BLOCK, 0, s>>>(pairs, qmap, 0, p.n_qd, qstat, ticket + 1, flags,
+                                                                 nullptr);
+    k_batch_probe<KeyT><<<grid_for(p.n_qtiles - p.n_qd), BATCH_BLOCK, 0, s>>>(pairs, qmap, p.n_qd, p.n_qtiles, qstat,
+                                                                             ticket + 6, flags, flags + 1);
   }
   HG_CUDA(cudaPeekAtLastError(), "hg_batch_run: kernel launch");
   return HG_OK;

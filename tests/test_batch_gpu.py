@@ -208,3 +208,30 @@ def test_batch_graph_replay(hg):
     for i in range(len(keys)):
         _check_pair(hg, b, i, keys2[i], queries2[i], buckets[i], wi[i], kb)
     del g
+
+
+def test_batch_large_tables_partitioned_probe(hg):
+    """Pairs whose table exceeds the L2 form's 24 MB budget (2^21 u64 keys with
+    an index) take the partitioned probe; one of them has its queries drawn
+    from a handful of keys, so its query partitions overflow and the gated
+    direct probe redoes the partitioned probes.  Small pairs ride along in
+    the direct form."""
+    import torch
+    rng = np.random.default_rng(5)
+    keys, queries, buckets, wi = [], [], [], []
+    for i, (n, nq, dup) in enumerate([((1 << 21) + 3, 1 << 21, False), (1 << 21, (1 << 21) - 7, True),
+                                       (3000, 2000, False), (100, 5000, False)]):
+        a = oracle.gen_uniform(n, 8, 700 + i)
+        q = oracle.gen_overlap(nq, a, 0.5, 800 + i)
+        if dup:  # every query one of 16 keys of A: a few query partitions hold them all
+            q = a[rng.integers(0, 16, size=nq)]
+        keys.append(a)
+        queries.append(q)
+        buckets.append(n)
+        wi.append(True)
+    caps = [max(_oracle_pair(keys[i], queries[i], buckets[i], wi[i])[3], 1) for i in range(len(keys))]
+    b = hg.Batch([from_np_u(a) for a in keys], [from_np_u(q) for q in queries], buckets, wi, caps).run()
+    torch.cuda.synchronize()
+    assert hg.device_error() == 0
+    for i in range(len(keys)):
+        _check_pair(hg, b, i, keys[i], queries[i], buckets[i], wi[i], 8)

@@ -433,6 +433,8 @@ def run_batched(args, rank, world, local):
                                ctypes.c_void_p(a_views[i].data_ptr()), n, m, 200_000 + i, sptr), "gen")
     B = [int(x) for x in sizes]
     batch = hg.Batch(a_views, q_views, B, with_index=False, pair_caps=B)
+    # size classes picked by the autotuner on this batch, outside the timed region
+    size_classes, tune_ms = batch.autotune()
     for _ in range(args.warmup):
         batch.run()
     torch.cuda.synchronize(dev)
@@ -557,6 +559,7 @@ def run_batched(args, rank, world, local):
                                f"buckets, n_i queries with U(0,1) drawn from A_i, pairs emitted; one "
                                f"hg_batch_run per step",
                    "pairs": args.pairs, "keys_total": n_total, "matches": matches,
+                   "size_classes": size_classes, "autotune_best_ms": tune_ms,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs (%d MiB per set) larger than L2; no flush" % (n_total * kb >> 20)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",

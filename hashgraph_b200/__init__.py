@@ -12,8 +12,8 @@ from __future__ import annotations
 
 import ctypes
 
-from ._capi import (ERR_DEVICE_TIMEOUT, ERR_PAIR_CAPACITY, BatchPair, HGError, build_library, check,
-                    lib, status_str)
+from ._capi import (ERR_DEVICE_TIMEOUT, ERR_PAIR_CAPACITY, BatchPair, BatchParams, HGError, build_library,
+                    check, lib, status_str)
 
 __all__ = [
     "HGError", "Table", "build_library", "lib", "hash_keys", "intersect", "device_error",
@@ -224,7 +224,7 @@ class Batch:
     """
 
     def __init__(self, keys, queries, n_buckets, with_index=False, pair_caps=None, emit=True,
-                 stream=None):
+                 stream=None, params=None):
         torch = _torch()
         n_pairs = len(keys)
         if len(queries) != n_pairs or len(n_buckets) != n_pairs:
@@ -264,9 +264,31 @@ class Batch:
             d.pair_cap = int(pair_caps[i]) if emit else 0
             d.d_count = self.counts.data_ptr() + 8 * i
         self.n_pairs = n_pairs
+        self._descs = descs
         self._h = ctypes.c_void_p()
-        check(lib().hg_batch_create(descs, n_pairs, kb, _stream(stream), ctypes.byref(self._h)),
-              "hg_batch_create")
+        self.params = dict(params) if params else None
+        self._create(stream)
+
+    def _create(self, stream=None):
+        prm = None
+        if self.params is not None:
+            prm = BatchParams(int(self.params["part_min"]), int(self.params["l2_table_bytes"]))
+        check(lib().hg_batch_create_params(self._descs, self.n_pairs, self.key_bytes,
+                                           ctypes.byref(prm) if prm is not None else None, _stream(stream),
+                                           ctypes.byref(self._h)), "hg_batch_create")
+
+    def autotune(self, stream=None) -> tuple[dict, float]:
+        """Times candidate size classes on this batch (hg_batch_autotune; the
+        outputs then hold the batch's results), re-plans the batch with the
+        fastest and returns (params, ms per run)."""
+        best = BatchParams()
+        ms = ctypes.c_float(0.0)
+        check(lib().hg_batch_autotune(self._descs, self.n_pairs, self.key_bytes, _stream(stream),
+                                      ctypes.byref(best), ctypes.byref(ms)), "hg_batch_autotune")
+        self.free(stream)
+        self.params = {"part_min": best.part_min, "l2_table_bytes": best.l2_table_bytes}
+        self._create(stream)
+        return dict(self.params), float(ms.value)
 
     def run(self, stream=None) -> "Batch":
         check(lib().hg_batch_run(self._h, _stream(stream)), "hg_batch_run")

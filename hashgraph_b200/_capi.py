@@ -39,6 +39,11 @@ _i32 = ctypes.c_int32
 _int = ctypes.c_int
 _sz = ctypes.c_size_t
 _pp = ctypes.POINTER(ctypes.c_void_p)
+class BatchParams(ctypes.Structure):
+    """hg_batch_params of include/hashgraph_b200.h."""
+    _fields_ = [("part_min", ctypes.c_uint64), ("l2_table_bytes", ctypes.c_uint64)]
+
+
 class BatchPair(ctypes.Structure):
     """hg_batch_pair of include/hashgraph_b200.h."""
     _fields_ = [
@@ -93,6 +98,10 @@ SIGNATURES = {
     "hg_batch_run": (_i32, [_p, _p]),
     "hg_batch_device_bytes": (_i32, [_p, ctypes.POINTER(_sz)]),
     "hg_batch_free": (None, [_p, _p]),
+    "hg_batch_params_default": (_i32, [ctypes.POINTER(BatchParams)]),
+    "hg_batch_create_params": (_i32, [ctypes.POINTER(BatchPair), _int, _int, ctypes.POINTER(BatchParams), _p, _pp]),
+    "hg_batch_autotune": (_i32, [ctypes.POINTER(BatchPair), _int, _int, _p, ctypes.POINTER(BatchParams),
+                                 ctypes.POINTER(ctypes.c_float)]),
     "hg_batch_build_intersect": (_i32, [ctypes.POINTER(BatchPair), _int, _int, _p]),
     "hg_table_save": (_i32, [_p, ctypes.c_char_p, _p]),
     "hg_table_load": (_i32, [ctypes.c_char_p, _pp, _p]),

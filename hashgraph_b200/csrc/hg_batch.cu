@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_probe(const BatchPairDev*
   }
 }
 
-// L2 form of a large pair's probe: the pair's table (at most BATCH_L2_TABLE
+// L2 form of a large pair's probe: the pair's table (at most l2_table_bytes
 // bytes) was built just before and is read from L2 while the CTAs, which take
 // tiles in pair order from a ticket, work on it.  Per thread BATCH_LQPT
 // queries side by side (bucket bounds, first entries, the rest of each
@@ -527,9 +527,9 @@ struct BatchProbe {
 };
 
 // Host-side batch: the plan, the device workspace and the descriptors.
-constexpr uint64_t BATCH_PART_MIN = 1ull << 14;  // keys (queries) from which a pair is partitioned
+constexpr uint64_t BATCH_PART_MIN = 1ull << 14;  // default: keys (queries) from which a pair is partitioned
 constexpr uint32_t BATCH_FINE_LOG2 = 11;          // fine width of the partitioned build
-constexpr uint64_t BATCH_L2_TABLE = uint64_t(24) << 20;  // table bytes up to which a large pair's probe reads L2
+constexpr uint64_t BATCH_L2_TABLE = uint64_t(24) << 20;  // default: table bytes up to which a large pair's probe reads L2
 
 struct BatchPlan {
   int n_pairs = 0;
@@ -562,7 +562,8 @@ struct hg_batch {
 
 namespace hg {
 
-static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_bytes, BatchPlan* plan,
+static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_bytes, const hg_batch_params& prm,
+                            BatchPlan* plan,
                             std::vector<BatchPairDev>* dev, std::vector<uint32_t>* kmap,
                             std::vector<uint32_t>* smap, std::vector<uint32_t>* qmap,
                             std::vector<uint32_t>* mtmap, std::vector<uint32_t>* mqmap,
@@ -602,7 +603,7 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
   for (int i = 0; i < n_pairs; i++) {
     BatchPairDev& d = (*dev)[i];
     const double per_b = double(d.n) * double(wb) / double(d.n_buckets);
-    d.pb = (d.n >= BATCH_PART_MIN && (d.n_buckets + wb - 1) / wb <= PASS1_GOOD_PARTS && per_b <= 4096.0) ? 1u : 0u;
+    d.pb = (d.n >= prm.part_min && (d.n_buckets + wb - 1) / wb <= PASS1_GOOD_PARTS && per_b <= 4096.0) ? 1u : 0u;
     if (d.pb) {
       p.capf = std::max(p.capf, slack_capacity(per_b, 64));
       p.wi_b = p.wi_b || d.idx_out != nullptr;
@@ -617,7 +618,7 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
   // the L2 form for large pairs whose whole table fits the L2 budget
   for (auto& d : *dev) {
     const uint64_t table_bytes = 4 * (d.n_buckets + 1) + d.n * (key_bytes + (d.idx_out ? 4 : 0));
-    d.pl = (d.nq >= BATCH_PART_MIN && d.n > 0 && table_bytes <= BATCH_L2_TABLE) ? 1u : 0u;
+    d.pl = (d.nq >= prm.part_min && d.n > 0 && table_bytes <= prm.l2_table_bytes) ? 1u : 0u;
   }
   // the probe's fine width: the widest whose staging fits one CTA
   for (uint32_t lq = 12; lq >= 10; lq--) {
@@ -627,7 +628,7 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
     for (auto& d : *dev) {
       const double per_q = double(d.nq) * double(wq) / double(d.n_buckets);
       const double per_a = double(d.n) * double(wq) / double(d.n_buckets);
-      d.pq = (!d.pl && d.nq >= BATCH_PART_MIN && d.n > 0 && (d.n_buckets + wq - 1) / wq <= PASS1_GOOD_PARTS &&
+      d.pq = (!d.pl && d.nq >= prm.part_min && d.n > 0 && (d.n_buckets + wq - 1) / wq <= PASS1_GOOD_PARTS &&
               per_q <= 8192.0 && per_a <= 8192.0) ? 1u : 0u;
       if (!d.pq) continue;
       any = true;
@@ -929,14 +930,25 @@ static hg_status batch_launch(const BatchPlan& p, char* ws, cudaStream_t s) {
 
 using namespace hg;
 
-extern "C" hg_status hg_batch_create(const hg_batch_pair* pairs, int n_pairs, int key_bytes, hg_stream_t stream,
-                                     hg_batch** out) {
+extern "C" hg_status hg_batch_params_default(hg_batch_params* params) {
+  if (!params) return HG_ERR_INVALID_ARGUMENT;
+  params->part_min = BATCH_PART_MIN;
+  params->l2_table_bytes = BATCH_L2_TABLE;
+  return HG_OK;
+}
+
+extern "C" hg_status hg_batch_create_params(const hg_batch_pair* pairs, int n_pairs, int key_bytes,
+                                            const hg_batch_params* params, hg_stream_t stream, hg_batch** out) {
   if (!out) return HG_ERR_INVALID_ARGUMENT;
   *out = nullptr;
+  hg_batch_params prm;
+  hg_batch_params_default(&prm);
+  if (params) prm = *params;
+  if (prm.part_min == 0) return lib_fail(HG_ERR_INVALID_ARGUMENT, "hg_batch_create: part_min must be positive");
   BatchPlan plan;
   std::vector<BatchPairDev> dev;
   std::vector<uint32_t> kmap, smap, qmap, mtmap, mqmap, fbmap, fqmap, lmap;
-  hg_status st = batch_plan(pairs, n_pairs, key_bytes, &plan, &dev, &kmap, &smap, &qmap, &mtmap, &mqmap, &fbmap,
+  hg_status st = batch_plan(pairs, n_pairs, key_bytes, prm, &plan, &dev, &kmap, &smap, &qmap, &mtmap, &mqmap, &fbmap,
                             &fqmap, &lmap);
   if (st != HG_OK) return st;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -972,6 +984,11 @@ extern "C" hg_status hg_batch_create(const hg_batch_pair* pairs, int n_pairs, in
   return HG_OK;
 }
 
+extern "C" hg_status hg_batch_create(const hg_batch_pair* pairs, int n_pairs, int key_bytes, hg_stream_t stream,
+                                     hg_batch** out) {
+  return hg_batch_create_params(pairs, n_pairs, key_bytes, nullptr, stream, out);
+}
+
 extern "C" hg_status hg_batch_run(const hg_batch* b, hg_stream_t stream) {
   if (!b) return HG_ERR_INVALID_ARGUMENT;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -999,4 +1016,79 @@ extern "C" hg_status hg_batch_build_intersect(const hg_batch_pair* pairs, int n_
   st = hg_batch_run(b, stream);
   hg_batch_free(b, stream);
   return st;
+}
+
+// The size classes of a batch -- direct form below part_min keys, L2 form of
+// the probe for tables up to l2_table_bytes, partitioned forms above -- set
+// the tile and thread shapes each pair gets.  The autotuner times candidate
+// boundaries on the caller's own batch (coordinate search: part_min over
+// 2^12 .. 2^16 with the default L2 budget, then the L2 budget over 0, 12, 24
+// and 48 MB with the best part_min; each candidate one warm-up run and the
+// best of two timed runs) and returns the fastest.  It runs the batch, so the
+// outputs hold the last candidate's results (the same results: every form
+// computes the same tables and the same pair sets).
+extern "C" hg_status hg_batch_autotune(const hg_batch_pair* pairs, int n_pairs, int key_bytes, hg_stream_t stream,
+                                       hg_batch_params* best, float* best_ms) {
+  if (!best) return HG_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  hg_batch_params cur;
+  hg_batch_params_default(&cur);
+  float cur_ms = -1.f;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  HG_CUDA(cudaEventCreate(&e0), "hg_batch_autotune: event");
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cuda_fail(ce, "hg_batch_autotune: event");
+  }
+  auto time_params = [&](const hg_batch_params& prm, float* ms) -> hg_status {
+    hg_batch* b = nullptr;
+    hg_status st = hg_batch_create_params(pairs, n_pairs, key_bytes, &prm, stream, &b);
+    if (st != HG_OK) return st;
+    float bestc = -1.f;
+    for (int r = 0; r < 3 && st == HG_OK; r++) {
+      cudaEventRecord(e0, s);
+      st = hg_batch_run(b, stream);
+      cudaEventRecord(e1, s);
+      const cudaError_t e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) st = cuda_fail(e, "hg_batch_autotune: run");
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (st == HG_OK && r > 0 && (bestc < 0.f || t < bestc)) bestc = t;  // run 0 warms up
+    }
+    hg_batch_free(b, stream);
+    *ms = bestc;
+    return st;
+  };
+  hg_status st = time_params(cur, &cur_ms);
+  const uint64_t part_mins[] = {1ull << 12, 1ull << 13, 1ull << 15, 1ull << 16};
+  for (uint64_t pm : part_mins) {
+    if (st != HG_OK) break;
+    hg_batch_params c = cur;
+    c.part_min = pm;
+    float t = 0.f;
+    st = time_params(c, &t);
+    if (st == HG_OK && t < cur_ms) {
+      cur = c;
+      cur_ms = t;
+    }
+  }
+  const uint64_t l2s[] = {0ull, uint64_t(12) << 20, uint64_t(48) << 20};
+  for (uint64_t l2 : l2s) {
+    if (st != HG_OK) break;
+    hg_batch_params c = cur;
+    c.l2_table_bytes = l2;
+    float t = 0.f;
+    st = time_params(c, &t);
+    if (st == HG_OK && t < cur_ms) {
+      cur = c;
+      cur_ms = t;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != HG_OK) return st;
+  *best = cur;
+  if (best_ms) *best_ms = cur_ms;
+  return HG_OK;
 }

@@ -275,6 +275,23 @@ hg_status hg_batch_create(const hg_batch_pair* pairs, int n_pairs, int key_bytes
  * into a CUDA graph and the graph replayed after the callers' input buffers
  * are refilled. */
 hg_status hg_batch_run(const hg_batch* batch, hg_stream_t stream);
+/* The size classes of a batch: pairs of at least part_min keys take the
+ * partitioned build, and (queries) the L2 form of the probe when their whole
+ * table (offsets, keys, index) is at most l2_table_bytes (0: never), the
+ * partitioned probe otherwise; smaller pairs take the direct form. */
+typedef struct hg_batch_params {
+  uint64_t part_min;        /* default 2^14 */
+  uint64_t l2_table_bytes;  /* default 24 MB */
+} hg_batch_params;
+hg_status hg_batch_params_default(hg_batch_params* params);
+/* hg_batch_create with explicit size classes (params NULL: the defaults). */
+hg_status hg_batch_create_params(const hg_batch_pair* pairs, int n_pairs, int key_bytes,
+                                 const hg_batch_params* params, hg_stream_t stream, hg_batch** out);
+/* Autotuner of the size classes: times candidate boundaries on this batch
+ * (it runs the batch: the outputs hold its results) and returns the fastest
+ * in *best and its time in *best_ms (optional).  Synchronises the stream. */
+hg_status hg_batch_autotune(const hg_batch_pair* pairs, int n_pairs, int key_bytes, hg_stream_t stream,
+                            hg_batch_params* best, float* best_ms);
 /* Device bytes the batch holds (workspace and descriptors). */
 hg_status hg_batch_device_bytes(const hg_batch* batch, size_t* bytes);
 /* Frees the batch's device memory stream-ordered on `stream`. */

@@ -235,3 +235,40 @@ def test_batch_large_tables_partitioned_probe(hg):
     assert hg.device_error() == 0
     for i in range(len(keys)):
         _check_pair(hg, b, i, keys[i], queries[i], buckets[i], wi[i], 8)
+
+
+@pytest.mark.parametrize("params", [{"part_min": 1 << 10, "l2_table_bytes": 0},
+                                    {"part_min": 1 << 12, "l2_table_bytes": 1 << 20},
+                                    {"part_min": 1 << 20, "l2_table_bytes": 24 << 20}])
+def test_batch_size_classes_match_oracle(hg, params):
+    """Every choice of size-class boundaries gives the oracle's results: with
+    part_min 2^10 and no L2 form, mid-sized pairs take the partitioned probe;
+    with a 1 MB L2 budget some take the L2 form and some the partitioned one;
+    with part_min 2^20 everything is direct."""
+    import torch
+    keys, queries, buckets, wi = _make_batch_inputs(8, 40, 31, max_log2=16)
+    caps = [max(_oracle_pair(keys[i], queries[i], buckets[i], wi[i])[3], 1) for i in range(len(keys))]
+    b = hg.Batch([from_np_u(a) for a in keys], [from_np_u(q) for q in queries], buckets, wi, caps,
+                 params=params).run()
+    torch.cuda.synchronize()
+    assert hg.device_error() == 0
+    for i in range(len(keys)):
+        _check_pair(hg, b, i, keys[i], queries[i], buckets[i], wi[i], 8)
+
+
+def test_batch_autotune(hg):
+    """The autotuner returns boundaries from its candidate set and the
+    re-planned batch still gives the oracle's results."""
+    import torch
+    keys, queries, buckets, wi = _make_batch_inputs(8, 48, 41, max_log2=17)
+    caps = [max(_oracle_pair(keys[i], queries[i], buckets[i], wi[i])[3], 1) for i in range(len(keys))]
+    b = hg.Batch([from_np_u(a) for a in keys], [from_np_u(q) for q in queries], buckets, wi, caps)
+    params, ms = b.autotune()
+    assert params["part_min"] in (1 << 12, 1 << 13, 1 << 14, 1 << 15, 1 << 16)
+    assert params["l2_table_bytes"] in (0, 12 << 20, 24 << 20, 48 << 20)
+    assert ms > 0
+    b.run()
+    torch.cuda.synchronize()
+    assert hg.device_error() == 0
+    for i in range(len(keys)):
+        _check_pair(hg, b, i, keys[i], queries[i], buckets[i], wi[i], 8)

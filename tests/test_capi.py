@@ -195,3 +195,19 @@ def test_shard_argument_checks_without_device(capi):
     assert L.hg_shard_route_workspace_size(1000, 8, ctypes.byref(out)) == 0 and out.value > 0
     assert L.hg_shard_histogram(f, 10, 8, 100, 40000, f, None) == -6
     assert L.hg_shard_histogram(f, 10, 8, 0, 16, f, None) == -1
+
+
+def test_batch_params_without_device(capi):
+    """Size-class defaults, and argument checks of the parameterised create and
+    the autotuner before any device call."""
+    L = capi.lib()
+    prm = capi.BatchParams()
+    assert L.hg_batch_params_default(ctypes.byref(prm)) == 0
+    assert (prm.part_min, prm.l2_table_bytes) == (1 << 14, 24 << 20)
+    assert L.hg_batch_params_default(None) == -1
+    h = ctypes.c_void_p()
+    pairs = (capi.BatchPair * 1)()
+    bad = capi.BatchParams(0, 1 << 20)
+    assert L.hg_batch_create_params(pairs, 1, 8, ctypes.byref(bad), None, ctypes.byref(h)) == -1
+    assert L.hg_batch_create_params(pairs, 1, 8, None, None, None) == -1
+    assert L.hg_batch_autotune(pairs, 1, 8, None, None, None) == -1

@@ -255,8 +255,11 @@ extern "C" hg_status hg_shard_histogram(const void* d_keys, uint64_t n, int key_
   // ceil(2^64 / width) for width >= 2; 0 marks width 1
   const uint64_t magic = width == 1 ? 0ull : UINT64_MAX / width + 1;
   const size_t smem = size_t(n_bins) * 4;
+  // two CTAs per SM: each CTA flushes up to n_bins 64-bit atomics at its end,
+  // so fewer, longer-running CTAs keep that flush small (2^24 keys, 16000
+  // bins: 6.9M L2 atomic sectors per launch with 8 CTAs per SM)
   const uint64_t chunks = (n + uint64_t(HIST_BLOCK) * HIST_V - 1) / (uint64_t(HIST_BLOCK) * HIST_V);
-  const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(chunks, uint64_t(device_sm_count()) * 8)));
+  const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(chunks, uint64_t(device_sm_count()) * 2)));
   Phase ph(s, "shard_histogram");
   count_launch();
   if (key_bytes == 8) {

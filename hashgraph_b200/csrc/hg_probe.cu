@@ -527,6 +527,11 @@ __global__ void __launch_bounds__(CPROBE_BLOCK)
     for (int j = 0; j < QPT; j++) {
       const uint32_t r = r0 + j * CPROBE_BLOCK + threadIdx.x;
       key[j] = r < m ? __ldcs(qk + r) : KeyT(0);
+      // the position is read only at emission, after the tile's scan: bring
+      // its line into L2 now (no register held), so that read waits on L2
+      if constexpr (EMIT) {
+        if (r < m) asm volatile("prefetch.global.L2 [%0];" ::"l"(qi + r));
+      }
     }
 #pragma unroll
     for (int j = 0; j < QPT; j++) {

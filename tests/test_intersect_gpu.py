@@ -186,3 +186,31 @@ def test_partitioned_probe_of_unaligned_table(hg):
     assert c == oc
     np.testing.assert_array_equal(_sorted_pairs(to_np_u(pairs[:c], 4)), _sorted_pairs(op))
     assert hg.device_error() == 0
+
+
+@pytest.mark.parametrize("probe_path", [0, 1, 2])
+def test_intersect_zipf_count(hg, probe_path):
+    """Zipf(1.1) keys on both sides (a few keys hold most of the mass): the
+    exact multiset-join count; long buckets for the head keys."""
+    cdf = oracle.zipf_cdf(1 << 14, 1.1)
+    a = oracle.gen_zipf(1 << 16, 8, cdf, 21)
+    q = oracle.gen_zipf(1 << 16, 8, cdf, 22)
+    t = hg.Table.build(from_np_u(a), 1 << 16, with_index=True)
+    count, _ = t.intersect(from_np_u(q), emit=False, path=probe_path)
+    assert int(count.item()) == oracle.join_count(a, q)
+    assert hg.device_error() == 0
+
+
+@pytest.mark.parametrize("probe_path", [1, 2])
+def test_intersect_one_query_key_overflows(hg, probe_path):
+    """Every query is the same key: its bucket range gets all the queries,
+    overflows its slots in pass 1, and the gated direct probe answers."""
+    a = oracle.gen_uniform(1 << 15, 8, 31)
+    q = np.full(10_000, a[5], dtype=np.uint64)
+    t = hg.Table.build(from_np_u(a), 1 << 15, with_index=True)
+    count, pairs = t.intersect(from_np_u(q), pair_cap=10_000, path=probe_path)
+    assert int(count.item()) == 10_000
+    p = to_np_u(pairs, 4)
+    assert np.all(p[:, 0] == 5)
+    np.testing.assert_array_equal(np.sort(p[:, 1]), np.arange(10_000, dtype=np.uint32))
+    assert hg.device_error() == 0

@@ -934,7 +934,10 @@ hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_in
     p.g.smem2 = split_smem(p.g.split_log2, key_bytes, with_index, p.g.n_parts);
     part_ok = p.g.smem1 <= SMEM_BUDGET && p.g.smem2 <= SMEM_BUDGET;
   }
-  const uint64_t footprint = n * (key_bytes + rec) + 4 * n_buckets;
+  // the partitioned path pays off with many keys; a sparse table (few keys,
+  // many buckets) stays direct, whose workspace is O(buckets / 4096) where the
+  // partitioned one keeps slack slots in every partition (O(buckets))
+  const uint64_t footprint = n * (key_bytes + rec);
   int path = force_path;
   if (path < 0) path = (part_ok && footprint > (48ull << 20)) ? BUILD_PARTITIONED : BUILD_DIRECT;
   // A table too dense to stage a fine partition in shared memory (a few

@@ -211,3 +211,49 @@ def test_batch_params_without_device(capi):
     assert L.hg_batch_create_params(pairs, 1, 8, ctypes.byref(bad), None, ctypes.byref(h)) == -1
     assert L.hg_batch_create_params(pairs, 1, 8, None, None, None) == -1
     assert L.hg_batch_autotune(pairs, 1, 8, None, None, None) == -1
+
+
+@pytest.mark.parametrize("kb", [4, 8])
+@pytest.mark.parametrize("with_index", [0, 1])
+def test_planner_over_shapes(capi, kb, with_index):
+    """Every build and probe plan over a grid of table shapes succeeds, and the
+    workspaces stay within their bounds: the coarse probe holds one pass of
+    the query records (+ slack), the partitioned forms two, the direct forms
+    only status words."""
+    L = capi.lib()
+    out = ctypes.c_size_t(0)
+    for n in (0, 1, 1000, 1 << 20, 1 << 26, (1 << 30) - 1):
+        for B in (1, 7, max(n, 1), 2 * max(n, 1), 1 << 32):
+            if B > (1 << 32):
+                continue
+            rec = kb + 4 * with_index
+            for path in (-1, 0, 1):
+                assert L.hg_build_workspace_size_path(n, kb, B, with_index, path, ctypes.byref(out)) == 0
+                # records twice with slack, plus per-partition slack slots and counters on
+                # the partitioned path (up to about 0.15 byte per bucket for a sparse table;
+                # the planner takes it from 48 MB of keys on, so a near-empty table with
+                # many buckets stays direct)
+                per_bucket = B // 512 if path == 0 else B // 6
+                assert out.value <= 2.6 * n * rec + per_bucket + (64 << 20), (n, B, path, out.value)
+            nq = n
+            for path in (-1, 0, 1, 2):
+                assert L.hg_intersect_workspace_size_path(n, with_index, B, nq, kb, 1, path,
+                                                          ctypes.byref(out)) == 0, (n, B, path)
+                bound = {0: 8 * (nq // 1024 + 1) + 4096,
+                         1: 2.6 * nq * (kb + 4) + B // 6 + (64 << 20),
+                         2: 1.3 * nq * (kb + 4) + B // 512 + (64 << 20)}
+                # the planner's own choice (-1) is the direct or the coarse probe here
+                assert out.value <= bound[path if path >= 0 else 2] + 8 * (nq // 1024 + 1), (n, B, path,
+                                                                                             out.value)
+    # beyond the 32-bit limits: a clear error, no plan
+    assert L.hg_build_workspace_size(1 << 32, kb, 1 << 20, with_index, ctypes.byref(out)) == -6
+    assert L.hg_intersect_workspace_size(1 << 20, with_index, 1 << 20, 1 << 32, kb, 1, ctypes.byref(out)) == -6
+
+
+def test_sparse_table_plans_direct(capi):
+    """One key into 2^32 buckets: the planner keeps the direct path and its
+    workspace of scan status words (8 MB), not the partitioned one's slack."""
+    L = capi.lib()
+    out = ctypes.c_size_t(0)
+    assert L.hg_build_workspace_size(1, 8, 1 << 32, 1, ctypes.byref(out)) == 0
+    assert out.value < (16 << 20)

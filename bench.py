@@ -4,7 +4,8 @@
                     [--workload large|large_zipf|small|capacity_lf1|capacity_lf05|capacity_lf2]
 
 One step = build table A from n keys resident in HBM, then intersect n query
-keys against it (pairs emitted).  Metric: build & intersect keys/s = n (keys
+keys against it (pairs emitted; count only for large_zipf, whose output would
+be about 1.4e15 pairs).  Metric: build & intersect keys/s = n (keys
 per set) / (t_build + t_intersect).  Default workload (N=1): A = 2^28 uint64
 keys uniform (seed 3), queries = 2^28 uint64 keys with 25% drawn from A,
 n_buckets = 2^28.  Under torchrun every rank runs its own replica (weak
@@ -12,7 +13,11 @@ scaling; no data-path collective); the step time is the max over ranks.
 
 Prints ONE JSON line on rank 0.  `--impl reference` times the CPU
 implementation of the same algorithm (the oracle's multithreaded build +
-probe, on all host threads) on a bounded sample of the same workload.
+probe, on all host threads) on the same workload (a 2^28-key sample of the
+2^30-key capacity workloads).  On the large and small workloads our arm also
+times, outside its own timed region, the reference's own MultiHashGraph
+(built for sm_100a from its sources into oracle/_ref/) on the same inputs
+(`reference_gpu`).
 """
 from __future__ import annotations
 
@@ -34,6 +39,8 @@ UNIT = "keys/s"
 WORKLOADS = {
     # name: (key_bytes, n, n_buckets_fn, kind, seed_a, seed_q, overlap, with_index)
     "large": (8, 1 << 28, lambda n: n, "uniform", 3, 30, 0.25, False),
+    # skewed variant of the large workload: Zipf(1.1) over one 2^24-key universe, count only
+    "large_zipf": (8, 1 << 28, lambda n: n, "zipf", 3, 30, 0.0, False),
     "small": (4, 1 << 20, lambda n: n, "uniform", 1, 2, 0.5, False),
     "capacity_lf1": (4, 1 << 30, lambda n: n, "uniform", 4, 40, 0.1, True),
     "capacity_lf05": (4, 1 << 30, lambda n: 2 * n, "uniform", 4, 40, 0.1, True),
@@ -201,6 +208,8 @@ def algorithmic_bytes(phase, kb, n, nq, B, with_index, pairs):
     pass; the fine passes add the 4-byte offsets and the 8-byte pairs."""
     rec = kb + (4 if with_index else 0)
     qrec = kb + 4
+    if phase.startswith("fallback_"):  # the gated direct kernels do the same role's work
+        phase = phase[len("fallback_"):]
     return {
         # build
         "multisplit": n * kb + n * rec,
@@ -220,6 +229,8 @@ def algorithmic_bytes(phase, kb, n, nq, B, with_index, pairs):
         "coarse_probe_count": nq * qrec + n * rec + 4 * (B + 1),
         "probe_emit": nq * kb + n * rec + 4 * (B + 1) + 8 * pairs,
         "probe_count": nq * kb + n * rec + 4 * (B + 1),
+        # the heavy-key count reads at most every key of A once
+        "heavy_keys": n * kb,
     }.get(phase)
 
 
@@ -280,7 +291,17 @@ def run_ours(args, rank, world, local):
     if hg.device_error() != 0:
         raise RuntimeError("device error during warm-up")
 
-    # ---- timed region: inputs resident in HBM (2^28 x 8 B per set >> 126 MB L2)
+    # ---- timed region: inputs resident in HBM.  Sets larger than L2 (126 MB)
+    # need no flush; smaller ones get L2 flushed (a 256 MiB buffer written)
+    # before every timed step, outside the step's events.
+    l2_bytes = 126 << 20
+    flush = None
+    if (n + nq) * kb < 2 * l2_bytes:
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+        l2_note = ("inputs fit in L2 (each set %.1f MiB vs 126 MB L2): L2 flushed before every timed step by "
+                   "writing a 256 MiB buffer (outside the step's events)" % (n * kb / 2**20))
+    else:
+        l2_note = "inputs larger than L2 (each set %d MiB vs 126 MB L2); no flush" % (n * kb >> 20)
     hg.profile_enable(True)
     hg.profile_read()
     clocks = ClockSampler(local)
@@ -291,6 +312,8 @@ def run_ours(args, rank, world, local):
     clocks.start()
     time.sleep(0.3)
     for k in range(args.steps):
+        if flush is not None:
+            flush.fill_(k & 0xFF)
         ev[2 * k].record(stream)
         step(a_keys, q_keys)
         ev[2 * k + 1].record(stream)
@@ -300,6 +323,7 @@ def run_ours(args, rank, world, local):
     clk = clocks.stop()
     phases = hg.profile_read()
     hg.profile_enable(False)
+    del flush
     step_ms = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
     total_ms = sum(step_ms)
     total_ms_max = max_over_ranks(total_ms, world)
@@ -357,7 +381,18 @@ def run_ours(args, rank, world, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
-        cpu = cpu_baseline(args.workload, n_sample=args.cpu_sample)
+        cpu = cpu_baseline(args.workload, n_sample=cpu_sample_size(args, n))
+
+    # the reference's own GPU build + intersect on the same inputs, outside our
+    # timed region, with this process's device memory released first
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.skip_ref_gpu and kind == "uniform":
+        table = ws = pairs = count = a_keys = q_keys = None  # noqa: F841 (releases the device buffers)
+        import gc
+        gc.collect()
+        torch.cuda.synchronize(dev)
+        torch.cuda.empty_cache()
+        ref_gpu = reference_gpu(args.workload, n, value)
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -368,7 +403,7 @@ def run_ours(args, rank, world, local):
                    "n_buckets": B, "key_bytes": kb, "with_index": with_index, "emit_pairs": emit,
                    "matches": n_matches, "build_path": args.build_path, "probe_path": args.probe_path,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (each set %d MiB vs 126 MB L2); no flush" % (n * kb >> 20)},
+                   "l2": l2_note},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "traffic": measured_traffic(dom, kb, with_index, n, nq, B),
@@ -385,9 +420,73 @@ def run_ours(args, rank, world, local):
                           "intersect_frac_of_measured_hbm": isect_bytes / (probe_ms * 1e-3) / 1e9 / peak if probe_ms else None},
         "phases_ms": phase_avg, "phase_share": phase_share,
         "clocks": clk, "e2e": e2e, "gpu_launches": launches, "cpu_baseline": cpu,
+        "reference_gpu": ref_gpu,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def reference_gpu(workload, n, our_value, repeats=3):
+    """Times the reference's own MultiHashGraph with gpuCount = 1 (built for
+    sm_100a from its unmodified sources into oracle/_ref/ by oracle/Makefile)
+    on the same seeded inputs as our arm, through its public API as its test
+    main drives it: construct A and B, build A, build B, intersect, timed with
+    CUDA events (oracle/ref_multi_driver.cu).  The sequence runs `repeats`
+    times in one process; the first run is what the reference's test main
+    times (it includes the first touch of its managed memory), the best run
+    is its steady state, against which our ratio is taken."""
+    import tempfile
+
+    import numpy as np
+
+    import oracle
+    kb, _, bfn, kind, seed_a, seed_q, overlap, with_index = WORKLOADS[workload]
+    exe = oracle.ref_binary("ref_multi" if kb == 8 else "ref_multi32")
+    if exe is None:
+        return {"unavailable": "oracle/_ref/ref_multi* not built (the reference sources were absent at build time)"}
+    B = bfn(n)
+    a = oracle.gen_uniform(n, kb, seed_a)
+    q = oracle.gen_overlap(n, a, overlap, seed_q)
+    with tempfile.TemporaryDirectory() as td:
+        fa, fq = os.path.join(td, "a.bin"), os.path.join(td, "q.bin")
+        a.tofile(fa)
+        q.tofile(fq)
+        del a, q
+        try:
+            r = subprocess.run([exe, fa, str(n), fq, str(n), str(B), "-", "1", str(repeats)], capture_output=True,
+                               text=True, timeout=900)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": "reference run exceeded 900 s"}
+    if r.returncode != 0:
+        return {"unavailable": f"reference run failed (rc {r.returncode}): {r.stderr.strip()[-300:]}"}
+    runs = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if not runs:
+        return {"unavailable": "reference run printed no timing"}
+    best = min(runs, key=lambda x: x["total_s"])
+    first = runs[0]
+
+    def summary(x):
+        bi = x["build_a_s"] + x["intersect_s"]
+        return {"build_a_ms": x["build_a_s"] * 1e3, "build_b_ms": x["build_b_s"] * 1e3,
+                "intersect_ms": x["intersect_s"] * 1e3, "composite_ms": x["total_s"] * 1e3,
+                "build_a_plus_intersect_keys_per_s": n / bi if bi > 0 else None,
+                "composite_keys_per_s": n / x["total_s"] if x["total_s"] > 0 else None}
+
+    b = summary(best)
+    return {"impl": "reference MultiHashGraph (gpuCount 1, sm_100a, unmodified sources; oracle/_ref)",
+            "workload": "same seeded inputs as our arm; the reference builds both sets into tables "
+                        "(its intersect joins two tables) and emits the matched keys",
+            "runs": len(runs), "first_run": summary(first), "best_run": b,
+            "ours_over_reference_build_a_plus_intersect": (our_value / b["build_a_plus_intersect_keys_per_s"]
+                                                           if b["build_a_plus_intersect_keys_per_s"] else None),
+            "ours_over_reference_composite": (our_value / b["composite_keys_per_s"]
+                                              if b["composite_keys_per_s"] else None)}
+
+
+def cpu_sample_size(args, n):
+    """Keys per set the CPU arm processes: the whole workload up to 2^28 keys
+    per set (about 3 s per step on 16 host threads), a 2^28 sample beyond."""
+    return min(n, args.cpu_sample) if args.cpu_sample else min(n, 1 << 28)
 
 
 # ---------------------------------------------------------------------------
@@ -485,13 +584,16 @@ def run_batched(args, rank, world, local):
     compulsory = n_total * kb * 2 + 4 * sum_b + (n_total * kb * 2 + 4 * sum_b + 8 * matches)
     step_s = total_ms / args.steps * 1e-3
 
-    # the same pairs as one build + intersect call each (the launch-bound form)
-    ws_b = ctypes.c_size_t(0)
-    ws_q = ctypes.c_size_t(0)
-    nmax = int(sizes.max())
-    hg._capi.check(L.hg_build_workspace_size_path(nmax, kb, nmax, 0, 0, ctypes.byref(ws_b)), "ws")
-    hg._capi.check(L.hg_intersect_workspace_size_path(nmax, 0, nmax, nmax, kb, 1, 0, ctypes.byref(ws_q)), "ws")
-    ws = torch.empty(max(ws_b.value, ws_q.value, 1), dtype=torch.uint8, device=dev)
+    # the same pairs as one build + intersect call each (the launch-bound
+    # form), every call on the planner's own path choice, as a user would call
+    ws_need = 1
+    for nn in sorted(set(int(x) for x in sizes)):
+        ws_b = ctypes.c_size_t(0)
+        ws_q = ctypes.c_size_t(0)
+        hg._capi.check(L.hg_build_workspace_size_path(nn, kb, nn, 0, -1, ctypes.byref(ws_b)), "ws")
+        hg._capi.check(L.hg_intersect_workspace_size_path(nn, 0, nn, nn, kb, 1, -1, ctypes.byref(ws_q)), "ws")
+        ws_need = max(ws_need, ws_b.value, ws_q.value)
+    ws = torch.empty(ws_need, dtype=torch.uint8, device=dev)
 
     def plain_step():
         for i in range(args.pairs):
@@ -499,13 +601,13 @@ def run_batched(args, rank, world, local):
             hg._capi.check(L.hg_build_into_path(
                 ctypes.c_void_p(a_views[i].data_ptr()), n, kb, n, ctypes.c_void_p(batch.offsets[i].data_ptr()),
                 ctypes.c_void_p(batch.table_keys[i].data_ptr()), None, ctypes.c_void_p(ws.data_ptr()),
-                ws.numel(), 0, sptr), "plain build")
+                ws.numel(), -1, sptr), "plain build")
             hg._capi.check(L.hg_intersect_into_path(
                 ctypes.c_void_p(batch.offsets[i].data_ptr()), ctypes.c_void_p(batch.table_keys[i].data_ptr()),
                 None, n, n, kb, ctypes.c_void_p(q_views[i].data_ptr()), n, None,
                 ctypes.c_void_p(batch.pairs[i].data_ptr()), n,
                 ctypes.c_void_p(batch.counts.data_ptr() + 8 * i), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
-                0, sptr), "plain intersect")
+                -1, sptr), "plain intersect")
 
     plain_step()
     torch.cuda.synchronize(dev)
@@ -569,7 +671,7 @@ def run_batched(args, rank, world, local):
                           "frac_of_measured_hbm": compulsory / step_s / 1e9 / peak},
         "plain_calls": {"ms_per_step": plain_ms, "value": n_total / (plain_ms * 1e-3), "unit": UNIT,
                         "calls": 2 * args.pairs,
-                        "note": "one hg_build_into + hg_intersect_into (direct path) per pair, same buffers"},
+                        "note": "one hg_build_into + hg_intersect_into per pair (the planner's path), same buffers"},
         "phases_ms": phase_avg, "clocks": clk, "e2e": e2e, "gpu_launches": launches, "cpu_baseline": None,
     }
     if rank == 0:
@@ -781,14 +883,14 @@ def run_sharded(args, rank, world, local):
 # ---------------------------------------------------------------------------
 # CPU baseline / reference arm
 # ---------------------------------------------------------------------------
-def cpu_run(workload, n_sample, repeats=3):
-    import numpy as np
-
+def cpu_inputs(workload, n_sample):
+    """The workload's inputs on the host (the oracle's generators, the same
+    definitions as the device generators): n keys per set, at most the
+    workload's own n, with the workload's load factor."""
     import oracle
     kb, n_full, bfn, kind, seed_a, seed_q, overlap, with_index = WORKLOADS[workload]
     n = min(n_sample, n_full)
     B = max(1, int(bfn(n_full) * n // n_full))
-    threads = oracle.max_threads()
     if kind == "zipf":
         cdf = oracle.zipf_cdf(1 << 24, 1.1)
         a = oracle.gen_zipf(n, kb, cdf, seed_a)
@@ -796,25 +898,44 @@ def cpu_run(workload, n_sample, repeats=3):
     else:
         a = oracle.gen_uniform(n, kb, seed_a)
         q = oracle.gen_overlap(n, a, overlap, seed_q)
-    cap = n if kind != "zipf" else 0
-    best = None
-    for _ in range(repeats):
-        t0 = time.perf_counter()
-        off, k, i = oracle.build(a, B, with_index, threads=threads)
-        t1 = time.perf_counter()
-        c, _ = oracle.intersect(off, k, i, q, pair_cap=cap, threads=threads)
-        t2 = time.perf_counter()
-        dt = t2 - t0
-        if best is None or dt < best[0]:
-            best = (dt, t1 - t0, t2 - t1, c)
-    return n, B, threads, best
+    return n, B, a, q
 
 
-def cpu_baseline(workload, n_sample):
-    n, B, threads, (dt, tb, ti, c) = cpu_run(workload, n_sample)
+def cpu_step(workload, B, a, q, threads):
+    """One build + intersect on the host: the oracle's multithreaded stable
+    build and probe (pairs emitted, as on the GPU).  Zipf sets are counted
+    through a hash map of A's distinct keys instead of the probe, whose cost
+    is the product of the multiplicities.  Returns (seconds, build s,
+    intersect s, count)."""
+    import oracle
+    kind, with_index = WORKLOADS[workload][3], WORKLOADS[workload][7]
+    t0 = time.perf_counter()
+    off, k, i = oracle.build(a, B, with_index, threads=threads)
+    t1 = time.perf_counter()
+    if kind == "zipf":
+        c = oracle.join_count_hashed(k, q, max_distinct=1 << 24, threads=threads)
+    else:
+        c, _ = oracle.intersect(off, k, i, q, pair_cap=q.size, threads=threads)
+    t2 = time.perf_counter()
+    return t2 - t0, t1 - t0, t2 - t1, c
+
+
+def cpu_note(workload):
+    return ("zipf: build by the oracle's stable counting sort, count through a hash map of A's distinct keys"
+            if WORKLOADS[workload][3] == "zipf" else
+            "the oracle's multithreaded stable build and probe, pairs emitted")
+
+
+def cpu_baseline(workload, n_sample, repeats=2):
+    import oracle
+    threads = oracle.max_threads()
+    n, B, a, q = cpu_inputs(workload, n_sample)
+    best = min((cpu_step(workload, B, a, q, threads) for _ in range(repeats)), key=lambda x: x[0])
+    dt, tb, ti, c = best
     return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n} keys per set into {B} buckets (same generators and load factor), best of 3; "
-                      f"build {tb:.3f} s + intersect {ti:.3f} s"}
+            "sample": f"{n} keys per set into {B} buckets (the same seeded inputs"
+                      f"{'' if n == WORKLOADS[workload][1] else ', a sample with the same load factor'}), "
+                      f"best of {repeats}; build {tb:.3f} s + intersect {ti:.3f} s; {cpu_note(workload)}"}
 
 
 def run_reference_batched(args):
@@ -830,7 +951,7 @@ def run_reference_batched(args):
         q = oracle.gen_overlap(n, a, float(fracs[i]), 200_000 + i)
         inputs.append((a, q, n))
         total += n
-        if total >= args.cpu_sample // 4:
+        if total >= (args.cpu_sample or 1 << 26) // 4:
             break
     times = []
     for k in range(args.warmup + args.steps):
@@ -880,7 +1001,7 @@ def run_reference_serving(args):
         t_sum += time.perf_counter() - t0
         total += size
         k += 1
-        if total >= args.cpu_sample:
+        if total >= (args.cpu_sample or 1 << 26):
             break
     value = total / t_sum
     out = {
@@ -912,11 +1033,11 @@ def run_reference(args, rank, world):
     kb, n, bfn, kind, seed_a, seed_q, overlap, with_index = WORKLOADS[args.workload]
     n = args.n or n
     B = bfn(n)
-    ns = min(args.cpu_sample, n)
-    times = []
     cores = oracle.max_threads()
+    ns, BB, a, q = cpu_inputs(args.workload, cpu_sample_size(args, n))
+    times = []
     for k in range(args.warmup + args.steps):
-        nn, BB, cores, (dt, tb, ti, c) = cpu_run(args.workload, ns, repeats=1)
+        dt, tb, ti, c = cpu_step(args.workload, BB, a, q, cores)
         if k >= args.warmup:
             times.append(dt)
     total = sum(times)
@@ -929,9 +1050,10 @@ def run_reference(args, rank, world):
         "config": {"workload": describe(args.workload, kb, n, B, kind, overlap, with_index), "n": n,
                    "n_buckets": B, "key_bytes": kb, "with_index": with_index},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{ns} keys per set into {max(1, B * ns // n)} buckets per step "
-                                   "(the reference has no CPU build/intersect; this is the oracle's "
-                                   "multithreaded restatement of its algorithm)"},
+                         "sample": f"{ns} keys per set into {BB} buckets per step"
+                                   f"{' (the whole workload)' if ns == n else ' (a sample with the same load factor)'}; "
+                                   f"{cpu_note(args.workload)} (the reference has no CPU build/intersect; this is "
+                                   "the oracle's multithreaded restatement of its algorithm)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -949,8 +1071,10 @@ def main():
     ap.add_argument("--streams", type=int, default=4, help="serving CUDA streams")
     ap.add_argument("--pairs", type=int, default=4096, help="pairs of the batched workload")
     ap.add_argument("--n", type=int, default=0, help="override keys per set (parity/profiling runs)")
-    ap.add_argument("--cpu-sample", type=int, default=1 << 26)
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="keys per set of the CPU arm (0: the workload's own, at most 2^28)")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-ref-gpu", action="store_true", help="do not time the reference's GPU build")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--build-path", choices=["auto", "direct", "partitioned"], default="auto")
     ap.add_argument("--probe-path", choices=["auto", "direct", "partitioned"], default="auto")

@@ -27,6 +27,7 @@ STATUS_NAMES = {
     -7: "HG_ERR_NO_DEVICE",
     -8: "HG_ERR_KEY_WIDTH",
     -9: "HG_ERR_BUCKET_MISMATCH",
+    -10: "HG_ERR_DEVICE_STATE",
 }
 ERR_PAIR_CAPACITY = -4
 ERR_DEVICE_TIMEOUT = -5
@@ -66,6 +67,7 @@ SIGNATURES = {
     "hg_last_error": (ctypes.c_char_p, []),
     "hg_hash": (ctypes.c_uint32, [_u64]),
     "hg_device_error": (_i32, [_p, ctypes.POINTER(_i32)]),
+    "hg_debug_set_wait_limit": (_i32, [ctypes.c_uint32, _p]),
     "hg_build_workspace_size": (_i32, [_u64, _int, _u64, _int, ctypes.POINTER(_sz)]),
     "hg_build_into": (_i32, [_p, _u64, _int, _u64, _p, _p, _p, _p, _sz, _p]),
     "hg_build_workspace_size_path": (_i32, [_u64, _int, _u64, _int, _int, ctypes.POINTER(_sz)]),
@@ -115,6 +117,8 @@ SIGNATURES = {
     "hg_server_build": (_i32, [_p, _u64, _p, _u64, _u64, _int, ctypes.c_double, ctypes.POINTER(_u64)]),
     "hg_server_intersect": (_i32, [_p, _u64, _p, _u64, _p, _u64, ctypes.c_double, ctypes.POINTER(_u64)]),
     "hg_server_poll": (_i32, [_p, _int, ctypes.POINTER(ServerDone), _int, ctypes.POINTER(_int)]),
+    "hg_server_set_batching": (_i32, [_p, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double]),
+    "hg_server_batch_stats": (_i32, [_p, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "hg_server_stats": (_i32, [_p, ctypes.POINTER(_u64), ctypes.POINTER(_sz), ctypes.POINTER(_u64),
                                ctypes.POINTER(_u64)]),
     "hg_server_free": (None, [_p]),

@@ -41,6 +41,7 @@ extern "C" const char* hg_status_str(hg_status s) {
     case HG_ERR_NO_DEVICE: return "no CUDA device";
     case HG_ERR_KEY_WIDTH: return "key width must be 4 or 8 bytes and match between tables";
     case HG_ERR_BUCKET_MISMATCH: return "tables have different bucket counts";
+    case HG_ERR_DEVICE_STATE: return "a kernel found a position outside its output and wrote nothing";
     default: return "unknown status";
   }
 }
@@ -56,14 +57,24 @@ extern "C" hg_status hg_device_error(hg_stream_t stream, hg_status* code) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   hg_status st = cuda_status(cudaStreamSynchronize(s));
   if (st != HG_OK) return st;
-  int32_t v = 0;
+  int32_t v = 0, fault = 0;
   st = cuda_status(cudaMemcpyFromSymbol(&v, g_device_error, sizeof(v)));
+  if (st == HG_OK) st = cuda_status(cudaMemcpyFromSymbol(&fault, g_device_fault, sizeof(fault)));
   if (st != HG_OK) return st;
   const int32_t zero = 0;
   st = cuda_status(cudaMemcpyToSymbol(g_device_error, &zero, sizeof(zero)));
+  if (st == HG_OK) st = cuda_status(cudaMemcpyToSymbol(g_device_fault, &zero, sizeof(zero)));
   if (st != HG_OK) return st;
-  *code = v;
+  *code = fault ? fault : v;
   return HG_OK;
+}
+
+extern "C" hg_status hg_debug_set_wait_limit(uint32_t polls, hg_stream_t stream) {
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  hg_status st = cuda_status(cudaStreamSynchronize(s));
+  if (st != HG_OK) return st;
+  const uint32_t v = polls ? polls : LOOKBACK_SPIN_LIMIT;
+  return cuda_status(cudaMemcpyToSymbol(g_lookback_limit, &v, sizeof(v)));
 }
 
 // ---------------------------------------------------------------------------

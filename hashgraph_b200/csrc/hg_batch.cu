@@ -32,6 +32,8 @@
 // batched form; per pair it replaces build + intersect of
 // src/MultiHashGraph.cu:408-740.
 #include <algorithm>
+#include <cstring>
+#include <new>
 #include <vector>
 
 #include "hg_device.cuh"
@@ -71,6 +73,7 @@ struct BatchPairDev {
   uint32_t a_bulk;                  // the table's arrays are 16-byte aligned
   uint32_t pl;                      // L2 form of the probe: chunks [ltile0, ltile0 + ltiles)
   uint64_t ltile0, ltiles;
+  uint32_t prebuilt;                // the table is already built: the pair is only probed
 };
 
 // Flags of a batch run: [0] a table's partitioned build overflowed, [1] a
@@ -88,11 +91,11 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_clear(const BatchPairDev*
                                                             const uint32_t* __restrict__ stile_pair, uint64_t s_begin,
                                                             uint64_t s_end, const uint32_t* flags,
                                                             const uint32_t* gate) {
-  if (gated_off(gate)) return;
+  if (entry_skip(gate)) return;
   if (!gate)  // the ungated launch zeroes every pair's count
     for (uint64_t i = uint64_t(blockIdx.x) * BATCH_BLOCK + threadIdx.x; i < uint64_t(n_pairs);
          i += uint64_t(gridDim.x) * BATCH_BLOCK)
-      *pairs[i].count = 0ull;
+      if (pairs[i].count) *pairs[i].count = 0ull;
   for (uint64_t t = s_begin + blockIdx.x; t < s_end; t += gridDim.x) {
     const BatchPairDev& P = pairs[stile_pair[t]];
     if (batch_skip_build(P, flags)) continue;
@@ -109,7 +112,7 @@ template <typename KeyT>
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_count(const BatchPairDev* __restrict__ pairs,
                                                             const uint32_t* __restrict__ ktile_pair, uint64_t k_begin,
                                                             uint64_t k_end, const uint32_t* flags, const uint32_t* gate) {
-  if (gated_off(gate)) return;
+  if (entry_skip(gate)) return;
   for (uint64_t t = k_begin + blockIdx.x; t < k_end; t += gridDim.x) {
     const BatchPairDev& P = pairs[ktile_pair[t]];
     if (batch_skip_build(P, flags)) continue;
@@ -136,7 +139,7 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scan(const BatchPairDev* 
                                                            const uint32_t* __restrict__ stile_pair, uint64_t s_begin,
                                                            uint64_t s_end, uint64_t* __restrict__ status, unsigned* ticket,
                                                            const uint32_t* flags, const uint32_t* gate) {
-  if (gated_off(gate)) return;
+  if (entry_skip(gate)) return;
   constexpr int TILE = BATCH_BLOCK * ITEMS;
   static_assert(TILE == BATCH_STILE, "scan tile");
   __shared__ uint32_t s[TILE + TILE / 32];
@@ -201,7 +204,7 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scatter(const BatchPairDe
                                                               const uint32_t* __restrict__ ktile_pair,
                                                               uint64_t k_begin, uint64_t k_end, const uint32_t* flags,
                                                               const uint32_t* gate) {
-  if (gated_off(gate)) return;
+  if (entry_skip(gate)) return;
   for (uint64_t t = k_begin + blockIdx.x; t < k_end; t += gridDim.x) {
     const BatchPairDev& P = pairs[ktile_pair[t]];
     if (batch_skip_build(P, flags)) continue;
@@ -230,7 +233,8 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_scatter(const BatchPairDe
     for (uint32_t u = 0; u < BATCH_KPT; u++) {
       const uint64_t i = base + u * BATCH_BLOCK + threadIdx.x;
       const uint32_t pos = __shfl_sync(FULL_MASK, got[u], leader[u]) + rank[u];
-      if (i < P.n) {
+      if (i < P.n && pos >= P.n) record_fault(HG_ERR_DEVICE_STATE);  // offsets past n: write nothing
+      else if (i < P.n) {
         out[pos] = k[u];
         if (idx) idx[pos] = static_cast<uint32_t>(i);
       }
@@ -247,7 +251,7 @@ __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_probe(const BatchPairDev*
                                                             uint64_t q_end, uint64_t* __restrict__ status,
                                                             unsigned* ticket, const uint32_t* flags,
                                                             const uint32_t* gate) {
-  if (gated_off(gate)) return;
+  if (entry_skip(gate)) return;
   __shared__ uint64_t red[BATCH_BLOCK / 32 + 1];
   __shared__ uint64_t s_tile, s_prefix;
   while (true) {
@@ -340,6 +344,7 @@ template <typename KeyT>
 __global__ void __launch_bounds__(BATCH_BLOCK) k_batch_l2probe(const BatchPairDev* __restrict__ pairs,
                                                               const uint32_t* __restrict__ lchunk_pair,
                                                               uint64_t n_lchunks, unsigned* ticket) {
+  if (entry_skip(nullptr)) return;
   constexpr int NW = BATCH_BLOCK / 32;
   __shared__ uint64_t red[NW + 1];
   __shared__ unsigned s_t[2];
@@ -577,8 +582,11 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
   dev->resize(n_pairs);
   for (int i = 0; i < n_pairs; i++) {
     const hg_batch_pair& a = pairs[i];
-    if (a.n_buckets == 0 || !a.d_offsets || !a.d_count) return lib_fail(HG_ERR_INVALID_ARGUMENT, "hg_batch_create: pair without buckets, offsets or count");
-    if ((a.n > 0 && (!a.d_keys || !a.d_keys_out)) || (a.nq > 0 && !a.d_query))
+    if (a.n_buckets == 0 || !a.d_offsets || (a.nq > 0 && !a.d_count))
+      return lib_fail(HG_ERR_INVALID_ARGUMENT, "hg_batch_create: pair without buckets, offsets or count");
+    // d_keys NULL with n > 0: the table is already built in d_offsets /
+    // d_keys_out / d_idx_out and is only probed
+    if ((a.n > 0 && !a.d_keys_out) || (a.nq > 0 && !a.d_query))
       return lib_fail(HG_ERR_INVALID_ARGUMENT, "hg_batch_create: pair with keys or queries but no buffer");
     if (a.n >= (1ull << 32) || a.nq >= (1ull << 32) || a.n_buckets > (1ull << 32))
       return lib_fail(HG_ERR_TOO_LARGE, "hg_batch_create: a pair exceeds 2^32 keys, queries or buckets");
@@ -595,6 +603,7 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
     d.n_buckets = a.n_buckets;
     d.pair_cap = a.d_pairs ? a.pair_cap : 0;
     d.bm = BucketMap::make(a.n_buckets);
+    d.prebuilt = (a.n > 0 && !a.d_keys) ? 1u : 0u;
   }
   // Partitioned form: large pairs whose buckets make at most PASS1_GOOD_PARTS
   // fine partitions and whose partitions fit a CTA's shared memory.
@@ -603,7 +612,8 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
   for (int i = 0; i < n_pairs; i++) {
     BatchPairDev& d = (*dev)[i];
     const double per_b = double(d.n) * double(wb) / double(d.n_buckets);
-    d.pb = (d.n >= prm.part_min && (d.n_buckets + wb - 1) / wb <= PASS1_GOOD_PARTS && per_b <= 4096.0) ? 1u : 0u;
+    d.pb = (!d.prebuilt && d.n >= prm.part_min && (d.n_buckets + wb - 1) / wb <= PASS1_GOOD_PARTS && per_b <= 4096.0)
+               ? 1u : 0u;
     if (d.pb) {
       p.capf = std::max(p.capf, slack_capacity(per_b, 64));
       p.wi_b = p.wi_b || d.idx_out != nullptr;
@@ -660,7 +670,7 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
   auto assign = [&](bool partitioned_build, bool partitioned_probe) {
     for (int i = 0; i < n_pairs; i++) {
       BatchPairDev& d = (*dev)[i];
-      if ((d.pb != 0) == partitioned_build) {
+      if (!d.prebuilt && (d.pb != 0) == partitioned_build) {
         d.ktile0 = p.n_ktiles;
         d.stile0 = p.n_stiles;
         p.n_ktiles += (d.n + BATCH_KTILE - 1) / BATCH_KTILE;
@@ -689,8 +699,8 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
   qmap->resize(p.n_qtiles);
   for (int i = 0; i < n_pairs; i++) {
     const BatchPairDev& d = (*dev)[i];
-    const uint64_t kt = (d.n + BATCH_KTILE - 1) / BATCH_KTILE;
-    const uint64_t st = (d.n_buckets + BATCH_STILE - 1) / BATCH_STILE;
+    const uint64_t kt = d.prebuilt ? 0 : (d.n + BATCH_KTILE - 1) / BATCH_KTILE;
+    const uint64_t st = d.prebuilt ? 0 : (d.n_buckets + BATCH_STILE - 1) / BATCH_STILE;
     std::fill(kmap->begin() + d.ktile0, kmap->begin() + d.ktile0 + kt, uint32_t(i));
     std::fill(smap->begin() + d.stile0, smap->begin() + d.stile0 + st, uint32_t(i));
     std::fill(qmap->begin() + d.qtile0, qmap->begin() + d.qtile0 + d.qtiles, uint32_t(i));
@@ -983,6 +993,62 @@ extern "C" hg_status hg_batch_create_params(const hg_batch_pair* pairs, int n_pa
   *out = b;
   return HG_OK;
 }
+
+namespace hg {
+
+// Staged creation, for the serving engine: the descriptors and tile maps are
+// packed into the caller's pinned buffer at their device offsets and
+// uploaded with ONE asynchronous copy, and the workspace comes from `pool`
+// (stream-ordered).  Nothing synchronises: the caller keeps `pinned`
+// untouched until the copy has completed (an event recorded after the
+// batch's run covers it).  HG_ERR_TOO_LARGE when the descriptors do not fit
+// `pinned_cap` bytes.
+hg_status batch_create_staged(const hg_batch_pair* pairs, int n_pairs, int key_bytes, const hg_batch_params* params,
+                              cudaStream_t s, cudaMemPool_t pool, void* pinned, size_t pinned_cap, hg_batch** out) {
+  *out = nullptr;
+  hg_batch_params prm;
+  hg_batch_params_default(&prm);
+  if (params) prm = *params;
+  BatchPlan plan;
+  std::vector<BatchPairDev> dev;
+  std::vector<uint32_t> kmap, smap, qmap, mtmap, mqmap, fbmap, fqmap, lmap;
+  hg_status st = batch_plan(pairs, n_pairs, key_bytes, prm, &plan, &dev, &kmap, &smap, &qmap, &mtmap, &mqmap, &fbmap,
+                            &fqmap, &lmap);
+  if (st != HG_OK) return st;
+  const size_t desc_bytes = plan.off_fbkeys;  // the descriptor regions lead the workspace
+  if (desc_bytes > pinned_cap) return HG_ERR_TOO_LARGE;
+  char* h = static_cast<char*>(pinned);
+  auto pack = [&](size_t off, const void* src, size_t bytes) {
+    if (bytes) std::memcpy(h + off, src, bytes);
+  };
+  pack(plan.off_pairs, dev.data(), dev.size() * sizeof(BatchPairDev));
+  pack(plan.off_kmap, kmap.data(), kmap.size() * 4);
+  pack(plan.off_smap, smap.data(), smap.size() * 4);
+  pack(plan.off_qmap, qmap.data(), qmap.size() * 4);
+  pack(plan.off_mtmap, mtmap.data(), mtmap.size() * 4);
+  pack(plan.off_mqmap, mqmap.data(), mqmap.size() * 4);
+  pack(plan.off_fbmap, fbmap.data(), fbmap.size() * 4);
+  pack(plan.off_fqmap, fqmap.data(), fqmap.size() * 4);
+  pack(plan.off_lmap, lmap.data(), lmap.size() * 4);
+  hg_batch* b = new (std::nothrow) hg_batch();
+  if (!b) return HG_ERR_OUT_OF_MEMORY;
+  b->plan = plan;
+  cudaGetDevice(&b->device);
+  void* mem = nullptr;
+  cudaError_t e = pool ? cudaMallocFromPoolAsync(&mem, plan.total, pool, s) : cudaMallocAsync(&mem, plan.total, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(mem, h, desc_bytes, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) {
+    if (mem) cudaFreeAsync(mem, s);
+    delete b;
+    cudaGetLastError();
+    return cuda_fail(e, "batch: staged creation");
+  }
+  b->d_mem = static_cast<char*>(mem);
+  *out = b;
+  return HG_OK;
+}
+
+}  // namespace hg
 
 extern "C" hg_status hg_batch_create(const hg_batch_pair* pairs, int n_pairs, int key_bytes, hg_stream_t stream,
                                      hg_batch** out) {

@@ -53,6 +53,29 @@ __device__ __forceinline__ bool gated_off(const uint32_t* gate) {
   return gate != nullptr && (*reinterpret_cast<const volatile uint32_t*>(gate) & FLAG_OVERFLOW) == 0;
 }
 
+// Entry test of every kernel that reads other kernels' results or writes at
+// computed positions: true when a device fault is pending or the gate is
+// closed.  One thread decides and the CTA follows, so every thread of the CTA
+// returns together (the fault word may be set by another stream's kernel at
+// any moment, and a CTA split between returning and running would leave its
+// barriers and warp collectives short).  Contains __syncthreads().
+__device__ __forceinline__ bool entry_skip(const uint32_t* gate) {
+  __shared__ int s_skip;
+  if (threadIdx.x == 0) s_skip = (device_faulted() || gated_off(gate)) ? 1 : 0;
+  __syncthreads();
+  return s_skip != 0;
+}
+
+// The same for the partitioned paths' kernels, which run only while the
+// overflow flag is clear (the gated direct kernels take over once it is set).
+__device__ __forceinline__ bool entry_skip_on_overflow(const uint32_t* flags) {
+  __shared__ int s_skip;
+  if (threadIdx.x == 0)
+    s_skip = (device_faulted() || (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW)) ? 1 : 0;
+  __syncthreads();
+  return s_skip != 0;
+}
+
 // Loads the V keys lane `lane` owns in chunk [base, base + 32V); marks which
 // exist.  Full chunks use one or two 16-byte vector loads per lane.
 template <typename KeyT, int V>
@@ -84,7 +107,7 @@ __device__ __forceinline__ void load_chunk(const KeyT* __restrict__ keys, uint64
 template <typename KeyT, int V>
 __global__ void __launch_bounds__(256) k_count(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
                                                uint32_t* __restrict__ cnt, const uint32_t* gate) {
-  if (gated_off(gate)) return;
+  if (entry_skip(gate)) return;
   const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
   const uint64_t nchunks = (n + 32ull * V - 1) / (32ull * V);
   for (uint64_t c = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; c < nchunks;
@@ -102,7 +125,7 @@ __global__ void __launch_bounds__(256) k_scatter(const KeyT* __restrict__ keys, 
                                                  uint32_t* __restrict__ cursor, KeyT* __restrict__ keys_out,
                                                  uint32_t* __restrict__ idx_out, const uint32_t* __restrict__ key_idx,
                                                  const uint32_t* gate) {
-  if (gated_off(gate)) return;
+  if (entry_skip(gate)) return;
   const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
   const uint64_t nchunks = (n + 32ull * V - 1) / (32ull * V);
   for (uint64_t c = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; c < nchunks;
@@ -114,7 +137,8 @@ __global__ void __launch_bounds__(256) k_scatter(const KeyT* __restrict__ keys, 
 #pragma unroll
     for (int j = 0; j < V; j++) {
       const uint32_t pos = warp_aggregated_inc(cursor, bm.of_key(k[j]), ok[j]);
-      if (ok[j]) {
+      if (ok[j] && pos >= n) record_fault(HG_ERR_DEVICE_STATE);  // offsets past n: write nothing
+      else if (ok[j]) {
         keys_out[pos] = k[j];
         if constexpr (WITH_IDX) {
           const uint64_t i = base + lane_id() * V + j;
@@ -122,6 +146,138 @@ __global__ void __launch_bounds__(256) k_scatter(const KeyT* __restrict__ keys, 
         }
       }
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Direct path under skew.  The gated direct kernels run when the partitioned
+// path overflowed, that is when some buckets are far above their expected
+// size (heavy duplicates, Zipf keys).  Then a few buckets take most of the
+// keys, and even warp-aggregated global atomics serialise on them: at 2^28
+// Zipf(1.1) keys the hottest counter gets one atomic from nearly every warp.
+// These forms aggregate per CTA first, in a shared-memory table of the
+// chunk's buckets (open addressing, bucket id -> count): each chunk of
+// SKEW_CHUNK keys costs one global atomic per distinct bucket in it, so a hot
+// bucket gets one per chunk.  A key whose bucket finds no slot within
+// SKEW_PROBES steps takes a global atomic of its own.
+// ---------------------------------------------------------------------------
+constexpr int SKEW_BLOCK = 256;
+constexpr int SKEW_KPT = 8;
+constexpr uint32_t SKEW_CHUNK = uint32_t(SKEW_BLOCK) * SKEW_KPT;
+constexpr uint32_t SKEW_SLOTS = 4096;
+constexpr uint32_t SKEW_PROBES = 8;
+constexpr uint32_t SKEW_EMPTY = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint32_t skew_slot(uint32_t b) { return (b * 0x9E3779B1u) >> 20; }
+
+// Slot of bucket b in the chunk's table (claimed if new), or SKEW_SLOTS.
+__device__ __forceinline__ uint32_t skew_place(uint32_t* s_b, uint32_t b) {
+  if (b == SKEW_EMPTY) return SKEW_SLOTS;
+  uint32_t h = skew_slot(b);
+  for (uint32_t p = 0; p < SKEW_PROBES; p++) {
+    const uint32_t prev = atomicCAS(s_b + h, SKEW_EMPTY, b);
+    if (prev == SKEW_EMPTY || prev == b) return h;
+    h = (h + 1) & (SKEW_SLOTS - 1);
+  }
+  return SKEW_SLOTS;
+}
+
+template <typename KeyT>
+__global__ void __launch_bounds__(SKEW_BLOCK) k_count_skew(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
+                                                           uint32_t* __restrict__ cnt, const uint32_t* gate) {
+  if (entry_skip(gate)) return;
+  __shared__ uint32_t s_b[SKEW_SLOTS], s_c[SKEW_SLOTS];
+  for (uint32_t i = threadIdx.x; i < SKEW_SLOTS; i += SKEW_BLOCK) {
+    s_b[i] = SKEW_EMPTY;
+    s_c[i] = 0;
+  }
+  __syncthreads();
+  for (uint64_t base = uint64_t(blockIdx.x) * SKEW_CHUNK; base < n; base += uint64_t(gridDim.x) * SKEW_CHUNK) {
+#pragma unroll
+    for (int u = 0; u < SKEW_KPT; u++) {
+      const uint64_t i = base + uint64_t(u) * SKEW_BLOCK + threadIdx.x;
+      if (i < n) {
+        const uint32_t b = bm.of_key(__ldcs(keys + i));
+        const uint32_t h = skew_place(s_b, b);
+        if (h < SKEW_SLOTS) atomicAdd(s_c + h, 1u);
+        else atomicAdd(cnt + b, 1u);
+      }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < SKEW_SLOTS; i += SKEW_BLOCK) {
+      const uint32_t c = s_c[i];
+      if (c) {
+        atomicAdd(cnt + s_b[i], c);
+        s_c[i] = 0;
+      }
+      s_b[i] = SKEW_EMPTY;
+    }
+    __syncthreads();
+  }
+}
+
+// Scatter: a chunk's keys take a rank in their bucket's slot, one global
+// atomic per slot reserves the bucket's run for the chunk, then every key is
+// written at run start + rank.
+template <typename KeyT, bool WITH_IDX>
+__global__ void __launch_bounds__(SKEW_BLOCK) k_scatter_skew(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
+                                                             uint32_t* __restrict__ cursor, KeyT* __restrict__ keys_out,
+                                                             uint32_t* __restrict__ idx_out,
+                                                             const uint32_t* __restrict__ key_idx,
+                                                             const uint32_t* gate) {
+  if (entry_skip(gate)) return;
+  __shared__ uint32_t s_b[SKEW_SLOTS], s_c[SKEW_SLOTS];  // s_c: the chunk's count, then its run start
+  for (uint32_t i = threadIdx.x; i < SKEW_SLOTS; i += SKEW_BLOCK) {
+    s_b[i] = SKEW_EMPTY;
+    s_c[i] = 0;
+  }
+  __syncthreads();
+  for (uint64_t base = uint64_t(blockIdx.x) * SKEW_CHUNK; base < n; base += uint64_t(gridDim.x) * SKEW_CHUNK) {
+    KeyT k[SKEW_KPT];
+    uint32_t where[SKEW_KPT];  // slot << 16 | rank, or the position taken by a global atomic
+    uint32_t direct = 0;       // bit u: where[u] is a position
+#pragma unroll
+    for (int u = 0; u < SKEW_KPT; u++) {
+      const uint64_t i = base + uint64_t(u) * SKEW_BLOCK + threadIdx.x;
+      k[u] = KeyT(0);
+      where[u] = 0;
+      if (i < n) {
+        k[u] = __ldcs(keys + i);
+        const uint32_t b = bm.of_key(k[u]);
+        const uint32_t h = skew_place(s_b, b);
+        if (h < SKEW_SLOTS) {
+          where[u] = (h << 16) | atomicAdd(s_c + h, 1u);
+        } else {
+          where[u] = atomicAdd(cursor + b, 1u);
+          direct |= 1u << u;
+        }
+      }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < SKEW_SLOTS; i += SKEW_BLOCK) {
+      const uint32_t c = s_c[i];
+      if (c) s_c[i] = atomicAdd(cursor + s_b[i], c);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < SKEW_KPT; u++) {
+      const uint64_t i = base + uint64_t(u) * SKEW_BLOCK + threadIdx.x;
+      if (i < n) {
+        const uint32_t pos = (direct >> u) & 1u ? where[u] : s_c[where[u] >> 16] + (where[u] & 0xffffu);
+        if (pos < n) {
+          keys_out[pos] = k[u];
+          if constexpr (WITH_IDX) idx_out[pos] = key_idx ? key_idx[i] : static_cast<uint32_t>(i);
+        } else {
+          record_fault(HG_ERR_DEVICE_STATE);  // offsets past n: write nothing
+        }
+      }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < SKEW_SLOTS; i += SKEW_BLOCK) {
+      s_c[i] = 0;
+      s_b[i] = SKEW_EMPTY;
+    }
+    __syncthreads();
   }
 }
 
@@ -133,7 +289,7 @@ __global__ void __launch_bounds__(BLOCK) k_scan_u32(uint32_t* __restrict__ data,
                                                     uint64_t* __restrict__ status, unsigned* ticket,
                                                     uint32_t* first_slot, uint32_t* total_out,
                                                     const uint32_t* gate) {
-  if (gated_off(gate)) return;
+  if (entry_skip(gate)) return;
   constexpr int TILE = BLOCK * ITEMS;
   __shared__ uint32_t s[TILE + TILE / 32];
   __shared__ uint32_t red[BLOCK / 32 + 1];
@@ -190,7 +346,7 @@ __global__ void __launch_bounds__(BLOCK) k_scan_u32(uint32_t* __restrict__ data,
 }
 
 __global__ void k_fill_u32(uint32_t* p, uint64_t count, uint32_t value, const uint32_t* gate) {
-  if (gated_off(gate)) return;
+  if (entry_skip(gate)) return;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
        i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
     p[i] = value;
@@ -251,6 +407,7 @@ struct TableTiles {
 
 template <typename KeyT, bool WITH_IDX, int BLOCK, int KPT, bool BULK, typename Src>
 __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(Src src, uint32_t max_parts, uint32_t* flags) {
+  if (entry_skip(nullptr)) return;
   constexpr uint32_t TILE = BLOCK * KPT;
   constexpr uint32_t APT = PASS1_APT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -413,7 +570,7 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
                                                  uint32_t* flags) {
   constexpr uint32_t KPT = 8;
   constexpr uint32_t TILE = BLOCK * KPT;
-  if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
+  if (entry_skip_on_overflow(flags)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t S = 1u << split_log2;
   int64_t* eoff = reinterpret_cast<int64_t*>(smem_raw);  // element offset of sorted position 0, per fine partition
@@ -627,7 +784,7 @@ struct TableFine {
 template <typename KeyT, bool WITH_IDX, int BLOCK, typename Src>
 __global__ void __launch_bounds__(BLOCK) k_fine_build(Src src, uint64_t capf, uint32_t fine_log2,
                                                       const uint32_t* flags) {
-  if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
+  if (entry_skip_on_overflow(flags)) return;
   constexpr int NW = BLOCK / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t W = 1u << fine_log2;
@@ -644,7 +801,11 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(Src src, uint64_t capf, ui
   // thread 0 loads a partition's start and size one iteration before it issues its copy
   auto load_meta = [&](uint64_t f) -> uint2 { return f < n_live ? src.meta(f) : make_uint2(0u, 0u); };
   auto issue = [&](uint64_t f, uint32_t buf, uint2 mt) {
-    const uint32_t m = mt.y - mt.x;
+    uint32_t m = mt.y - mt.x;
+    if (mt.y < mt.x || m > capf) {  // a partition larger than its slots: bad device state
+      record_fault(HG_ERR_DEVICE_STATE);
+      m = 0;
+    }
     s_base[buf] = mt.x;
     s_m[buf] = m;
     const FinePart<KeyT> fp = src.at(f);
@@ -772,6 +933,12 @@ static void launch_direct_count(const KeyT* keys, uint64_t n, BucketMap bm, uint
   const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(want, uint64_t(device_sm_count()) * 8)));
   Phase ph(s, gate ? "fallback_count" : "count");
   count_launch();
+  if (gate) {  // the fallback runs under skew: CTA-aggregated counting
+    const uint64_t cchunks = (n + SKEW_CHUNK - 1) / SKEW_CHUNK;
+    const unsigned sgrid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(cchunks, uint64_t(device_sm_count()) * 4)));
+    k_count_skew<KeyT><<<sgrid, SKEW_BLOCK, 0, s>>>(keys, n, bm, cnt, gate);
+    return;
+  }
   k_count<KeyT, V><<<grid, 256, 0, s>>>(keys, n, bm, cnt, gate);
 }
 
@@ -783,6 +950,12 @@ static void launch_direct_scatter(const KeyT* keys, uint64_t n, BucketMap bm, ui
   const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(want, uint64_t(device_sm_count()) * 8)));
   Phase ph(s, gate ? "fallback_scatter" : "scatter");
   count_launch();
+  if (gate) {  // the fallback runs under skew: CTA-aggregated cursor bumps
+    const uint64_t cchunks = (n + SKEW_CHUNK - 1) / SKEW_CHUNK;
+    const unsigned sgrid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(cchunks, uint64_t(device_sm_count()) * 4)));
+    k_scatter_skew<KeyT, WI><<<sgrid, SKEW_BLOCK, 0, s>>>(keys, n, bm, cursor, out, idx, key_idx, gate);
+    return;
+  }
   k_scatter<KeyT, V, WI><<<grid, 256, 0, s>>>(keys, n, bm, cursor, out, idx, key_idx, gate);
 }
 

@@ -59,13 +59,32 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`.  Returns false (and records
-// HG_ERR_DEVICE_TIMEOUT) if it did not complete within MBAR_SPIN_LIMIT polls.
+// Bounded wait for phase `parity` of `bar`.  Returns false (and records the
+// fault HG_ERR_DEVICE_TIMEOUT) if it did not complete within MBAR_SPIN_LIMIT
+// polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   for (uint32_t i = 0; i < MBAR_SPIN_LIMIT; i++)
     if (mbar_try_wait(bar, parity)) return true;
-  record_error(HG_ERR_DEVICE_TIMEOUT);
+  record_fault(HG_ERR_DEVICE_TIMEOUT);
   return false;
+}
+
+// Per-thread asynchronous copy of BYTES (4, 8 or 16; both addresses aligned to
+// BYTES) from global to shared memory (cp.async: no register holds the data
+// while it is in flight).  Only src_bytes are read, the rest of the BYTES is
+// zero-filled (src_bytes = 0: nothing is read).  The issuing thread completes
+// its groups with cp_async_wait<N>(), after which it may read what it copied.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Waits until at most N of this thread's committed groups are still in flight.
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // Issues a bulk copy of `bytes` (multiple of 16, both ends 16-byte aligned)

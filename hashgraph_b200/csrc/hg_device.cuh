@@ -125,6 +125,23 @@ __device__ __forceinline__ void record_error(int32_t code) {
   atomicCAS(reinterpret_cast<int*>(&g_device_error), 0, code);
 }
 
+// Device-side fault word: the first fault (a bounded wait that gave up, or a
+// position found outside its output).  The device state that produced it is
+// not trusted, so while it is set every kernel of the library returns at
+// entry, writing nothing, until the host reads and clears it with
+// hg_device_error() -- a fault ends in a clean error status, never in a write
+// through bad offsets.
+__device__ int32_t g_device_fault = 0;
+
+__device__ __forceinline__ void record_fault(int32_t code) {
+  atomicCAS(reinterpret_cast<int*>(&g_device_fault), 0, code);
+  record_error(code);
+}
+
+__device__ __forceinline__ bool device_faulted() {
+  return *reinterpret_cast<const volatile int32_t*>(&g_device_fault) != 0;
+}
+
 __host__ __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 __host__ __device__ constexpr size_t align_up_dev(size_t x, size_t a) { return (x + a - 1) / a * a; }
 

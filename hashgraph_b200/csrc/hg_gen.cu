@@ -16,6 +16,7 @@
 namespace hg {
 
 constexpr uint64_t GOLDEN = 0x9E3779B97F4A7C15ull;
+constexpr uint64_t ZIPF_UNIVERSE_SEED = 0x21BF;  // keys of a Zipf universe: mix64(rank ^ salt)
 
 __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -76,6 +77,7 @@ __global__ void k_gen_bounded(KeyT* out, uint64_t n, uint64_t seed, uint64_t bou
 template <typename KeyT>
 __global__ void k_gather_pair_keys(const KeyT* keys, const uint32_t* pairs, uint64_t count, int which,
                                    int64_t* out) {
+  if (entry_skip(nullptr)) return;
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += uint64_t(gridDim.x) * blockDim.x)
     out[i] = static_cast<int64_t>(keys[pairs[2 * i + which]]);
 }
@@ -162,6 +164,7 @@ extern "C" hg_status hg_gather_pair_keys(const void* d_keys, int key_bytes, cons
 template <typename KeyT>
 __global__ void k_export_reference(const KeyT* keys, const uint32_t* idx, uint64_t n, const uint32_t* off,
                                    uint64_t n_buckets, unsigned char* kv16, int64_t* off64) {
+  if (entry_skip(nullptr)) return;
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
   for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += stride) {
     unsigned char* rec = kv16 + 16 * j;
@@ -218,7 +221,9 @@ extern "C" hg_status hg_gen_zipf(void* d_out, uint64_t n, int key_bytes, const u
   if (n == 0) return HG_OK;
   if (!d_out || !d_cdf || universe == 0) return HG_ERR_INVALID_ARGUMENT;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const uint64_t salt = rand64(seed, 4, 0);
+  // The rank -> key map depends on the universe only, so sets drawn with
+  // different seeds from one universe share their keys (a join has matches).
+  const uint64_t salt = rand64(ZIPF_UNIVERSE_SEED, 4, universe);
   if (key_bytes == 8)
     k_gen_zipf<uint64_t><<<gen_grid(n), 256, 0, s>>>(static_cast<uint64_t*>(d_out), n, d_cdf, universe, seed, salt);
   else

@@ -174,18 +174,32 @@ extern "C" hg_status hg_table_load_arrays(const char* path, uint32_t* d_offsets,
     return lib_fail(HG_ERR_INVALID_ARGUMENT, "hg_table_load_arrays: sizes differ from the file's");
   if ((h.n > 0 && !d_keys) || (h.with_index && h.n > 0 && !d_idx))
     return lib_fail(HG_ERR_INVALID_ARGUMENT, "hg_table_load_arrays: missing destination array");
+  if (!h.with_index && d_idx)
+    return lib_fail(HG_ERR_INVALID_ARGUMENT,
+                    "hg_table_load_arrays: the file holds no input positions, but d_idx was given");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   Pinned stage;
   HG_CUDA(cudaMallocHost(&stage.p, IO_CHUNK), "hg_table_load: staging buffer");
   uint64_t sum = FNV_BASIS;
   const uint64_t off_bytes = 4 * (n_buckets + 1);
-  // offsets[0] must be 0 and offsets[n_buckets] must be n
+  // offsets[0] must be 0, offsets[n_buckets] must be n, and the offsets must
+  // not decrease (checked chunk by chunk on the host, before each chunk is
+  // copied, carrying the last value across chunks): the probes read
+  // keys[offsets[b] .. offsets[b+1]) without further checks.
+  uint32_t prev = 0;
   st = load_array(hf.f, d_offsets, off_bytes, stage.p, s, &sum,
                   [&](uint64_t off, const unsigned char* p, size_t len) -> hg_status {
                     uint32_t v;
                     if (off == 0) {
                       std::memcpy(&v, p, 4);
                       if (v != 0) return lib_fail(HG_ERR_INVALID_ARGUMENT, "table file: offsets[0] is not 0");
+                    }
+                    for (size_t x = 0; x + 4 <= len; x += 4) {
+                      std::memcpy(&v, p + x, 4);
+                      if (v < prev || v > h.n)
+                        return lib_fail(HG_ERR_INVALID_ARGUMENT,
+                                        "table file: offsets decrease or exceed n");
+                      prev = v;
                     }
                     if (off + len == off_bytes) {
                       std::memcpy(&v, p + len - 4, 4);

@@ -24,7 +24,10 @@
 // Host code sees only a host-side stand-in for g_noalloc_scratch; its device
 // address comes from cudaGetSymbolAddress, taken once per device on the
 // first call with that device current (so the first call on each device
-// should happen before any stream capture).
+// should happen before any stream capture).  The address is kept together
+// with the id of the CUDA context it was taken in; after a device reset
+// (a new primary context, the module loaded again) the next call takes it
+// again.
 #include <mutex>
 
 #include "hg_device.cuh"
@@ -38,18 +41,48 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = NOALLOC_MAX_TILES * 8 + 2 * WS_ALIGN;  
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-// Device address of g_noalloc_scratch on the current device (looked up once).
+// Id of the current CUDA context (cuCtxGetCurrent + cuCtxGetId, reached
+// through the runtime's driver entry points so the library needs no link to
+// the driver library), or 0 when it cannot be read.
+static unsigned long long current_context_id() {
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
+// Device address of g_noalloc_scratch on the current device: looked up once
+// per device and context (every call when the context id cannot be read).
 static hg_status noalloc_scratch(void** out) {
   static std::mutex mu;
   static void* addr[64] = {nullptr};
+  static unsigned long long ctx_of[64] = {0};
   int dev = 0;
   HG_CUDA(cudaGetDevice(&dev), "hg_build_into_noalloc: cudaGetDevice");
   if (dev < 0 || dev >= 64) return lib_fail(HG_ERR_INVALID_ARGUMENT, "hg_build_into_noalloc: device index >= 64");
+  const unsigned long long ctx = current_context_id();
   std::lock_guard<std::mutex> g(mu);
-  if (!addr[dev]) {
+  if (!addr[dev] || ctx == 0 || ctx != ctx_of[dev]) {
     void* p = nullptr;
     HG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch), "hg_build_into_noalloc: cudaGetSymbolAddress");
     addr[dev] = p;
+    ctx_of[dev] = current_context_id();  // the lookup makes the device's context current
   }
   *out = addr[dev];
   return HG_OK;

@@ -96,6 +96,7 @@ struct ProbePlan {
   uint64_t tiles = 0;  // direct path: tiles of queries
   PartGeometry g;      // partitioned path (pass 3 stages A's slice)
   size_t off_status = 0, off_ticket = 0, off_flags = 0;
+  size_t off_heavy = 0;  // count only: heavy-key set of the direct probe
   size_t off_pcount = 0, off_pstatus = 0, off_fcount = 0, off_fstatus = 0;
   size_t off_pkeys = 0, off_pidx = 0, off_fkeys = 0, off_fidx = 0;
   size_t total = 0;

@@ -28,6 +28,170 @@ constexpr int PROBE_BLOCK = 256;
 constexpr int PROBE_QPT = 4;
 constexpr uint64_t PROBE_TILE = uint64_t(PROBE_BLOCK) * PROBE_QPT;
 
+// ---------------------------------------------------------------------------
+// Skew in count-only probes.  A query costs the length of its bucket in A.
+// Under heavy duplication (Zipf keys) a few buckets hold tens of millions of
+// copies of one key, and every copy of that key among the queries would scan
+// its bucket: the product of the two multiplicities, as in the reference's
+// nested bucket loop.  A count-only probe therefore first finds A's heavy
+// keys.  S evenly spaced CSR positions of A (S about n_a / 64: a sample by
+// mass, so a key with m copies is hit about m * S / n_a times) whose bucket
+// holds at least HEAVY_MIN_LEN entries put their key into an open-addressing
+// set, and the first sample in each such bucket lists the bucket.  One scan
+// of the listed buckets counts the copies of every key in the set (all copies
+// of a key sit in its bucket, so the counts are exact): a warp per bucket, and
+// buckets of more than HEAVY_HUGE entries shared by all CTAs in chunks.  A
+// query whose bucket is that long and whose key is in the set adds that count
+// without a scan; any other query with a bucket of COOP_MIN_LEN or more
+// entries is scanned by its whole warp (32 entries per step, coalesced)
+// instead of by one thread.  The count is exact in every case: the sample
+// only decides which keys skip their scan.
+// ---------------------------------------------------------------------------
+constexpr uint32_t HEAVY_PROBES = 32;        // bound on a set lookup / insertion
+constexpr uint32_t HEAVY_MIN_LEN = 64;       // buckets at least this long are sampled for keys
+constexpr uint32_t COOP_MIN_LEN = 64;        // buckets at least this long are scanned by a warp
+constexpr uint32_t HEAVY_HUGE = 1u << 16;    // longer listed buckets are counted by all CTAs
+constexpr uint32_t HEAVY_HUGE_MAX = 1u << 16;  // listed huge buckets (n_a < 2^32)
+constexpr uint32_t HEAVY_CHUNK = 1u << 14;   // bucket entries per counting work item of a huge bucket
+
+// Sample count and set size for a table of n_a keys: S = n_a / 64 rounded up
+// to a power of two in [2^10, 2^22], and S / 8 slots (at least 2^10).
+inline uint32_t heavy_samples(uint64_t n_a) {
+  uint64_t s = 1024;
+  while (s < (n_a >> 6) && s < (1ull << 22)) s <<= 1;
+  return static_cast<uint32_t>(s);
+}
+inline uint32_t heavy_slots(uint64_t n_a) { return std::max<uint32_t>(1024u, heavy_samples(n_a) >> 3); }
+inline size_t heavy_bytes(uint64_t n_a) {
+  return size_t(heavy_slots(n_a)) * 16 + size_t(heavy_samples(n_a)) * 8 + size_t(HEAVY_HUGE_MAX) * 8 + 16;
+}
+
+// The set lives in the workspace, zeroed before the probe: a slot holds ~key
+// (0 = empty, so the all-ones 64-bit key is never heavy) and its count.
+struct HeavySet {
+  unsigned long long* key;    // [slots] ~key
+  unsigned long long* count;  // [slots] copies in A
+  uint2* bucket;              // [samples] listed buckets {lo, hi} of at most HEAVY_HUGE entries
+  uint2* huge;                // [HEAVY_HUGE_MAX] listed longer buckets
+  unsigned* n_list;           // [0] listed buckets, [1] listed huge buckets
+  uint32_t mask;              // slots - 1
+  uint32_t samples;
+};
+
+__device__ __forceinline__ uint32_t heavy_slot(uint64_t key, uint32_t mask) {
+  return static_cast<uint32_t>((key * 0x9E3779B97F4A7C15ull) >> 40) & mask;
+}
+
+// Slot of `key` in the set, or ~0u when it is not there.
+template <typename KeyT>
+__device__ __forceinline__ uint32_t heavy_find(const HeavySet& hs, KeyT key) {
+  const unsigned long long stored = ~static_cast<unsigned long long>(key);
+  if (stored == 0 || hs.key == nullptr) return ~0u;
+  uint32_t h = heavy_slot(static_cast<uint64_t>(key), hs.mask);
+  for (uint32_t p = 0; p < HEAVY_PROBES; p++) {
+    const unsigned long long v = hs.key[h];
+    if (v == stored) return h;
+    if (v == 0) return ~0u;
+    h = (h + 1) & hs.mask;
+  }
+  return ~0u;
+}
+
+// One thread per sample position.
+template <typename KeyT>
+__global__ void __launch_bounds__(256)
+    k_heavy_find(const uint32_t* __restrict__ a_off, const KeyT* __restrict__ a_keys, uint64_t n_a, BucketMap bm,
+                 HeavySet hs, const uint32_t* gate) {
+  if (entry_skip(gate)) return;
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t S = hs.samples;
+  if (i >= S || n_a == 0) return;
+  const uint64_t pos = (i * n_a + n_a / 2) / S;
+  const KeyT key = a_keys[pos];
+  const uint32_t b = bm.of_key(key);
+  const uint32_t lo = a_off[b], hi = a_off[b + 1];
+  if (hi - lo < HEAVY_MIN_LEN || pos < lo || pos >= hi) return;
+  const uint64_t ppos = i > 0 ? ((i - 1) * n_a + n_a / 2) / S : 0;
+  if (i == 0 || ppos < lo) {  // the bucket's first sample lists it
+    if (hi - lo <= HEAVY_HUGE) {
+      const unsigned c = atomicAdd(hs.n_list, 1u);
+      if (c < hs.samples) hs.bucket[c] = make_uint2(lo, hi);
+    } else {
+      const unsigned c = atomicAdd(hs.n_list + 1, 1u);
+      if (c < HEAVY_HUGE_MAX) hs.huge[c] = make_uint2(lo, hi);
+    }
+  } else if (a_keys[ppos] == key) {
+    return;  // the previous sample, in the same bucket, named this key
+  }
+  const unsigned long long stored = ~static_cast<unsigned long long>(key);
+  if (stored == 0) return;
+  uint32_t h = heavy_slot(static_cast<uint64_t>(key), hs.mask);
+  for (uint32_t p = 0; p < HEAVY_PROBES; p++) {
+    const unsigned long long prev = atomicCAS(hs.key + h, 0ull, stored);
+    if (prev == 0 || prev == stored) return;
+    h = (h + 1) & hs.mask;
+  }
+}
+
+// Counts the set's keys in entries [x0, x1) of A with stride `step` from
+// `first`: a thread keeps a run (slot, copies) and adds it to the set when
+// the slot changes; at the end the warp adds its runs (one add when every
+// lane holds the same slot).  Called by whole warps.
+template <typename KeyT>
+__device__ __forceinline__ void heavy_count_range(const KeyT* __restrict__ a_keys, const HeavySet& hs, uint32_t first,
+                                                  uint32_t x1, uint32_t step) {
+  uint32_t run_slot = ~0u;
+  unsigned long long run = 0;
+  for (uint32_t x = first; x < x1; x += step) {
+    const uint32_t h = heavy_find(hs, a_keys[x]);
+    if (h != run_slot) {
+      if (run) atomicAdd(hs.count + run_slot, run);
+      run_slot = h;
+      run = 0;
+    }
+    run += (h != ~0u);
+  }
+  const uint32_t lead_slot = __shfl_sync(FULL_MASK, run_slot, 0);
+  if (__all_sync(FULL_MASK, run_slot == lead_slot)) {
+    run = warp_sum(run);
+    if (lane_id() == 0 && run) atomicAdd(hs.count + lead_slot, run);
+  } else if (run) {
+    atomicAdd(hs.count + run_slot, run);
+  }
+}
+
+// Listed buckets of at most HEAVY_HUGE entries: one warp each.
+template <typename KeyT>
+__global__ void __launch_bounds__(256) k_heavy_count(const KeyT* __restrict__ a_keys, HeavySet hs,
+                                                     const uint32_t* gate) {
+  if (entry_skip(gate)) return;
+  const uint32_t n_b = min(*reinterpret_cast<volatile unsigned*>(hs.n_list), hs.samples);
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n_b; c += warps) {
+    const uint2 bk = hs.bucket[c];
+    heavy_count_range(a_keys, hs, bk.x + lane_id(), bk.y, 32u);
+  }
+}
+
+// Listed buckets of more than HEAVY_HUGE entries: bucket c is cut into
+// HEAVY_CHUNK-entry items, item j goes to CTA (c + j) mod grid, so a bucket of
+// tens of millions of entries is shared by all CTAs.
+template <typename KeyT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_heavy_count_huge(const KeyT* __restrict__ a_keys, HeavySet hs,
+                                                            const uint32_t* gate) {
+  if (entry_skip(gate)) return;
+  const uint32_t n_b = min(*reinterpret_cast<volatile unsigned*>(hs.n_list + 1), HEAVY_HUGE_MAX);
+  const uint32_t grid = gridDim.x;
+  for (uint32_t c = 0; c < n_b; c++) {
+    const uint2 bk = hs.huge[c];
+    const uint32_t chunks = (bk.y - bk.x + HEAVY_CHUNK - 1) / HEAVY_CHUNK;
+    for (uint32_t j = (blockIdx.x + grid - c % grid) % grid; j < chunks; j += grid) {
+      const uint32_t x0 = bk.x + j * HEAVY_CHUNK;
+      heavy_count_range(a_keys, hs, x0 + threadIdx.x, min(bk.y, x0 + HEAVY_CHUNK), uint32_t(BLOCK));
+    }
+  }
+}
+
 // Direct probe.  Persistent: CTAs take tiles of PROBE_TILE queries in ticket
 // order (count-only tiles need no order and use the same loop).
 template <typename KeyT, bool EMIT, bool A_IDX, bool Q_IDX>
@@ -35,8 +199,8 @@ __global__ void __launch_bounds__(PROBE_BLOCK)
     k_probe(const uint32_t* __restrict__ a_off, const KeyT* __restrict__ a_keys, const uint32_t* __restrict__ a_idx,
             BucketMap bm, const KeyT* __restrict__ q, uint64_t nq, const uint32_t* __restrict__ q_idx,
             uint32_t* __restrict__ pairs, uint64_t cap, unsigned long long* d_count, uint64_t* status,
-            unsigned* ticket, const uint32_t* gate) {
-  if (gated_off(gate)) return;
+            unsigned* ticket, const uint32_t* gate, HeavySet hs) {
+  if (entry_skip(gate)) return;
   __shared__ uint64_t red[PROBE_BLOCK / 32 + 1];
   __shared__ uint64_t s_tile, s_prefix;
   const uint64_t ntiles = (nq + PROBE_TILE - 1) / PROBE_TILE;
@@ -62,21 +226,64 @@ __global__ void __launch_bounds__(PROBE_BLOCK)
         hi[j] = a_off[b + 1];
       }
     }
-    // first bucket entries of all the thread's queries are loaded together
-    KeyT first[PROBE_QPT];
-#pragma unroll
-    for (int j = 0; j < PROBE_QPT; j++) first[j] = lo[j] < hi[j] ? a_keys[lo[j]] : KeyT(0);
-#pragma unroll
-    for (int j = 0; j < PROBE_QPT; j++) {
-      if (lo[j] < hi[j]) {
-        c += (first[j] == key[j]);
-        for (uint32_t x = lo[j] + 1; x < hi[j]; x++) c += (a_keys[x] == key[j]);
-      }
-    }
     if constexpr (!EMIT) {
+      // count only: heavy keys take their count from the set, other long
+      // buckets are scanned by the warp, short ones by the thread
+      uint32_t pend = 0, own = 0;
+#pragma unroll
+      for (int j = 0; j < PROBE_QPT; j++) {
+        const uint32_t len = hi[j] - lo[j];
+        const uint32_t h = len >= HEAVY_MIN_LEN ? heavy_find(hs, key[j]) : ~0u;
+        if (h != ~0u) c += hs.count[h];
+        else if (len >= COOP_MIN_LEN) pend |= 1u << j;
+        else if (len) own |= 1u << j;
+      }
+      KeyT first[PROBE_QPT];
+#pragma unroll
+      for (int j = 0; j < PROBE_QPT; j++) first[j] = (own >> j) & 1u ? a_keys[lo[j]] : KeyT(0);
+#pragma unroll
+      for (int j = 0; j < PROBE_QPT; j++) {
+        if ((own >> j) & 1u) {
+          c += (first[j] == key[j]);
+          for (uint32_t x = lo[j] + 1; x < hi[j]; x++) c += (a_keys[x] == key[j]);
+        }
+      }
+      const unsigned lane = lane_id();
+      while (true) {
+        const unsigned who = __ballot_sync(FULL_MASK, pend != 0);
+        if (!who) break;
+        const int leader = __ffs(who) - 1;
+        const int jl = __shfl_sync(FULL_MASK, pend ? __ffs(pend) - 1 : 0, leader);
+        KeyT kk = key[0];
+        uint32_t x0 = lo[0], x1 = hi[0];
+#pragma unroll
+        for (int j = 1; j < PROBE_QPT; j++) {
+          if (jl == j) {
+            kk = key[j];
+            x0 = lo[j];
+            x1 = hi[j];
+          }
+        }
+        if (lane == static_cast<unsigned>(leader)) pend &= pend - 1;
+        kk = __shfl_sync(FULL_MASK, kk, leader);
+        x0 = __shfl_sync(FULL_MASK, x0, leader);
+        x1 = __shfl_sync(FULL_MASK, x1, leader);
+        for (uint32_t x = x0 + lane; x < x1; x += 32) c += (a_keys[x] == kk);
+      }
       counted += c;
       __syncthreads();
     } else {
+      // first bucket entries of all the thread's queries are loaded together
+      KeyT first[PROBE_QPT];
+#pragma unroll
+      for (int j = 0; j < PROBE_QPT; j++) first[j] = lo[j] < hi[j] ? a_keys[lo[j]] : KeyT(0);
+#pragma unroll
+      for (int j = 0; j < PROBE_QPT; j++) {
+        if (lo[j] < hi[j]) {
+          c += (first[j] == key[j]);
+          for (uint32_t x = lo[j] + 1; x < hi[j]; x++) c += (a_keys[x] == key[j]);
+        }
+      }
       uint64_t tile_total;
       const uint64_t excl = block_exclusive_scan<PROBE_BLOCK>(c, red, &tile_total);
       if (threadIdx.x < 32) {
@@ -198,7 +405,7 @@ struct TableProbe {
 template <typename KeyT, bool A_IDX, bool EMIT, int BLOCK, typename Src>
 __global__ void __launch_bounds__(BLOCK)
     k_fine_probe(Src src, uint64_t capq, uint32_t fine_log2, uint32_t capa, const uint32_t* flags) {
-  if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
+  if (entry_skip_on_overflow(flags)) return;
   constexpr uint32_t EPK = 16 / sizeof(KeyT);  // keys per 16 bytes
   constexpr uint32_t QCH = FPROBE_QCH;
   constexpr int NW = BLOCK / 32;
@@ -273,7 +480,11 @@ __global__ void __launch_bounds__(BLOCK)
         }
       }
     }
-    const uint32_t m = mt.qe - mt.qb;
+    uint32_t m = mt.qe - mt.qb;
+    if (mt.qe < mt.qb || m > capq) {  // more queries than the partition's slots: bad device state
+      record_fault(HG_ERR_DEVICE_STATE);
+      m = 0;
+    }
     s_as[b] = as;
     s_ae[b] = ae;
     s_al[b] = al;
@@ -491,7 +702,7 @@ __global__ void __launch_bounds__(CPROBE_BLOCK)
                    const uint32_t* __restrict__ a_off, const KeyT* __restrict__ a_keys,
                    const uint32_t* __restrict__ a_idx, BucketMap bm, uint32_t* __restrict__ pairs, uint64_t pair_cap,
                    unsigned long long* d_count, unsigned* ticket, const uint32_t* flags) {
-  if (*reinterpret_cast<const volatile uint32_t*>(flags) & FLAG_OVERFLOW) return;
+  if (entry_skip_on_overflow(flags)) return;
   constexpr int NW = CPROBE_BLOCK / 32;
   constexpr uint32_t TILE = uint32_t(CPROBE_BLOCK) * QPT;
   __shared__ uint64_t red[NW + 1];
@@ -709,6 +920,8 @@ hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, 
   p.off_status = off;  off = align_up(off + (emit ? p.tiles * 8 : 0));
   p.off_ticket = off;  off = align_up(off + 4 * sizeof(unsigned));
   p.off_flags = off;   off = align_up(off + sizeof(uint32_t));
+  // count only: the heavy-key set of the direct probe (zeroed with the counters)
+  p.off_heavy = off;   off = align_up(off + (emit ? 0 : heavy_bytes(n_a)));
   if (path == PROBE_PARTITIONED) {
     const PartGeometry& g = p.g;
     p.off_pcount = off;  off = align_up(off + (g.n_parts + 1) * 4);
@@ -735,18 +948,46 @@ hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, 
   return HG_OK;
 }
 
+static HeavySet heavy_set(const ProbePlan& p, char* ws) {
+  HeavySet hs{nullptr, nullptr, nullptr, nullptr, nullptr, 0u, 0u};
+  if (p.emit) return hs;
+  const size_t slots = heavy_slots(p.n_a), samples = heavy_samples(p.n_a);
+  char* h = ws + p.off_heavy;
+  hs.key = reinterpret_cast<unsigned long long*>(h);
+  hs.count = reinterpret_cast<unsigned long long*>(h + slots * 8);
+  hs.bucket = reinterpret_cast<uint2*>(h + slots * 16);
+  hs.huge = reinterpret_cast<uint2*>(h + slots * 16 + samples * 8);
+  hs.n_list = reinterpret_cast<unsigned*>(h + slots * 16 + samples * 8 + size_t(HEAVY_HUGE_MAX) * 8);
+  hs.mask = static_cast<uint32_t>(slots - 1);
+  hs.samples = static_cast<uint32_t>(samples);
+  return hs;
+}
+
 template <typename KeyT, bool EMIT>
 static void launch_probe_direct(const ProbePlan& p, const uint32_t* a_off, const KeyT* a_keys, const uint32_t* a_idx,
                                 const KeyT* q, const uint32_t* q_idx, uint32_t* pairs, uint64_t cap,
                                 unsigned long long* d_count, uint64_t* status, unsigned* ticket, const uint32_t* gate,
-                                cudaStream_t s) {
+                                HeavySet hs, cudaStream_t s) {
   const BucketMap bm = p.bucket_map();
+  if constexpr (!EMIT) {
+    // the heavy keys of A (their set was zeroed with the workspace)
+    if (p.n_a > 0 && hs.key != nullptr) {
+      Phase ph(s, gate ? "fallback_heavy_keys" : "heavy_keys");
+      count_launch();
+      k_heavy_find<KeyT><<<(hs.samples + 255) / 256, 256, 0, s>>>(a_off, a_keys, p.n_a, bm, hs, gate);
+      const unsigned grid = static_cast<unsigned>(device_sm_count()) * 4;
+      count_launch();
+      k_heavy_count<KeyT><<<grid, 256, 0, s>>>(a_keys, hs, gate);
+      count_launch();
+      k_heavy_count_huge<KeyT, 256><<<grid, 256, 0, s>>>(a_keys, hs, gate);
+    }
+  }
   const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(p.tiles, uint64_t(device_sm_count()) * 8));
   Phase ph(s, gate ? (EMIT ? "fallback_probe_emit" : "fallback_probe_count") : (EMIT ? "probe_emit" : "probe_count"));
   count_launch();
 #define HG_PROBE_LAUNCH(AI, QI)                                                                            \
   k_probe<KeyT, EMIT, AI, QI><<<grid, PROBE_BLOCK, 0, s>>>(a_off, a_keys, a_idx, bm, q, p.nq, q_idx, pairs, \
-                                                          cap, d_count, status, ticket, gate)
+                                                          cap, d_count, status, ticket, gate, hs)
   if (a_idx) {
     if (q_idx) HG_PROBE_LAUNCH(true, true); else HG_PROBE_LAUNCH(true, false);
   } else {
@@ -809,7 +1050,8 @@ static hg_status run_probe_partitioned(const ProbePlan& p, const uint32_t* a_off
   }
   // Fallback when a query partition overflowed (heavy duplicates): the direct
   // probe, gated on the flag.
-  launch_probe_direct<KeyT, EMIT>(p, a_off, a_keys, a_idx, q, q_idx, pairs, cap, d_count, status, ticket, flags, s);
+  launch_probe_direct<KeyT, EMIT>(p, a_off, a_keys, a_idx, q, q_idx, pairs, cap, d_count, status, ticket, flags,
+                                  heavy_set(p, ws), s);
   return HG_OK;
 }
 
@@ -833,7 +1075,7 @@ static hg_status run_probe_coarse(const ProbePlan& p, const uint32_t* a_off, con
                                                        "probe_multisplit", s);
   if (st != HG_OK) return st;
   {
-    // queries per thread (tuning override HG_CPROBE_QPT = 1, 2 or 4): fewer
+    // queries per thread (tuning override HG_CPROBE_QPT = 1 or 2): fewer
     // queries per thread keep more warps resident, which hides the L2 latency
     // of the bucket reads better (2^28 u64 with pairs: 8 -> 4.94 ms, 4 ->
     // 3.85, 2 -> 3.36, 1 -> 3.84)
@@ -841,7 +1083,7 @@ static hg_status run_probe_coarse(const ProbePlan& p, const uint32_t* a_off, con
     const int block = CPROBE_BLOCK;
     if (const char* e = std::getenv("HG_CPROBE_QPT")) {
       const int v = std::atoi(e);
-      qpt = (v == 1 || v == 4) ? v : 2;
+      qpt = v == 1 ? 1 : 2;
     }
     const uint32_t tiles_per_part =
         static_cast<uint32_t>((g.part_cap + uint64_t(block) * qpt - 1) / (uint64_t(block) * qpt));
@@ -867,13 +1109,13 @@ static hg_status run_probe_coarse(const ProbePlan& p, const uint32_t* a_off, con
       else go(k_coarse_probe<KeyT, EMIT, false, Q>);
     };
     if (qpt == 1) pick(std::integral_constant<int, 1>{});
-    else if (qpt == 4) pick(std::integral_constant<int, 4>{});
     else pick(std::integral_constant<int, 2>{});
     if (st != HG_OK) return st;
   }
   // Fallback when a query range overflowed its slots (heavy duplicates): the
   // direct probe, gated on the flag.
-  launch_probe_direct<KeyT, EMIT>(p, a_off, a_keys, a_idx, q, q_idx, pairs, cap, d_count, status, ticket, flags, s);
+  launch_probe_direct<KeyT, EMIT>(p, a_off, a_keys, a_idx, q, q_idx, pairs, cap, d_count, status, ticket, flags,
+                                  heavy_set(p, ws), s);
   return HG_OK;
 }
 
@@ -903,8 +1145,12 @@ hg_status launch_probe(const ProbePlan& p, const uint32_t* a_off, const void* a_
     }
     const cudaError_t e = cudaMemsetAsync(ws, 0, p.total, s);
     if (e != cudaSuccess) { st = cuda_fail(e, "intersect: workspace memset"); return; }
-    if (emit) launch_probe_direct<KeyT, true>(p, a_off, ak, a_idx, qk, q_idx, pairs, pair_cap, d_count, status, ticket, nullptr, s);
-    else launch_probe_direct<KeyT, false>(p, a_off, ak, a_idx, qk, q_idx, pairs, pair_cap, d_count, status, ticket, nullptr, s);
+    if (emit)
+      launch_probe_direct<KeyT, true>(p, a_off, ak, a_idx, qk, q_idx, pairs, pair_cap, d_count, status, ticket, nullptr,
+                                      heavy_set(p, ws), s);
+    else
+      launch_probe_direct<KeyT, false>(p, a_off, ak, a_idx, qk, q_idx, pairs, pair_cap, d_count, status, ticket,
+                                       nullptr, heavy_set(p, ws), s);
   };
   if (p.key_bytes == 4) run(uint32_t{});
   else run(uint64_t{});

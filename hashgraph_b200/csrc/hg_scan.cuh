@@ -20,6 +20,9 @@ constexpr uint64_t ST_AGGREGATE = 1ull << 62;
 constexpr uint64_t ST_PREFIX = 2ull << 62;
 constexpr uint64_t ST_VALUE = (1ull << 62) - 1;
 constexpr uint32_t LOOKBACK_SPIN_LIMIT = 1u << 22;
+// Polls a look-back makes before it gives up: LOOKBACK_SPIN_LIMIT unless a
+// test lowered it (hg_debug_set_wait_limit) to make the wait run out.
+__device__ uint32_t g_lookback_limit = LOOKBACK_SPIN_LIMIT;
 
 __device__ __forceinline__ uint64_t ld_acquire(const uint64_t* p) {
   cuda::atomic_ref<const unsigned long long, cuda::thread_scope_device> r(
@@ -87,13 +90,14 @@ __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint64_
   uint64_t excl = 0;
   int64_t pred = static_cast<int64_t>(tile) - 1;
   uint32_t spins = 0;
+  const uint32_t limit = *reinterpret_cast<const volatile uint32_t*>(&g_lookback_limit);
   unsigned sleep_ns = 8;
   while (true) {
     const int64_t j = pred - static_cast<int64_t>(lane);
     uint64_t s = j >= 0 ? ld_acquire(status + j) : ST_PREFIX;
     while (__any_sync(FULL_MASK, (s >> 62) == 0)) {
-      if (++spins > LOOKBACK_SPIN_LIMIT) {
-        record_error(HG_ERR_DEVICE_TIMEOUT);
+      if (++spins > limit) {
+        record_fault(HG_ERR_DEVICE_TIMEOUT);  // later kernels return at entry
         return excl;
       }
       __nanosleep(sleep_ns);

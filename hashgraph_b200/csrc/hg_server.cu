@@ -17,9 +17,25 @@
 // the next build instead of being unmapped at the next synchronisation.
 // Latency = arrival time (the caller's CLOCK_MONOTONIC stamp) to the device
 // completion of the request's last operation, mapped onto the host clock by
-// one reference event recorded when the server starts.
+// a reference event (re-taken every REF_MAX_AGE_S).
+//
+// Continuous batching: a request of at most `batch_small` keys is not
+// launched on its own.  It joins a queue, and the queue is flushed as ONE
+// batched launch sequence (hg_batch: build-only pairs for the queued builds,
+// probe-only pairs for the queued intersects, against resident tables or
+// tables built in the same batch) when it holds `batch_max` requests, when
+// its oldest request has waited `batch_wait` seconds (checked at every poll),
+// before any request that is launched on its own (so requests keep their
+// order), and when the caller blocks for completions.  A flush is cut into
+// segments of builds followed by intersects, in submission order, so every
+// intersect sees the tables the requests before it left: a build after an
+// intersect, or a second build of one table, starts a new segment.  Each
+// segment takes one stream, waits for the builds (on other streams) of the
+// tables it probes, and uploads its descriptors from a pinned ring buffer
+// without synchronising.
 #include <time.h>
 
+#include <algorithm>
 #include <deque>
 #include <list>
 #include <unordered_map>
@@ -51,6 +67,22 @@ struct ServerReq {
   uint32_t slot;              // count slot (intersect)
 };
 
+// A request waiting in the batching queue.
+struct QueuedReq {
+  int kind;                   // 0 build, 1 intersect
+  uint64_t table_id;
+  const void* data;           // keys (build) or queries (intersect)
+  uint64_t n, n_buckets;
+  int with_index;
+  uint32_t* d_pairs;
+  uint64_t pair_cap;
+  double arrival;
+  uint64_t ticket;
+};
+
+constexpr size_t STAGE_BYTES = size_t(4) << 20;  // pinned descriptor buffer of one batch
+constexpr int STAGE_RING = 8;
+
 static double monotonic_s() {
   timespec ts;
   clock_gettime(CLOCK_MONOTONIC, &ts);
@@ -79,6 +111,18 @@ struct hg_server {
   cudaStream_t clock_stream = nullptr;  // carries only `ref`, so `ref` completes at once
   cudaEvent_t ref = nullptr;
   double ref_host = 0;
+  // continuous batching
+  bool batching = true;
+  uint64_t batch_small = 1ull << 16;
+  uint32_t batch_max = 256;
+  double batch_wait = 100e-6;
+  std::vector<hg::QueuedReq> queue;
+  double queued_since = 0;
+  std::vector<void*> stage;             // pinned descriptor buffers (a ring)
+  std::vector<cudaEvent_t> stage_done;  // recorded after the batch that used the buffer
+  std::vector<uint8_t> stage_used;
+  size_t stage_next = 0;
+  uint64_t batches = 0, batched_requests = 0;
 };
 
 namespace hg {
@@ -119,9 +163,16 @@ static void evict(hg_server* s, uint64_t id) {
   s->tables.erase(it);
 }
 
-static void make_room(hg_server* s, size_t need) {
-  while (!s->lru.empty() && (s->bytes + need > s->budget || s->tables.size() >= size_t(s->max_tables))) {
-    evict(s, s->lru.front());
+// Evicts least recently used tables until `need` more bytes and one more
+// table fit.  Tables in `pinned` (built by the batch being planned, not yet
+// launched) are never evicted; if only they are left, the budget is exceeded
+// until the next build.
+static void make_room(hg_server* s, size_t need, const std::vector<uint64_t>* pinned = nullptr) {
+  auto it = s->lru.begin();
+  while (it != s->lru.end() && (s->bytes + need > s->budget || s->tables.size() >= size_t(s->max_tables))) {
+    const uint64_t id = *it++;
+    if (pinned && std::find(pinned->begin(), pinned->end(), id) != pinned->end()) continue;
+    evict(s, id);
     s->evictions++;
   }
 }
@@ -167,6 +218,131 @@ static cudaError_t rebase_clock(hg_server* s) {
   return e;
 }
 
+// Launches one segment of the queue (builds, then intersects) as one batch.
+static hg_status launch_segment(hg_server* s, const QueuedReq* q, size_t n) {
+  uint64_t keys = 0;
+  for (size_t i = 0; i < n; i++) keys += q[i].n;
+  const int si = pick_stream(s, 20e-6 + double(keys) * 4e-11);
+  cudaStream_t st = s->streams[si];
+  std::vector<hg_batch_pair> pairs;
+  std::vector<ServerReq> reqs;
+  std::vector<uint64_t> built;  // table ids this segment builds
+  pairs.reserve(n);
+  reqs.reserve(n);
+  for (size_t i = 0; i < n; i++) {
+    const QueuedReq& r = q[i];
+    ServerReq sr{r.ticket, r.kind, 0, r.arrival, nullptr, 0};
+    if (r.kind == 0) {
+      const size_t bytes = (r.n_buckets + 1) * 4 + r.n * (s->key_bytes + (r.with_index ? 4 : 0));
+      if (s->tables.count(r.table_id)) evict(s, r.table_id);  // replaced (not built in this segment)
+      make_room(s, bytes, &built);
+      ServerTable t;
+      t.n = r.n;
+      t.n_buckets = r.n_buckets;
+      t.with_index = r.with_index != 0;
+      t.bytes = bytes;
+      t.stream = si;
+      cudaError_t e = cudaMallocFromPoolAsync(&t.offsets, (r.n_buckets + 1) * 4, s->pool, st);
+      if (e == cudaSuccess && r.n) e = cudaMallocFromPoolAsync(&t.keys, r.n * s->key_bytes, s->pool, st);
+      if (e == cudaSuccess && r.n && r.with_index)
+        e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&t.idx), r.n * 4, s->pool, st);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t.ready, cudaEventDisableTiming);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (t.offsets) cudaFreeAsync(t.offsets, st);
+        if (t.keys) cudaFreeAsync(t.keys, st);
+        if (t.idx) cudaFreeAsync(t.idx, st);
+        return cuda_fail(e, "hg_server: table allocation");
+      }
+      s->lru.push_back(r.table_id);
+      t.lru = std::prev(s->lru.end());
+      s->bytes += bytes;
+      s->tables.emplace(r.table_id, t);
+      built.push_back(r.table_id);
+      pairs.push_back(hg_batch_pair{r.data, r.n, r.n_buckets, nullptr, 0, t.offsets, t.keys, t.idx, nullptr, 0,
+                                    nullptr});
+    } else {
+      uint32_t slot = 0;
+      hg_status hs = reserve_slot(s, &slot);
+      if (hs != HG_OK) return hs;
+      sr.slot = slot;
+      auto it = s->tables.find(r.table_id);
+      if (it == s->tables.end()) {
+        sr.missed = 1;
+      } else {
+        ServerTable& t = it->second;
+        s->lru.splice(s->lru.end(), s->lru, t.lru);
+        if (std::find(built.begin(), built.end(), r.table_id) == built.end() && t.stream != si)
+          cudaStreamWaitEvent(st, t.ready, 0);
+        pairs.push_back(hg_batch_pair{nullptr, t.n, t.n_buckets, r.data, r.n, t.offsets, t.keys, t.idx, r.d_pairs,
+                                      r.d_pairs ? r.pair_cap : 0, s->d_counts + slot});
+      }
+    }
+    reqs.push_back(sr);
+  }
+  if (!pairs.empty()) {
+    const size_t k = s->stage_next;
+    s->stage_next = (k + 1) % s->stage.size();
+    if (s->stage_used[k]) HG_CUDA(cudaEventSynchronize(s->stage_done[k]), "hg_server: descriptor buffer");
+    hg_batch* b = nullptr;
+    hg_status hs = batch_create_staged(pairs.data(), int(pairs.size()), s->key_bytes, nullptr, st, s->pool,
+                                       s->stage[k], STAGE_BYTES, &b);
+    if (hs != HG_OK) return hs;
+    hs = hg_batch_run(b, reinterpret_cast<hg_stream_t>(st));
+    hg_batch_free(b, reinterpret_cast<hg_stream_t>(st));
+    if (hs != HG_OK) return hs;
+    HG_CUDA(cudaEventRecord(s->stage_done[k], st), "hg_server: event");
+    s->stage_used[k] = 1;
+    s->batches++;
+    s->batched_requests += n;
+  }
+  for (uint64_t id : built) cudaEventRecord(s->tables[id].ready, st);
+  for (ServerReq& sr : reqs) {
+    if (sr.kind == 1 && !sr.missed)
+      cudaMemcpyAsync(s->h_counts + sr.slot, s->d_counts + sr.slot, sizeof(unsigned long long),
+                      cudaMemcpyDeviceToHost, st);
+    sr.done = take_event(s);
+    cudaEventRecord(sr.done, st);
+    s->inflight.push_back(sr);
+  }
+  return HG_OK;
+}
+
+// Launches every queued request, one segment per run of builds followed by
+// intersects (a build after an intersect, or a second build of one table,
+// starts the next segment), at most batch_max requests each.
+static hg_status flush_queue(hg_server* s) {
+  size_t i = 0;
+  const size_t n = s->queue.size();
+  hg_status st = HG_OK;
+  while (i < n && st == HG_OK) {
+    size_t j = i;
+    bool seen_intersect = false;
+    std::vector<uint64_t> ids;
+    while (j < n && j - i < s->batch_max) {
+      const QueuedReq& r = s->queue[j];
+      if (r.kind == 0) {
+        if (seen_intersect || std::find(ids.begin(), ids.end(), r.table_id) != ids.end()) break;
+        ids.push_back(r.table_id);
+      } else {
+        seen_intersect = true;
+      }
+      j++;
+    }
+    st = launch_segment(s, s->queue.data() + i, j - i);
+    i = j;
+  }
+  s->queue.clear();
+  return st;
+}
+
+static hg_status enqueue(hg_server* s, const QueuedReq& r) {
+  if (s->queue.empty()) s->queued_since = monotonic_s();
+  s->queue.push_back(r);
+  if (s->queue.size() >= s->batch_max) return flush_queue(s);
+  return HG_OK;
+}
+
 }  // namespace hg
 
 using namespace hg;
@@ -175,6 +351,7 @@ extern "C" double hg_server_now(void) { return monotonic_s(); }
 
 extern "C" void hg_server_free(hg_server* s) {
   if (!s) return;
+  if (!s->queue.empty()) flush_queue(s);  // queued requests still run: their inputs may be the caller's to reuse
   for (auto& st : s->streams) cudaStreamSynchronize(st);
   if (!s->streams.empty()) {
     cudaStream_t st = s->streams[0];
@@ -193,6 +370,8 @@ extern "C" void hg_server_free(hg_server* s) {
   for (auto p : s->pair_buf) cudaFree(p);
   if (s->d_counts) cudaFree(s->d_counts);
   if (s->h_counts) cudaFreeHost(s->h_counts);
+  for (auto h : s->stage) cudaFreeHost(h);
+  for (auto e : s->stage_done) cudaEventDestroy(e);
   if (s->ref) cudaEventDestroy(s->ref);
   if (s->clock_stream) cudaStreamDestroy(s->clock_stream);
   for (auto& st : s->streams) cudaStreamDestroy(st);
@@ -251,6 +430,17 @@ extern "C" hg_status hg_server_create(size_t budget_bytes, int max_tables, int n
   }
   if (e == cudaSuccess) e = cudaMalloc(&s->d_counts, sizeof(unsigned long long) * s->n_slots);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_counts, sizeof(unsigned long long) * s->n_slots);
+  for (int i = 0; i < STAGE_RING && e == cudaSuccess; i++) {
+    void* h = nullptr;
+    e = cudaMallocHost(&h, STAGE_BYTES);
+    if (e != cudaSuccess) break;
+    s->stage.push_back(h);
+    cudaEvent_t ev = nullptr;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) break;
+    s->stage_done.push_back(ev);
+    s->stage_used.push_back(0);
+  }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->clock_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&s->ref);
   if (e == cudaSuccess) e = rebase_clock(s);
@@ -291,6 +481,14 @@ extern "C" hg_status hg_server_build(hg_server* s, uint64_t table_id, const void
   if (!s || !ticket || (n > 0 && !d_keys) || n_buckets == 0) return HG_ERR_INVALID_ARGUMENT;
   if (n > s->max_keys || n_buckets > s->max_keys)
     return lib_fail(HG_ERR_TOO_LARGE, "hg_server_build: more keys or buckets than the server's max_keys");
+  if (s->batching && n <= s->batch_small) {
+    *ticket = s->next_ticket++;
+    return enqueue(s, QueuedReq{0, table_id, d_keys, n, n_buckets, with_index, nullptr, 0, arrival_s, *ticket});
+  }
+  if (!s->queue.empty()) {  // queued requests go first
+    hg_status qs = flush_queue(s);
+    if (qs != HG_OK) return qs;
+  }
   const size_t bytes = (n_buckets + 1) * 4 + n * (s->key_bytes + (with_index ? 4 : 0));
   if (s->tables.count(table_id)) evict(s, table_id);  // replaced
   make_room(s, bytes);
@@ -339,6 +537,14 @@ extern "C" hg_status hg_server_intersect(hg_server* s, uint64_t table_id, const 
                                          uint32_t* d_pairs, uint64_t pair_cap, double arrival_s, uint64_t* ticket) {
   if (!s || !ticket || (nq > 0 && !d_query)) return HG_ERR_INVALID_ARGUMENT;
   if (nq > s->max_keys) return lib_fail(HG_ERR_TOO_LARGE, "hg_server_intersect: more queries than max_keys");
+  if (s->batching && nq <= s->batch_small) {
+    *ticket = s->next_ticket++;
+    return enqueue(s, QueuedReq{1, table_id, d_query, nq, 0, 0, d_pairs, pair_cap, arrival_s, *ticket});
+  }
+  if (!s->queue.empty()) {  // queued requests go first
+    hg_status qs = flush_queue(s);
+    if (qs != HG_OK) return qs;
+  }
   uint32_t slot = 0;
   hg_status hs = reserve_slot(s, &slot);
   if (hs != HG_OK) return hs;
@@ -372,6 +578,10 @@ extern "C" hg_status hg_server_intersect(hg_server* s, uint64_t table_id, const 
 extern "C" hg_status hg_server_poll(hg_server* s, int block, hg_server_done* out, int max_out, int* n_out) {
   if (!s || !n_out || (max_out > 0 && !out)) return HG_ERR_INVALID_ARGUMENT;
   *n_out = 0;
+  if (!s->queue.empty() && (block || monotonic_s() - s->queued_since >= s->batch_wait)) {
+    hg_status qs = flush_queue(s);
+    if (qs != HG_OK) return qs;
+  }
   if (block && !s->inflight.empty() && max_out > 0) {
     const cudaError_t e = cudaEventSynchronize(s->inflight.front().done);
     if (e != cudaSuccess) return cuda_fail(e, "hg_server_poll: wait");
@@ -410,6 +620,27 @@ extern "C" hg_status hg_server_stats(const hg_server* s, uint64_t* resident_tabl
   if (resident_tables) *resident_tables = s->tables.size();
   if (resident_bytes) *resident_bytes = s->bytes;
   if (evictions) *evictions = s->evictions;
-  if (inflight) *inflight = s->inflight.size();
+  if (inflight) *inflight = s->inflight.size() + s->queue.size();
+  return HG_OK;
+}
+
+extern "C" hg_status hg_server_set_batching(hg_server* s, int enabled, uint64_t small_max, uint32_t max_queued,
+                                            double max_wait_s) {
+  if (!s || max_queued == 0 || max_wait_s < 0) return HG_ERR_INVALID_ARGUMENT;
+  if (!s->queue.empty()) {
+    hg_status st = flush_queue(s);
+    if (st != HG_OK) return st;
+  }
+  s->batching = enabled != 0;
+  s->batch_small = small_max;
+  s->batch_max = max_queued;
+  s->batch_wait = max_wait_s;
+  return HG_OK;
+}
+
+extern "C" hg_status hg_server_batch_stats(const hg_server* s, uint64_t* batches, uint64_t* batched_requests) {
+  if (!s) return HG_ERR_INVALID_ARGUMENT;
+  if (batches) *batches = s->batches;
+  if (batched_requests) *batched_requests = s->batched_requests;
   return HG_OK;
 }

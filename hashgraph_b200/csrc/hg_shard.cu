@@ -69,6 +69,7 @@ template <typename KeyT>
 __global__ void __launch_bounds__(HIST_BLOCK) k_shard_hist(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
                                                            uint64_t bin_magic, uint32_t n_bins,
                                                            unsigned long long* __restrict__ bins) {
+  if (entry_skip(nullptr)) return;
   extern __shared__ uint32_t s_bin[];
   for (uint32_t i = threadIdx.x; i < n_bins; i += HIST_BLOCK) s_bin[i] = 0;
   __syncthreads();
@@ -120,6 +121,7 @@ template <typename KeyT>
 __global__ void __launch_bounds__(ROUTE_BLOCK, 4) k_route_count(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm,
                                                              ShardSplits splits, int G,
                                                              uint32_t* __restrict__ tile_counts, uint64_t tiles) {
+  if (entry_skip(nullptr)) return;
   __shared__ uint64_t s_split[SHARD_MAX + 1];
   __shared__ uint32_t s_wc[ROUTE_WARPS][SHARD_MAX];
   for (int i = threadIdx.x; i <= G; i += ROUTE_BLOCK) s_split[i] = splits.s[i];
@@ -149,6 +151,7 @@ __global__ void __launch_bounds__(ROUTE_BLOCK, 4) k_route_scatter(const KeyT* __
                                                                const uint32_t* __restrict__ tile_start, uint64_t tiles,
                                                                KeyT* __restrict__ keys_out,
                                                                uint32_t* __restrict__ idx_out, uint32_t index_base) {
+  if (entry_skip(nullptr)) return;
   __shared__ uint64_t s_split[SHARD_MAX + 1];
   __shared__ uint32_t s_wc[ROUTE_WARPS][SHARD_MAX];
   for (int i = threadIdx.x; i <= G; i += ROUTE_BLOCK) s_split[i] = splits.s[i];
@@ -179,8 +182,12 @@ __global__ void __launch_bounds__(ROUTE_BLOCK, 4) k_route_scatter(const KeyT* __
     if (d[j] < SHARD_MAX) {
       const uint32_t at = s_wc[w][d[j]];
       const uint32_t pos = at + __popc(peers & lanemask_lt());
-      keys_out[pos] = k[j];
-      if constexpr (WITH_IDX) idx_out[pos] = index_base + static_cast<uint32_t>(base + uint64_t(j) * 32 + lane_id());
+      if (pos < n) {
+        keys_out[pos] = k[j];
+        if constexpr (WITH_IDX) idx_out[pos] = index_base + static_cast<uint32_t>(base + uint64_t(j) * 32 + lane_id());
+      } else {
+        record_fault(HG_ERR_DEVICE_STATE);  // tile starts past n: write nothing
+      }
       __syncwarp(peers);
       if (lane_id() == unsigned(__ffs(peers) - 1)) s_wc[w][d[j]] = at + __popc(peers);
     }
@@ -191,6 +198,7 @@ __global__ void __launch_bounds__(ROUTE_BLOCK, 4) k_route_scatter(const KeyT* __
 // offsets[r] = first routed key of shard r (offsets[G] = n).
 __global__ void k_route_offsets(const uint32_t* __restrict__ tile_start, uint64_t tiles, int G, uint64_t n,
                                 unsigned long long* __restrict__ offsets) {
+  if (entry_skip(nullptr)) return;
   const int r = threadIdx.x;
   if (r < G) offsets[r] = tiles ? tile_start[uint64_t(r) * tiles] : 0ull;
   if (r == G) offsets[r] = n;

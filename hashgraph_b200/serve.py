@@ -31,6 +31,7 @@ class Request:
     with_index: bool = False
     queries: object = None         # intersect: device query tensor
     pair_cap: int = 0
+    pairs: object = None           # intersect: optional int32 [pair_cap, 2] device tensor for the pairs
     # filled when the request completes
     count: int | None = None
     latency_s: float | None = None
@@ -46,10 +47,14 @@ def now() -> float:
 class Server:
     """A native serving engine on the current device: `budget_bytes` of
     resident tables at most, `max_tables` tables at most, `n_streams` CUDA
-    streams, tables of up to `max_keys` keys and buckets."""
+    streams, tables of up to `max_keys` keys and buckets.  With `batching`,
+    requests of at most `batch_small` keys are coalesced into batched launches
+    (continuous batching: at most `batch_max` per launch, none waiting longer
+    than `batch_wait_s` once the caller polls)."""
 
     def __init__(self, budget_bytes: int, max_tables: int = 512, n_streams: int = 4, max_keys: int = 1 << 24,
-                 key_bytes: int = 8, device=None):
+                 key_bytes: int = 8, device=None, batching: bool = True, batch_small: int = 1 << 16,
+                 batch_max: int = 256, batch_wait_s: float = 100e-6):
         import torch
         if device is not None:
             torch.cuda.set_device(torch.device(device))
@@ -57,6 +62,8 @@ class Server:
         self._h = ctypes.c_void_p()
         check(lib().hg_server_create(int(budget_bytes), int(max_tables), int(n_streams), int(max_keys), key_bytes,
                                      ctypes.byref(self._h)), "hg_server_create")
+        check(lib().hg_server_set_batching(self._h, int(batching), int(batch_small), int(batch_max),
+                                           float(batch_wait_s)), "hg_server_set_batching")
         self._pending: dict[int, Request] = {}
         self._done = (ServerDone * 1024)()
 
@@ -71,7 +78,9 @@ class Server:
             check(L.hg_server_build(self._h, r.table_id, _ptr(r.keys), r.keys.numel(), r.n_buckets, int(r.with_index),
                                     r.arrival, ctypes.byref(t)), "hg_server_build")
         else:
-            check(L.hg_server_intersect(self._h, r.table_id, _ptr(r.queries), r.queries.numel(), None, r.pair_cap,
+            pairs = _ptr(r.pairs) if r.pairs is not None else None
+            cap = min(r.pair_cap, r.pairs.shape[0]) if r.pairs is not None else r.pair_cap
+            check(L.hg_server_intersect(self._h, r.table_id, _ptr(r.queries), r.queries.numel(), pairs, cap,
                                         r.arrival, ctypes.byref(t)), "hg_server_intersect")
         r.ticket = t.value
         self._pending[r.ticket] = r
@@ -105,7 +114,10 @@ class Server:
         b = ctypes.c_size_t(0)
         check(lib().hg_server_stats(self._h, ctypes.byref(t), ctypes.byref(b), ctypes.byref(e), ctypes.byref(f)),
               "hg_server_stats")
-        return {"resident_tables": t.value, "resident_bytes": b.value, "evictions": e.value, "inflight": f.value}
+        nb, nr = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        check(lib().hg_server_batch_stats(self._h, ctypes.byref(nb), ctypes.byref(nr)), "hg_server_batch_stats")
+        return {"resident_tables": t.value, "resident_bytes": b.value, "evictions": e.value, "inflight": f.value,
+                "batches": nb.value, "batched_requests": nr.value}
 
     def free(self) -> None:
         if self._h:

@@ -51,6 +51,8 @@ typedef int32_t hg_status;
 #define HG_ERR_NO_DEVICE        (-7)
 #define HG_ERR_KEY_WIDTH        (-8) /* key_bytes not 4 or 8, or tables of different key width */
 #define HG_ERR_BUCKET_MISMATCH  (-9) /* tables built with different n_buckets */
+#define HG_ERR_DEVICE_STATE     (-10) /* a kernel found a position outside its output (device state
+                                        * inconsistent, e.g. after a wait that gave up) and wrote nothing */
 
 /* Human-readable text for a status code (static storage). */
 const char* hg_status_str(hg_status status);
@@ -67,9 +69,21 @@ const char* hg_last_error(void);
  * (include/SingleHashGraphOperators.cuh:31-69). */
 uint32_t hg_hash(uint64_t key);
 
-/* Reads (then clears) the per-device error word after synchronising `stream`.
- * *code receives HG_OK or the first HG_ERR_* recorded by a kernel. */
+/* Reads (then clears) the per-device error words after synchronising `stream`.
+ * *code receives HG_OK, the fault (HG_ERR_DEVICE_TIMEOUT: a bounded device-side
+ * wait gave up; HG_ERR_DEVICE_STATE: a position outside its output) when one
+ * was recorded, else the first HG_ERR_* recorded by a kernel (for instance
+ * HG_ERR_PAIR_CAPACITY).  After a fault every kernel of the library on the
+ * device returns at entry, writing nothing, until this call clears it: every
+ * result produced since the fault is invalid.  The reference has no device
+ * error path (it prints and calls exit(0), include/MultiHashGraph.cuh:56-57). */
 hg_status hg_device_error(hg_stream_t stream, hg_status* code);
+
+/* Test hook (no counterpart in the reference): the number of polls a
+ * decoupled look-back makes before it gives up and records
+ * HG_ERR_DEVICE_TIMEOUT.  0 restores the default (2^22).  Lowering it makes
+ * the bounded wait run out on purpose, to test the error path. */
+hg_status hg_debug_set_wait_limit(uint32_t polls, hg_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * Build with caller-owned outputs and workspace.
@@ -247,6 +261,14 @@ hg_status hg_intersect_tables(const hg_table* a, const hg_table* b, uint32_t* d_
  * HG_ERR_PAIR_CAPACITY in the device error word.  All pairs share the key
  * width.  Every pointer is device memory owned by the caller; the buffers
  * must not overlap between pairs.
+ *
+ * Probe-only and build-only pairs: a pair whose d_keys is NULL while n > 0
+ * names a table already built (by hg_build_into, an earlier batch or a table
+ * file) in d_offsets / d_keys_out / d_idx_out; the batch only probes it, and
+ * it may be the table another pair of the same batch builds (every build of
+ * a run finishes before its first probe).  A pair with nq = 0 is only built;
+ * its d_count may then be NULL.  The serving engine coalesces its queued
+ * requests into such batches.
  * ---------------------------------------------------------------------- */
 typedef struct hg_batch_pair {
   const void* d_keys;
@@ -396,14 +418,26 @@ hg_status hg_server_reserve(hg_server* server, size_t bytes);
 hg_status hg_server_build(hg_server* server, uint64_t table_id, const void* d_keys, uint64_t n,
                           uint64_t n_buckets, int with_index, double arrival_s, uint64_t* ticket);
 /* Probes d_query[0..nq) (the same rules as the keys of a build) against
- * table `table_id`; pairs go to d_pairs (or,
- * when NULL, to a per-stream buffer the next request overwrites). */
+ * table `table_id`; pairs go to d_pairs (or, when NULL, nowhere for a
+ * batched request and to a per-stream buffer the next request overwrites for
+ * one launched on its own). */
 hg_status hg_server_intersect(hg_server* server, uint64_t table_id, const void* d_query, uint64_t nq,
                               uint32_t* d_pairs, uint64_t pair_cap, double arrival_s, uint64_t* ticket);
 /* Reports up to max_out completed requests (block: wait for the oldest). */
 hg_status hg_server_poll(hg_server* server, int block, hg_server_done* out, int max_out, int* n_out);
 hg_status hg_server_stats(const hg_server* server, uint64_t* resident_tables, size_t* resident_bytes,
                           uint64_t* evictions, uint64_t* inflight);
+/* Continuous batching (no counterpart in the reference, which has no serving
+ * path).  Requests of at most small_max keys (queries) are queued and
+ * launched together as one batched launch sequence (see hg_batch): when
+ * max_queued are queued, when the oldest has waited max_wait_s (checked by
+ * hg_server_poll), before a request launched on its own, and when
+ * hg_server_poll blocks.  Defaults: enabled, 2^16 keys, 256 requests, 100 us.
+ * enabled = 0 launches every request on its own. */
+hg_status hg_server_set_batching(hg_server* server, int enabled, uint64_t small_max, uint32_t max_queued,
+                                 double max_wait_s);
+/* Batched launches so far and the requests they carried. */
+hg_status hg_server_batch_stats(const hg_server* server, uint64_t* batches, uint64_t* batched_requests);
 /* Waits for all work, frees every table and the server. */
 void hg_server_free(hg_server* server);
 

@@ -77,6 +77,8 @@ def lib():
         L.or_intersect_mt.argtypes = [_p, _u64, _p, _p, ctypes.c_int, _p, _u64, _p, _u64, ctypes.c_int]
         L.or_join_count_sorted.restype = _u64
         L.or_join_count_sorted.argtypes = [_p, _u64, _p, _u64, ctypes.c_int]
+        L.or_join_count_hashed.restype = _u64
+        L.or_join_count_hashed.argtypes = [_p, _u64, _p, _u64, ctypes.c_int, _u64, ctypes.c_int]
         L.or_max_threads.restype = ctypes.c_int
         L.or_max_threads.argtypes = []
         _lib = L
@@ -193,6 +195,22 @@ def join_count(a_keys: np.ndarray, b_keys: np.ndarray) -> int:
     a = np.sort(a_keys)
     b = np.sort(b_keys)
     return int(lib().or_join_count_sorted(_ptr(a), a.size, _ptr(b), b.size, a.dtype.itemsize))
+
+
+def join_count_hashed(a_keys: np.ndarray, b_keys: np.ndarray, max_distinct: int | None = None,
+                      threads: int = 0) -> int:
+    """sum over keys of multA(k) * multB(k) through a hash map of A's
+    distinct keys (linear time; for skewed sets of hundreds of millions)."""
+    a_keys = np.ascontiguousarray(a_keys)
+    b_keys = np.ascontiguousarray(b_keys)
+    if a_keys.dtype != b_keys.dtype:
+        raise TypeError("key dtype mismatch")
+    md = a_keys.size if max_distinct is None else int(max_distinct)
+    c = int(lib().or_join_count_hashed(_ptr(a_keys), a_keys.size, _ptr(b_keys), b_keys.size,
+                                       _kb(a_keys.dtype), md, int(threads)))
+    if c == (1 << 64) - 1:
+        raise MemoryError("join-count map could not be allocated or filled up")
+    return c
 
 
 def max_threads() -> int:

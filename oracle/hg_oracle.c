@@ -157,7 +157,9 @@ int or_zipf_cdf(uint64_t* cdf, uint64_t U, double s) {
 }
 
 void or_gen_zipf(void* out, uint64_t n, int kb, const uint64_t* cdf, uint64_t U, uint64_t seed) {
-  uint64_t salt = or_rand64(seed, 4, 0);
+  /* rank -> key depends on the universe only: sets drawn with different
+   * seeds share keys */
+  uint64_t salt = or_rand64(0x21BF, 4, U);
   #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < (int64_t)n; i++) {
     uint64_t u = or_rand64(seed, 3, (uint64_t)i);
@@ -277,12 +279,38 @@ int or_build_mt(const void* keys, uint64_t n, int kb, uint64_t B, uint32_t* offs
   return 0;
 }
 
-/* Canonical bucket order: ascending (key, idx).  Buckets are short, so an
- * insertion sort per bucket is enough for the sizes the tests check. */
+/* Canonical bucket order: ascending (key, idx).  Short buckets take an
+ * insertion sort; long ones (heavy duplicates, hot buckets) a qsort of
+ * (key, idx) records, so a bucket of millions of entries stays O(L log L). */
+typedef struct { uint64_t key; uint32_t idx; } or_rec;
+
+static int or_rec_cmp(const void* x, const void* y) {
+  const or_rec* a = (const or_rec*)x;
+  const or_rec* b = (const or_rec*)y;
+  if (a->key != b->key) return a->key < b->key ? -1 : 1;
+  return (a->idx > b->idx) - (a->idx < b->idx);
+}
+
 void or_canonicalize(const uint32_t* offsets, uint64_t B, void* keys, int kb, uint32_t* idx) {
   #pragma omp parallel for schedule(dynamic, 1024)
   for (int64_t b = 0; b < (int64_t)B; b++) {
     uint32_t s = offsets[b], e = offsets[b + 1];
+    if (e - s > 32) {
+      or_rec* r = (or_rec*)malloc((size_t)(e - s) * sizeof(or_rec));
+      if (r) {
+        for (uint32_t j = s; j < e; j++) {
+          r[j - s].key = load_key(keys, j, kb);
+          r[j - s].idx = idx ? idx[j] : 0;
+        }
+        qsort(r, e - s, sizeof(or_rec), or_rec_cmp);
+        for (uint32_t j = s; j < e; j++) {
+          store_key(keys, j, kb, r[j - s].key);
+          if (idx) idx[j] = r[j - s].idx;
+        }
+        free(r);
+        continue;
+      }
+    }
     for (uint32_t j = s + 1; j < e; j++) {
       uint64_t k = load_key(keys, j, kb);
       uint32_t x = idx ? idx[j] : 0;
@@ -379,6 +407,65 @@ uint64_t or_join_count_sorted(const void* a, uint64_t na, const void* b, uint64_
     total += ci * cj;
   }
   return total;
+}
+
+/* The same count, sum over keys of multA(k) * multB(k), through a hash map of
+ * A's distinct keys and their multiplicities (open addressing, CAS inserts);
+ * linear in na + nb, so it also checks heavily skewed inputs at full size,
+ * where probing every query's bucket costs the product of the multiplicities.
+ * Returns UINT64_MAX when the map cannot be allocated. */
+#define OR_EMPTY_SLOT 0xFFFFFFFFFFFFFFFFull
+uint64_t or_join_count_hashed(const void* a, uint64_t na, const void* b, uint64_t nb, int kb,
+                              uint64_t max_distinct, int threads) {
+  if (threads <= 0) threads = omp_get_max_threads();
+  uint64_t cap = 1024;
+  uint64_t want = max_distinct < na ? max_distinct : na;
+  while (cap < 2 * want) cap <<= 1;
+  uint64_t* slot_key = (uint64_t*)malloc((size_t)cap * sizeof(uint64_t));
+  uint64_t* slot_cnt = (uint64_t*)calloc((size_t)cap, sizeof(uint64_t));
+  if (!slot_key || !slot_cnt) { free(slot_key); free(slot_cnt); return UINT64_MAX; }
+  for (uint64_t i = 0; i < cap; i++) slot_key[i] = OR_EMPTY_SLOT;
+  uint64_t empty_key_count = 0, full = 0;  /* the key equal to the empty marker */
+  const uint64_t mask = cap - 1;
+  #pragma omp parallel for num_threads(threads) schedule(static) reduction(+ : empty_key_count)
+  for (int64_t i = 0; i < (int64_t)na; i++) {
+    uint64_t k = load_key(a, (uint64_t)i, kb);
+    if (k == OR_EMPTY_SLOT) { empty_key_count++; continue; }
+    uint64_t h = or_mix64(k) & mask, probes = 0;
+    for (;;) {
+      uint64_t cur = __atomic_load_n(&slot_key[h], __ATOMIC_ACQUIRE);
+      if (cur == k) { __atomic_fetch_add(&slot_cnt[h], 1, __ATOMIC_RELAXED); break; }
+      if (cur == OR_EMPTY_SLOT) {
+        uint64_t expect = OR_EMPTY_SLOT;
+        if (__atomic_compare_exchange_n(&slot_key[h], &expect, k, 0, __ATOMIC_ACQ_REL, __ATOMIC_ACQUIRE) ||
+            expect == k) {
+          __atomic_fetch_add(&slot_cnt[h], 1, __ATOMIC_RELAXED);
+          break;
+        }
+        continue;  /* another key took the slot: look at it again */
+      }
+      h = (h + 1) & mask;
+      if (++probes > cap) { __atomic_store_n(&full, 1, __ATOMIC_RELAXED); break; }
+    }
+  }
+  uint64_t total = 0;
+  if (!full) {
+    #pragma omp parallel for num_threads(threads) schedule(static) reduction(+ : total)
+    for (int64_t i = 0; i < (int64_t)nb; i++) {
+      uint64_t k = load_key(b, (uint64_t)i, kb);
+      if (k == OR_EMPTY_SLOT) { total += empty_key_count; continue; }
+      uint64_t h = or_mix64(k) & mask;
+      for (;;) {
+        uint64_t cur = slot_key[h];
+        if (cur == k) { total += slot_cnt[h]; break; }
+        if (cur == OR_EMPTY_SLOT) break;
+        h = (h + 1) & mask;
+      }
+    }
+  }
+  free(slot_key);
+  free(slot_cnt);
+  return full ? UINT64_MAX : total;
 }
 
 int or_max_threads(void) { return omp_get_max_threads(); }

@@ -70,6 +70,11 @@ uint64_t or_intersect_mt(const uint32_t* a_offsets, uint64_t n_buckets, const vo
  * restated as sort + merge-join). */
 uint64_t or_join_count_sorted(const void* a_sorted, uint64_t na, const void* b_sorted,
                               uint64_t nb, int key_bytes);
+/* The same count through a hash map of A's distinct keys (at most
+ * max_distinct of them): linear time for skewed inputs.  UINT64_MAX if the map
+ * cannot be allocated or fills. */
+uint64_t or_join_count_hashed(const void* a, uint64_t na, const void* b, uint64_t nb, int key_bytes,
+                              uint64_t max_distinct, int threads);
 int or_max_threads(void);
 
 #ifdef __cplusplus

@@ -8,13 +8,17 @@
 // sequence with CUDA events (as the reference's test main does) and dumps the
 // results so tests can compare them with the oracle and with this library.
 //
-// usage: ref_multi <keysA> <nA> <keysB|-> <nB> <tableSize> <outdir|-> [warmup]
+// usage: ref_multi <keysA> <nA> <keysB|-> <nB> <tableSize> <outdir|-> [warmup] [repeats]
 //   keys files hold raw hkey_t (int64, or uint32 when built with -DB32).
+//   With repeats > 1 the whole sequence (construct, build A, build B,
+//   intersect) runs that many times on the same inputs; one JSON line per run.
 //   Outputs in outdir: A_offsets.i64 (hashRange+1 int64), A_edges.kv
 //   (keyval records), common.i64, pairs.key (hkey_t per match, B's key).
 #include "MultiHashGraph.cuh"
 
+#include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -147,10 +151,15 @@ int main(int argc, char** argv) {
     std::vector<hkey_t> wb(b.begin(), b.begin() + std::min<size_t>(b.size(), 4096));
     run(wa, wb, std::min<index_t>(tableSize, 4096), "-");
   }
-  RunTimes t = run(a, b, tableSize, argv[6]);
-  std::printf("{\"n_a\": %lld, \"n_b\": %lld, \"table_size\": %lld, \"build_a_s\": %.9f, "
-              "\"build_b_s\": %.9f, \"intersect_s\": %.9f, \"total_s\": %.9f}\n",
-              (long long)nA, (long long)nB, (long long)tableSize, t.build_a_ms / 1e3,
-              t.build_b_ms / 1e3, t.intersect_ms / 1e3, t.total_ms / 1e3);
+  const int repeats = argc > 8 ? std::max(1, std::atoi(argv[8])) : 1;
+  for (int r = 0; r < repeats; r++) {
+    // results are dumped from the last run only
+    RunTimes t = run(a, b, tableSize, r + 1 == repeats ? argv[6] : "-");
+    std::printf("{\"n_a\": %lld, \"n_b\": %lld, \"table_size\": %lld, \"run\": %d, \"build_a_s\": %.9f, "
+                "\"build_b_s\": %.9f, \"intersect_s\": %.9f, \"total_s\": %.9f}\n",
+                (long long)nA, (long long)nB, (long long)tableSize, r, t.build_a_ms / 1e3,
+                t.build_b_ms / 1e3, t.intersect_ms / 1e3, t.total_ms / 1e3);
+    std::fflush(stdout);
+  }
   return 0;
 }

@@ -67,7 +67,8 @@ def canonical_csr(offsets, keys):
 def part_hash(out):
     single, multi = oracle.ref_binary("ref_hash_single"), oracle.ref_binary("ref_hash_multi")
     if not single or not multi:
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+        ref_root = os.environ.get("REF_ROOT", "/root/reference")
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF_ROOT={ref_root}"], check=True)
         single, multi = oracle.ref_binary("ref_hash_single"), oracle.ref_binary("ref_hash_multi")
     edge = np.array([0, 1, 2, 42, 0xFFFFFFFF, 1 << 32, (1 << 32) + 5, 0xFFFFFFFFFFFFFFFF,
                      0x8000000000000000, 0x7FFFFFFF, 0x80000000, 0xDEADBEEFCAFEBABE], dtype=np.uint64)

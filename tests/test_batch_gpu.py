@@ -272,3 +272,57 @@ def test_batch_autotune(hg):
     assert hg.device_error() == 0
     for i in range(len(keys)):
         _check_pair(hg, b, i, keys[i], queries[i], buckets[i], wi[i], 8)
+
+
+@pytest.mark.parametrize("kb", [4, 8])
+def test_batch_probe_only_and_build_only_pairs(hg, kb):
+    """Probe-only pairs (d_keys NULL: the table was built before, by plain
+    calls, or by a build-only pair of the same batch) and build-only pairs
+    (nq = 0, no count): tables and pairs equal the oracle's."""
+    import ctypes
+
+    import torch
+    from hashgraph_b200._capi import BatchPair
+    L = hg.lib()
+    P = ctypes.c_void_p
+    s = P(torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(31 + kb)
+    sizes = [int(2 ** rng.uniform(4, 17)) for _ in range(24)] + [1 << 15, 1 << 16]
+    keys = [oracle.gen_uniform(n, kb, 700 + i) for i, n in enumerate(sizes)]
+    queries = [oracle.gen_overlap(n, keys[i], 0.5, 800 + i) for i, n in enumerate(sizes)]
+    dk = [from_np_u(a) for a in keys]
+    dq = [from_np_u(q) for q in queries]
+    kdt = torch.int32 if kb == 4 else torch.int64
+    offs = [torch.empty(n + 1, dtype=torch.int32, device="cuda") for n in sizes]
+    tkeys = [torch.empty(n, dtype=kdt, device="cuda") for n in sizes]
+    tidx = [torch.empty(n, dtype=torch.int32, device="cuda") for n in sizes]
+    counts = torch.zeros(len(sizes), dtype=torch.int64, device="cuda")
+    pairs = [torch.empty((n, 2), dtype=torch.int32, device="cuda") for n in sizes]
+    # even pairs: built beforehand by plain calls; odd pairs: built by a
+    # build-only pair of the batch
+    for i in range(0, len(sizes), 2):
+        t = hg.Table.build(dk[i], sizes[i], with_index=True)
+        offs[i].copy_(t.offsets)
+        tkeys[i].copy_(t.view_keys())
+        tidx[i].copy_(t.view_idx())
+    desc = []
+    for i, n in enumerate(sizes):
+        if i % 2:  # build-only
+            desc.append(BatchPair(P(dk[i].data_ptr()), n, n, None, 0, P(offs[i].data_ptr()), P(tkeys[i].data_ptr()),
+                                  P(tidx[i].data_ptr()), None, 0, None))
+    for i, n in enumerate(sizes):  # probe-only
+        desc.append(BatchPair(None, n, n, P(dq[i].data_ptr()), n, P(offs[i].data_ptr()), P(tkeys[i].data_ptr()),
+                              P(tidx[i].data_ptr()), P(pairs[i].data_ptr()), n, P(counts.data_ptr() + 8 * i)))
+    arr = (BatchPair * len(desc))(*desc)
+    for _ in range(2):  # a batch can be run again
+        b = ctypes.c_void_p()
+        assert L.hg_batch_create(arr, len(desc), kb, s, ctypes.byref(b)) == 0
+        assert L.hg_batch_run(b, s) == 0
+        L.hg_batch_free(b, s)
+        torch.cuda.synchronize()
+        assert hg.device_error() == 0
+        for i, n in enumerate(sizes):
+            off, k, idx, c, op = _oracle_pair(keys[i], queries[i], n, True)
+            np.testing.assert_array_equal(to_np_u(offs[i], 4), off)
+            assert int(counts[i].item()) == c
+            np.testing.assert_array_equal(_sorted_pairs(to_np_u(pairs[i][:c], 4)), _sorted_pairs(op))

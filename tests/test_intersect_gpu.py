@@ -201,6 +201,34 @@ def test_intersect_zipf_count(hg, probe_path):
     assert hg.device_error() == 0
 
 
+@pytest.mark.parametrize("probe_path", [0, 1, 2])
+@pytest.mark.parametrize("kb", [4, 8])
+def test_intersect_count_heavy_keys(hg, probe_path, kb):
+    """Count only, head keys with tens of thousands of copies in A (buckets
+    far above the heavy-key threshold): the heavy keys take their count from
+    the set, the rest of the long buckets are scanned by whole warps."""
+    cdf = oracle.zipf_cdf(1 << 10, 1.1)
+    a = oracle.gen_zipf(1 << 18, kb, cdf, 61)
+    q = oracle.gen_zipf(1 << 17, kb, cdf, 62)
+    t = hg.Table.build(from_np_u(a), 1 << 18, with_index=False)
+    count, _ = t.intersect(from_np_u(q), emit=False, path=probe_path)
+    assert int(count.item()) == oracle.join_count(a, q)
+    assert hg.device_error() == 0
+
+
+@pytest.mark.parametrize("n_buckets", [1, 64])
+def test_intersect_count_many_long_buckets(hg, n_buckets):
+    """Every bucket long, with far more distinct keys in them than the
+    heavy-key set holds (keys that find no slot are scanned by their warp):
+    the count stays exact."""
+    a = (oracle.gen_uniform(1 << 20, 8, 63) % np.uint64(1 << 16)).astype(np.uint64)
+    q = (oracle.gen_uniform(1 << 15, 8, 64) % np.uint64(1 << 17)).astype(np.uint64)
+    t = hg.Table.build(from_np_u(a), n_buckets, with_index=False)
+    count, _ = t.intersect(from_np_u(q), emit=False, path=0)
+    assert int(count.item()) == oracle.join_count(a, q)
+    assert hg.device_error() == 0
+
+
 @pytest.mark.parametrize("probe_path", [1, 2])
 def test_intersect_one_query_key_overflows(hg, probe_path):
     """Every query is the same key: its bucket range gets all the queries,

@@ -61,3 +61,72 @@ def test_damaged_files_are_refused(hg, tmp_path):
     with pytest.raises(hg.HGError):
         hg.Table.load(tmp_path / "magic.hgt")
     assert hg.device_error() == 0
+
+
+def _fnv1a64(data: bytes) -> int:
+    """FNV-1a 64 of `data` (the file checksum), byte by byte: the files here
+    are kept small."""
+    h = 0xcbf29ce484222325
+    for b in data:
+        h ^= b
+        h = (h * 0x100000001b3) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def _rewrite_with_checksum(raw: bytearray) -> bytearray:
+    import struct
+    out = bytearray(raw)
+    out[40:48] = struct.pack("<Q", _fnv1a64(bytes(out[64:])))
+    return out
+
+
+def test_forged_offsets_are_refused(hg, tmp_path):
+    """Offsets that decrease or pass n are refused even when the file's
+    checksum was recomputed (a crafted or hand-edited file): the probes read
+    each bucket's keys straight from the offsets."""
+    import struct
+    n, B = 2000, 1000
+    a = oracle.gen_uniform(n, 4, 21)
+    t = hg.Table.build(from_np_u(a), B, with_index=False)
+    path = tmp_path / "t.hgt"
+    t.save(path)
+    raw = bytearray(open(path, "rb").read())
+    assert _rewrite_with_checksum(raw) == raw  # the checksum restated here matches the library's
+    off0 = 64
+    # a decreasing pair of offsets in the middle
+    bad = bytearray(raw)
+    v = struct.unpack_from("<I", bad, off0 + 4 * 500)[0]
+    struct.pack_into("<I", bad, off0 + 4 * 500, v + 50)
+    open(tmp_path / "dec.hgt", "wb").write(_rewrite_with_checksum(bad))
+    with pytest.raises(hg.HGError) as e:
+        hg.Table.load(tmp_path / "dec.hgt")
+    assert e.value.status == -1
+    assert b"offsets decrease" in hg.lib().hg_last_error()
+    # an offset beyond n
+    bad = bytearray(raw)
+    struct.pack_into("<I", bad, off0 + 4 * 999, n + 7)
+    open(tmp_path / "big.hgt", "wb").write(_rewrite_with_checksum(bad))
+    with pytest.raises(hg.HGError):
+        hg.Table.load(tmp_path / "big.hgt")
+    assert hg.device_error() == 0
+
+
+def test_index_requested_from_a_file_without_one_is_refused(hg, tmp_path):
+    import ctypes
+
+    import torch
+    a = oracle.gen_uniform(1000, 8, 22)
+    t = hg.Table.build(from_np_u(a), 512, with_index=False)
+    path = tmp_path / "t.hgt"
+    t.save(path)
+    off = torch.empty(513, dtype=torch.int32, device="cuda")
+    keys = torch.empty(1000, dtype=torch.int64, device="cuda")
+    idx = torch.empty(1000, dtype=torch.int32, device="cuda")
+    P = ctypes.c_void_p
+    s = P(torch.cuda.current_stream().cuda_stream)
+    L = hg.lib()
+    assert L.hg_table_load_arrays(str(path).encode(), P(off.data_ptr()), P(keys.data_ptr()), P(idx.data_ptr()),
+                                  1000, 512, 8, s) == -1
+    assert L.hg_table_load_arrays(str(path).encode(), P(off.data_ptr()), P(keys.data_ptr()), None,
+                                  1000, 512, 8, s) == 0
+    np.testing.assert_array_equal(to_np_u(off, 4), to_np_u(t.offsets, 4))

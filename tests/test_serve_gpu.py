@@ -73,3 +73,84 @@ def test_missed_and_replaced_tables(hg):
     assert r2.count == oracle.join_count(a, b)
     assert srv.stats()["resident_tables"] == 1
     srv.free()
+
+
+def _served_specs(n_req, seed):
+    """Builds of table ids 0..15 (ids reused, so tables get replaced) and
+    intersects against them, sizes 2^U(6,14); slices of one key arena."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    specs, built = [], {}
+    for k in range(n_req):
+        size = int(2 ** rng.uniform(6, 14))
+        if k < 8 or rng.uniform() < 0.35:
+            tid = int(rng.integers(0, 16))
+            off = int(rng.integers(0, (1 << 20) - size))
+            built[tid] = (off, size)
+            specs.append(("build", tid, off, size))
+        else:
+            tid = int(rng.choice(sorted(built)))
+            toff, tn = built[tid]
+            off = min(toff + tn // 2, (1 << 20) - size)
+            specs.append(("intersect", tid, off, size))
+    return specs
+
+
+def test_served_pairs_equal_oracle_and_alone(hg):
+    """Saturated load: every request submitted at once, so the engine
+    coalesces them into batched launches (continuous batching).  Each served
+    intersect's count and sorted (index, query) pairs equal the oracle's on
+    the table resident when the request was submitted, and the same request
+    served alone (no batching, one request at a time) gives the same pairs."""
+    import numpy as np
+    import torch
+
+    import oracle
+    from hashgraph_b200.serve import Request, Server, now
+    from tests.conftest import to_np_u
+    arena_h = oracle.gen_uniform(1 << 20, 8, 19)
+    arena = torch.from_numpy(arena_h.view(np.int64)).cuda()
+    specs = _served_specs(300, 23)
+
+    def make(sp, t):
+        kind, tid, off, size = sp
+        sl = arena[off:off + size]
+        if kind == "build":
+            return Request("build", tid, t, keys=sl, n_buckets=size, with_index=True)
+        return Request("intersect", tid, t, queries=sl, pair_cap=size,
+                       pairs=torch.full((size, 2), -1, dtype=torch.int32, device="cuda"))
+
+    torch.cuda.synchronize()
+    server = Server(budget_bytes=1 << 30, max_tables=64, n_streams=4, max_keys=1 << 15, batch_max=64)
+    t0 = now()
+    reqs = [make(sp, t0) for sp in specs]
+    for r in reqs:
+        server.submit(r)
+    server.drain()
+    st = server.stats()
+    assert st["batches"] >= len(specs) // 64 and st["batched_requests"] == len(specs)
+    alone = Server(budget_bytes=1 << 30, max_tables=64, n_streams=1, max_keys=1 << 15, batching=False)
+    tables = {}
+    checked = 0
+    for sp, r in zip(specs, reqs):
+        kind, tid, off, size = sp
+        q = make(sp, now())
+        alone.submit(q)
+        alone.drain()
+        if kind == "build":
+            tables[tid] = oracle.build(arena_h[off:off + size], size, True)
+            continue
+        o_off, o_keys, o_idx = tables[tid]
+        oc, op = oracle.intersect(o_off, o_keys, o_idx, arena_h[off:off + size], pair_cap=size)
+        assert not r.missed and r.count == oc == q.count
+        got = to_np_u(r.pairs[:oc], 4).astype(np.uint64)
+        solo = to_np_u(q.pairs[:oc], 4).astype(np.uint64)
+        exp = op.astype(np.uint64)
+        key = lambda p: np.sort(p[:, 0] << 32 | p[:, 1])  # noqa: E731
+        np.testing.assert_array_equal(key(got), key(exp))
+        np.testing.assert_array_equal(key(solo), key(exp))
+        checked += 1
+    assert checked > 100
+    server.free()
+    alone.free()
+    assert hg.device_error() == 0

@@ -476,7 +476,8 @@ def reference_gpu(workload, n, our_value, repeats=3):
     return {"impl": "reference MultiHashGraph (gpuCount 1, sm_100a, unmodified sources; oracle/_ref)",
             "workload": "same seeded inputs as our arm; the reference builds both sets into tables "
                         "(its intersect joins two tables) and emits the matched keys",
-            "runs": len(runs), "first_run": summary(first), "best_run": b,
+            "runs": len(runs), "composite_ms_per_run": [x["total_s"] * 1e3 for x in runs],
+            "first_run": summary(first), "best_run": b,
             "ours_over_reference_build_a_plus_intersect": (our_value / b["build_a_plus_intersect_keys_per_s"]
                                                            if b["build_a_plus_intersect_keys_per_s"] else None),
             "ours_over_reference_composite": (our_value / b["composite_keys_per_s"]
@@ -713,7 +714,7 @@ def run_serving(args, rank, world, local):
     import torch
 
     import hashgraph_b200 as hg
-    from hashgraph_b200.serve import Request, Server, latency_summary, run_open_loop
+    from hashgraph_b200.serve import Request, Server, latency_summary, now, run_open_loop
 
     dev = torch.device("cuda", local)
     arena_keys = 1 << 27
@@ -752,7 +753,50 @@ def run_serving(args, rank, world, local):
     # each intersect's count against a serial run of the same request list
     st = server.stats()
     server.free()
-    serial = Server(budget_bytes=1 << 50, max_tables=1 << 30, n_streams=1, max_keys=1 << 24, device=dev)
+
+    # saturated: every request submitted at once, served (1) with continuous
+    # batching, (2) one launch per request on the same streams, (3) as plain
+    # calls, one build or intersect call after another on one stream; the
+    # counts (and misses) must be identical.  Once on the request mix above,
+    # once on small requests only (2^U(10,16) keys), where launches dominate.
+    def saturated_run(sp_list):
+        out, counts = {}, {}
+        total = sum(sp[4] for sp in sp_list)
+        for mode, kw in (("batched", dict(batching=True, n_streams=args.streams)),
+                         ("one_launch_per_request", dict(batching=False, n_streams=args.streams)),
+                         ("plain_calls", dict(batching=False, n_streams=1))):
+            srv = Server(budget_bytes=120 << 30, max_tables=512, max_keys=1 << 24, device=dev, **kw)
+            srv.reserve(RESERVE_BYTES)
+            for lg in range(10, 25, 2):
+                srv.submit(Request("build", -1, 0.0, keys=arena[: 1 << lg], n_buckets=1 << lg))
+                srv.submit(Request("intersect", -1, 0.0, queries=arena[: 1 << lg], pair_cap=1 << lg))
+                srv.drain()
+            torch.cuda.synchronize(dev)
+            rq = [make(sp) for sp in sp_list]
+            t0 = now()
+            for r in rq:
+                r.arrival = t0
+                srv.submit(r)
+            srv.drain()
+            span = now() - t0
+            bst = srv.stats()
+            srv.free()
+            counts[mode] = [(r.count, r.missed) for r in rq if r.kind == "intersect"]
+            out[mode] = {"makespan_ms": span * 1e3, "keys_per_s": total / span, "requests_per_s": len(rq) / span,
+                         "batches": bst["batches"], "batched_requests": bst["batched_requests"]}
+        if not (counts["batched"] == counts["one_launch_per_request"] == counts["plain_calls"]):
+            raise RuntimeError("saturated runs disagree on the intersect counts")
+        out["identical_counts"] = True
+        out["batched_over_plain_calls"] = out["batched"]["keys_per_s"] / out["plain_calls"]["keys_per_s"]
+        out["batched_over_one_launch_per_request"] = (out["batched"]["keys_per_s"] /
+                                                      out["one_launch_per_request"]["keys_per_s"])
+        return out
+
+    saturated = {"mix": saturated_run(specs),
+                 "small_requests": saturated_run(serving_requests(args.requests, args.rate, arena_keys, lo_log2=10,
+                                                                  hi_log2=16, seed=7))}
+    serial = Server(budget_bytes=1 << 50, max_tables=1 << 30, n_streams=1, max_keys=1 << 24, device=dev,
+                    batching=False)
     mismatches, checked = 0, 0
     for sp, r in zip(specs, reqs):
         q = make(sp)
@@ -770,12 +814,15 @@ def run_serving(args, rank, world, local):
         "dtype": "u64", "data": "synthetic (seeded splitmix64 key arena on the device; requests take slices)",
         "config": {"workload": f"serving: {args.requests} requests, Poisson arrivals at {args.rate}/s, 30% build / "
                                f"70% intersect, sizes 2^U(10,24) u64, <= 512 resident tables, 120 GB budget "
-                               f"({RESERVE_BYTES >> 30} GB reserved), LRU, {args.streams} streams",
+                               f"({RESERVE_BYTES >> 30} GB reserved), LRU, {args.streams} streams, continuous "
+                               f"batching of requests up to 2^16 keys",
                    "requests": args.requests, "rate_per_s": args.rate, "keys_total": keys_total,
                    "offered_keys_per_s": keys_total / (specs[-1][2] - specs[0][2]) if len(specs) > 1 else None,
                    "parallelism": "single GPU"},
         "latency": by_kind, "latency_all": latency_summary(done), "missed_intersects": missed,
         "evictions": st["evictions"], "serial_check": {"intersects_checked": checked, "mismatches": 0},
+        "batching": {"batches": st["batches"], "batched_requests": st["batched_requests"]},
+        "saturated": saturated,
         "clocks": clk, "e2e": None, "gpu_launches": launches, "cpu_baseline": None,
         "note": "native serving engine (hg_server_*); value = keys of all requests / makespan (first arrival "
                 "to last completion); latency = arrival to device completion of the request's last kernel",

@@ -564,7 +564,7 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(Src src, uint32_t max_p
 template <typename KeyT, bool WITH_IDX, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys, const uint32_t* __restrict__ pidx,
                                                  const uint32_t* __restrict__ pstart, uint32_t n_parts, uint64_t cap1,
-                                                 uint32_t tiles_per_part, BucketMap bm, uint32_t fine_log2,
+                                                 Div32 tpp, BucketMap bm, uint32_t fine_log2,
                                                  uint32_t split_log2, uint64_t capf, uint32_t* __restrict__ fcount,
                                                  KeyT* __restrict__ fkeys, uint32_t* __restrict__ fidx,
                                                  uint32_t* flags) {
@@ -587,12 +587,13 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
   __shared__ uint32_t s_next_cnt;
   __shared__ uint32_t s_wsum[BLOCK / 32];
   const uint32_t coarse_log2 = fine_log2 + split_log2;
-  const uint64_t vtiles = uint64_t(n_parts) * tiles_per_part;
+  const uint32_t tiles_per_part = tpp.d;
+  const uint64_t vtiles = uint64_t(n_parts) * tiles_per_part;  // below 2^32 (the planner keeps it so)
   // first valid virtual tile at or after vt (stepping by the grid); vtiles if none
   auto next_valid = [&](uint64_t vt, uint32_t* cnt) -> uint64_t {
     for (; vt < vtiles; vt += gridDim.x) {
-      const uint64_t q = vt / tiles_per_part;
-      const uint32_t r0 = static_cast<uint32_t>(vt % tiles_per_part) * TILE;
+      const uint32_t q = tpp.div(static_cast<uint32_t>(vt));
+      const uint32_t r0 = (static_cast<uint32_t>(vt) - q * tiles_per_part) * TILE;
       const uint32_t m = sps[q + 1] - sps[q];
       if (r0 < m) {
         *cnt = min(TILE, m - r0);
@@ -603,8 +604,8 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
     return vtiles;
   };
   auto issue = [&](uint64_t vt, uint32_t cnt, uint32_t buf) {
-    const uint64_t q = vt / tiles_per_part;
-    const uint64_t r0 = (vt % tiles_per_part) * TILE;
+    const uint64_t q = tpp.div(static_cast<uint32_t>(vt));
+    const uint64_t r0 = uint64_t(static_cast<uint32_t>(vt) - static_cast<uint32_t>(q) * tiles_per_part) * TILE;
     const uint32_t bk = (cnt * uint32_t(sizeof(KeyT)) + 15u) & ~15u;  // stays inside the partition's slots
     const uint32_t bi = WITH_IDX ? ((cnt * 4u + 15u) & ~15u) : 0u;
     mbar_arrive_expect_tx(&bar[buf], bk + bi);
@@ -640,7 +641,7 @@ __global__ void __launch_bounds__(BLOCK) k_split(const KeyT* __restrict__ pkeys,
       s_next = nx;
       s_next_cnt = cn;
     }
-    const uint64_t q = vt / tiles_per_part;
+    const uint64_t q = tpp.div(static_cast<uint32_t>(vt));
     const uint64_t b0 = q << coarse_log2;
     KeyT* ck = rk + buf * TILE;
     uint32_t* ci = ri + buf * TILE;
@@ -1228,7 +1229,7 @@ static hg_status run_partition_passes(const PartGeometry& g, uint64_t n, const K
     Phase ph(s, who[0] == 'b' ? "split" : "probe_split");
     count_launch();
     k_split<KeyT, WI, SPLIT_BLOCK><<<std::max(grid, 1u), SPLIT_BLOCK, g.smem2, s>>>(
-        pkeys, pidx, pcount, static_cast<uint32_t>(g.n_parts), g.part_cap, tiles_per_part, bm, g.fine_log2,
+        pkeys, pidx, pcount, static_cast<uint32_t>(g.n_parts), g.part_cap, Div32::make(tiles_per_part), bm, g.fine_log2,
         g.split_log2, g.fine_cap, fcount, fkeys, fidx, flags);
     HG_CUDA(cudaPeekAtLastError(), "split launch");
   }

@@ -177,6 +177,24 @@ __device__ __forceinline__ void warp_aggregated_count(CtrT* ctr, uint32_t slot, 
     atomicAdd(ctr + slot, static_cast<CtrT>(__popc(peers)));
 }
 
+// Quotient of 32-bit v by a fixed 32-bit divisor d >= 1 without a division
+// instruction sequence: q = mulhi64(M, v) with M = floor((2^64 - 1) / d) + 1,
+// exact for every 32-bit v (Lemire, Kaser, Kurz, "Faster remainder by direct
+// computation", 2019, with 64-bit M for 32-bit operands); d = 1 is v itself.
+struct Div32 {
+  uint64_t magic = 0;
+  uint32_t d = 1;
+  static Div32 make(uint32_t d) {
+    Div32 x;
+    x.d = d ? d : 1;
+    x.magic = x.d > 1 ? ~0ull / x.d + 1 : 0;
+    return x;
+  }
+  __device__ __forceinline__ uint32_t div(uint32_t v) const {
+    return d > 1 ? static_cast<uint32_t>(__umul64hi(magic, v)) : v;
+  }
+};
+
 // Streaming loads for data touched once.
 template <typename T>
 __device__ __forceinline__ T ld_stream(const T* p) { return __ldcs(p); }

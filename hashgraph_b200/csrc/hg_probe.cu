@@ -698,7 +698,7 @@ constexpr int CPROBE_BLOCK = 256;  // 512 and 1024 measured slower (3.50, 3.75 a
 template <typename KeyT, bool EMIT, bool A_IDX, int QPT>
 __global__ void __launch_bounds__(CPROBE_BLOCK)
     k_coarse_probe(const KeyT* __restrict__ pkeys, const uint32_t* __restrict__ pidx,
-                   const uint32_t* __restrict__ pcount, uint32_t n_parts, uint64_t part_cap, uint32_t tiles_per_part,
+                   const uint32_t* __restrict__ pcount, uint32_t n_parts, uint64_t part_cap, Div32 tpp,
                    const uint32_t* __restrict__ a_off, const KeyT* __restrict__ a_keys,
                    const uint32_t* __restrict__ a_idx, BucketMap bm, uint32_t* __restrict__ pairs, uint64_t pair_cap,
                    unsigned long long* d_count, unsigned* ticket, const uint32_t* flags) {
@@ -707,7 +707,8 @@ __global__ void __launch_bounds__(CPROBE_BLOCK)
   constexpr uint32_t TILE = uint32_t(CPROBE_BLOCK) * QPT;
   __shared__ uint64_t red[NW + 1];
   __shared__ unsigned s_vt[2];
-  const uint64_t vtiles = uint64_t(n_parts) * tiles_per_part;
+  const uint32_t tiles_per_part = tpp.d;
+  const uint64_t vtiles = uint64_t(n_parts) * tiles_per_part;  // below 2^32 (the planner keeps it so)
   const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
   auto a_ref = [&](uint32_t x) -> uint32_t {
     if constexpr (A_IDX) return a_idx[x];
@@ -723,8 +724,9 @@ __global__ void __launch_bounds__(CPROBE_BLOCK)
     const uint64_t vt = s_vt[it & 1];
     if (vt >= vtiles) break;
     if (threadIdx.x == 0) s_vt[(it + 1) & 1] = atomicAdd(ticket, 1u);
-    const uint64_t part = vt / tiles_per_part;
-    const uint32_t r0 = static_cast<uint32_t>(vt % tiles_per_part) * TILE;
+    const uint32_t part32 = tpp.div(static_cast<uint32_t>(vt));
+    const uint64_t part = part32;
+    const uint32_t r0 = (static_cast<uint32_t>(vt) - part32 * tiles_per_part) * TILE;
     const uint32_t m = pcount[part];
     if (r0 >= m) {  // the same for the whole CTA
       __syncthreads();
@@ -1098,7 +1100,7 @@ static hg_status run_probe_coarse(const ProbePlan& p, const uint32_t* a_off, con
       Phase ph(s, EMIT ? "coarse_probe_emit" : "coarse_probe_count");
       count_launch();
       kern<<<std::max(grid, 1u), block, 0, s>>>(pkeys, pidx, pcount, static_cast<uint32_t>(g.n_parts),
-                                                       g.part_cap, tiles_per_part, a_off, a_keys, a_idx, bm, pairs,
+                                                       g.part_cap, Div32::make(tiles_per_part), a_off, a_keys, a_idx, bm, pairs,
                                                        cap, d_count, ticket + 3, flags);
       const cudaError_t e = cudaPeekAtLastError();
       if (e != cudaSuccess) st = cuda_fail(e, "coarse-probe launch");

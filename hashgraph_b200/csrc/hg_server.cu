@@ -81,6 +81,7 @@ struct QueuedReq {
 };
 
 constexpr size_t STAGE_BYTES = size_t(4) << 20;  // pinned descriptor buffer of one batch
+constexpr size_t BATCH_MIN_REQUESTS = 4;          // smaller segments are launched request by request
 constexpr int STAGE_RING = 8;
 
 static double monotonic_s() {
@@ -107,6 +108,7 @@ struct hg_server {
   uint32_t n_slots = 0, next_slot = 0;
   std::vector<uint8_t> slot_busy;
   std::vector<cudaEvent_t> free_events;
+  std::unordered_map<cudaEvent_t, uint32_t> event_refs;  // requests sharing one completion event (a batch)
   cudaMemPool_t pool = nullptr;
   cudaStream_t clock_stream = nullptr;  // carries only `ref`, so `ref` completes at once
   cudaEvent_t ref = nullptr;
@@ -201,6 +203,26 @@ static hg_status reserve_slot(hg_server* s, uint32_t* slot) {
   return lib_fail(HG_ERR_TOO_LARGE, "hg_server: 65536 intersects in flight; poll before submitting more");
 }
 
+// `count` contiguous count slots (one copy brings a batch's counts back), or
+// HG_ERR_TOO_LARGE when no such run is free.
+static hg_status reserve_slot_run(hg_server* s, uint32_t count, uint32_t* first) {
+  if (count == 0 || count > s->n_slots) return HG_ERR_TOO_LARGE;
+  uint32_t start = s->next_slot + count <= s->n_slots ? s->next_slot : 0;
+  for (uint32_t tries = 0; tries < s->n_slots; tries++) {
+    uint32_t k = 0;
+    while (k < count && !s->slot_busy[start + k]) k++;
+    if (k == count) {
+      for (uint32_t j = 0; j < count; j++) s->slot_busy[start + j] = 1;
+      *first = start;
+      s->next_slot = (start + count) % s->n_slots;
+      return HG_OK;
+    }
+    start = start + k + 1;
+    if (start + count > s->n_slots) start = 0;
+  }
+  return lib_fail(HG_ERR_TOO_LARGE, "hg_server: no free run of count slots; poll before submitting more");
+}
+
 // The latency clock: a request's completion is its event's time after `ref`
 // (a float count of milliseconds) added to ref_host, the host time of `ref`.
 // The GPU's event timer and the host clock drift apart by tens of
@@ -218,10 +240,101 @@ static cudaError_t rebase_clock(hg_server* s) {
   return e;
 }
 
+// One request launched on its own (a library call on the least busy stream).
+static hg_status direct_build(hg_server* s, const QueuedReq& r, const std::vector<uint64_t>* pinned) {
+  const size_t bytes = (r.n_buckets + 1) * 4 + r.n * (s->key_bytes + (r.with_index ? 4 : 0));
+  if (s->tables.count(r.table_id)) evict(s, r.table_id);  // replaced
+  make_room(s, bytes, pinned);
+  const int si = pick_stream(s, 20e-6 + double(r.n) * 4e-11);
+  cudaStream_t st = s->streams[si];
+  ServerTable t;
+  t.n = r.n;
+  t.n_buckets = r.n_buckets;
+  t.with_index = r.with_index != 0;
+  t.bytes = bytes;
+  t.stream = si;
+  cudaError_t e = cudaMallocFromPoolAsync(&t.offsets, (r.n_buckets + 1) * 4, s->pool, st);
+  if (e == cudaSuccess && r.n) e = cudaMallocFromPoolAsync(&t.keys, r.n * s->key_bytes, s->pool, st);
+  if (e == cudaSuccess && r.n && r.with_index)
+    e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&t.idx), r.n * 4, s->pool, st);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t.ready, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (t.offsets) cudaFreeAsync(t.offsets, st);
+    if (t.keys) cudaFreeAsync(t.keys, st);
+    if (t.idx) cudaFreeAsync(t.idx, st);
+    return cuda_fail(e, "hg_server_build: table allocation");
+  }
+  hg_status hs = hg_build_into(r.data, r.n, s->key_bytes, r.n_buckets, t.offsets, t.keys, t.idx,
+                               s->ws[si], s->ws_bytes, reinterpret_cast<hg_stream_t>(st));
+  if (hs != HG_OK) {
+    cudaFreeAsync(t.offsets, st);
+    if (t.keys) cudaFreeAsync(t.keys, st);
+    if (t.idx) cudaFreeAsync(t.idx, st);
+    cudaEventDestroy(t.ready);
+    return hs;
+  }
+  cudaEventRecord(t.ready, st);
+  s->lru.push_back(r.table_id);
+  t.lru = std::prev(s->lru.end());
+  s->bytes += bytes;
+  s->tables.emplace(r.table_id, t);
+  ServerReq q{r.ticket, 0, 0, r.arrival, take_event(s), 0};
+  cudaEventRecord(q.done, st);
+  s->inflight.push_back(q);
+  return HG_OK;
+}
+
+static hg_status direct_intersect(hg_server* s, const QueuedReq& r) {
+  uint32_t slot = 0;
+  hg_status hs = reserve_slot(s, &slot);
+  if (hs != HG_OK) return hs;
+  auto it = s->tables.find(r.table_id);
+  const int si = pick_stream(s, 20e-6 + double(r.n) * 4e-11);
+  cudaStream_t st = s->streams[si];
+  ServerReq q{r.ticket, 1, 0, r.arrival, take_event(s), slot};
+  if (it == s->tables.end()) {
+    q.missed = 1;
+  } else {
+    ServerTable& t = it->second;
+    s->lru.splice(s->lru.end(), s->lru, t.lru);  // most recently used
+    cudaStreamWaitEvent(st, t.ready, 0);
+    uint32_t* pairs = r.d_pairs ? r.d_pairs : s->pair_buf[si];
+    const uint64_t cap = r.d_pairs ? r.pair_cap : std::min<uint64_t>(r.pair_cap, s->max_keys);
+    hs = hg_intersect_into(t.offsets, t.keys, t.idx, t.n, t.n_buckets, s->key_bytes, r.data, r.n, nullptr, pairs,
+                           cap, s->d_counts + slot, s->ws[si], s->ws_bytes, reinterpret_cast<hg_stream_t>(st));
+    if (hs != HG_OK) {
+      s->free_events.push_back(q.done);
+      s->slot_busy[slot] = 0;
+      return hs;
+    }
+    cudaMemcpyAsync(s->h_counts + slot, s->d_counts + slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+  }
+  cudaEventRecord(q.done, st);
+  s->inflight.push_back(q);
+  return HG_OK;
+}
+
+// True when a queued request names `table_id`.
+static bool queue_touches(const hg_server* s, uint64_t table_id) {
+  for (const QueuedReq& q : s->queue)
+    if (q.table_id == table_id) return true;
+  return false;
+}
+
 // Launches one segment of the queue (builds, then intersects) as one batch.
 static hg_status launch_segment(hg_server* s, const QueuedReq* q, size_t n) {
   uint64_t keys = 0;
-  for (size_t i = 0; i < n; i++) keys += q[i].n;
+  uint32_t isects = 0;
+  for (size_t i = 0; i < n; i++) {
+    keys += q[i].n;
+    isects += q[i].kind == 1;
+  }
+  uint32_t slot0 = 0, n_isect = 0;  // the segment's intersects count into slots [slot0, slot0 + isects)
+  if (isects) {
+    hg_status hs = reserve_slot_run(s, isects, &slot0);
+    if (hs != HG_OK) return hs;
+  }
   const int si = pick_stream(s, 20e-6 + double(keys) * 4e-11);
   cudaStream_t st = s->streams[si];
   std::vector<hg_batch_pair> pairs;
@@ -262,9 +375,7 @@ static hg_status launch_segment(hg_server* s, const QueuedReq* q, size_t n) {
       pairs.push_back(hg_batch_pair{r.data, r.n, r.n_buckets, nullptr, 0, t.offsets, t.keys, t.idx, nullptr, 0,
                                     nullptr});
     } else {
-      uint32_t slot = 0;
-      hg_status hs = reserve_slot(s, &slot);
-      if (hs != HG_OK) return hs;
+      const uint32_t slot = slot0 + n_isect++;
       sr.slot = slot;
       auto it = s->tables.find(r.table_id);
       if (it == s->tables.end()) {
@@ -297,12 +408,17 @@ static hg_status launch_segment(hg_server* s, const QueuedReq* q, size_t n) {
     s->batched_requests += n;
   }
   for (uint64_t id : built) cudaEventRecord(s->tables[id].ready, st);
+  if (isects) {  // missed intersects' slots are zeroed on the device first, so one copy serves all
+    for (const ServerReq& sr : reqs)
+      if (sr.kind == 1 && sr.missed) cudaMemsetAsync(s->d_counts + sr.slot, 0, sizeof(unsigned long long), st);
+    cudaMemcpyAsync(s->h_counts + slot0, s->d_counts + slot0, sizeof(unsigned long long) * isects,
+                    cudaMemcpyDeviceToHost, st);
+  }
+  cudaEvent_t done = take_event(s);  // one completion event for the whole segment
+  cudaEventRecord(done, st);
+  s->event_refs[done] = static_cast<uint32_t>(reqs.size());
   for (ServerReq& sr : reqs) {
-    if (sr.kind == 1 && !sr.missed)
-      cudaMemcpyAsync(s->h_counts + sr.slot, s->d_counts + sr.slot, sizeof(unsigned long long),
-                      cudaMemcpyDeviceToHost, st);
-    sr.done = take_event(s);
-    cudaEventRecord(sr.done, st);
+    sr.done = done;
     s->inflight.push_back(sr);
   }
   return HG_OK;
@@ -329,7 +445,14 @@ static hg_status flush_queue(hg_server* s) {
       }
       j++;
     }
-    st = launch_segment(s, s->queue.data() + i, j - i);
+    if (j - i < BATCH_MIN_REQUESTS) {  // too few to pay for a batch's fixed launches
+      for (size_t k = i; k < j && st == HG_OK; k++) {
+        const QueuedReq& r = s->queue[k];
+        st = r.kind == 0 ? direct_build(s, r, nullptr) : direct_intersect(s, r);
+      }
+    } else {
+      st = launch_segment(s, s->queue.data() + i, j - i);
+    }
     i = j;
   }
   s->queue.clear();
@@ -363,7 +486,13 @@ extern "C" void hg_server_free(hg_server* s) {
     }
     cudaStreamSynchronize(st);
   }
-  for (auto& r : s->inflight) cudaEventDestroy(r.done);
+  {
+    std::vector<cudaEvent_t> evs;
+    for (auto& r : s->inflight) evs.push_back(r.done);
+    std::sort(evs.begin(), evs.end());
+    evs.erase(std::unique(evs.begin(), evs.end()), evs.end());
+    for (auto e : evs) cudaEventDestroy(e);
+  }
   for (auto e : s->free_events) cudaEventDestroy(e);
   if (s->pool) cudaMemPoolDestroy(s->pool);
   for (auto p : s->ws) cudaFree(p);
@@ -481,98 +610,30 @@ extern "C" hg_status hg_server_build(hg_server* s, uint64_t table_id, const void
   if (!s || !ticket || (n > 0 && !d_keys) || n_buckets == 0) return HG_ERR_INVALID_ARGUMENT;
   if (n > s->max_keys || n_buckets > s->max_keys)
     return lib_fail(HG_ERR_TOO_LARGE, "hg_server_build: more keys or buckets than the server's max_keys");
-  if (s->batching && n <= s->batch_small) {
-    *ticket = s->next_ticket++;
-    return enqueue(s, QueuedReq{0, table_id, d_keys, n, n_buckets, with_index, nullptr, 0, arrival_s, *ticket});
-  }
-  if (!s->queue.empty()) {  // queued requests go first
+  *ticket = s->next_ticket++;
+  const QueuedReq r{0, table_id, d_keys, n, n_buckets, with_index, nullptr, 0, arrival_s, *ticket};
+  if (s->batching && n <= s->batch_small) return enqueue(s, r);
+  if (queue_touches(s, table_id)) {  // a queued request on this table goes first
     hg_status qs = flush_queue(s);
     if (qs != HG_OK) return qs;
   }
-  const size_t bytes = (n_buckets + 1) * 4 + n * (s->key_bytes + (with_index ? 4 : 0));
-  if (s->tables.count(table_id)) evict(s, table_id);  // replaced
-  make_room(s, bytes);
-  const int si = pick_stream(s, 20e-6 + double(n) * 4e-11);
-  cudaStream_t st = s->streams[si];
-  ServerTable t;
-  t.n = n;
-  t.n_buckets = n_buckets;
-  t.with_index = with_index != 0;
-  t.bytes = bytes;
-  t.stream = si;
-  cudaError_t e = cudaMallocFromPoolAsync(&t.offsets, (n_buckets + 1) * 4, s->pool, st);
-  if (e == cudaSuccess && n) e = cudaMallocFromPoolAsync(&t.keys, n * s->key_bytes, s->pool, st);
-  if (e == cudaSuccess && n && with_index)
-    e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&t.idx), n * 4, s->pool, st);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t.ready, cudaEventDisableTiming);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    if (t.offsets) cudaFreeAsync(t.offsets, st);
-    if (t.keys) cudaFreeAsync(t.keys, st);
-    if (t.idx) cudaFreeAsync(t.idx, st);
-    return cuda_fail(e, "hg_server_build: table allocation");
-  }
-  hg_status hs = hg_build_into(d_keys, n, s->key_bytes, n_buckets, t.offsets, t.keys, t.idx,
-                               s->ws[si], s->ws_bytes, reinterpret_cast<hg_stream_t>(st));
-  if (hs != HG_OK) {
-    cudaFreeAsync(t.offsets, st);
-    if (t.keys) cudaFreeAsync(t.keys, st);
-    if (t.idx) cudaFreeAsync(t.idx, st);
-    cudaEventDestroy(t.ready);
-    return hs;
-  }
-  cudaEventRecord(t.ready, st);
-  s->lru.push_back(table_id);
-  t.lru = std::prev(s->lru.end());
-  s->bytes += bytes;
-  s->tables.emplace(table_id, t);
-  ServerReq r{s->next_ticket++, 0, 0, arrival_s, take_event(s), 0};
-  cudaEventRecord(r.done, st);
-  s->inflight.push_back(r);
-  *ticket = r.ticket;
-  return HG_OK;
+  std::vector<uint64_t> pinned;  // tables queued intersects will read
+  for (const QueuedReq& q : s->queue) pinned.push_back(q.table_id);
+  return direct_build(s, r, &pinned);
 }
 
 extern "C" hg_status hg_server_intersect(hg_server* s, uint64_t table_id, const void* d_query, uint64_t nq,
                                          uint32_t* d_pairs, uint64_t pair_cap, double arrival_s, uint64_t* ticket) {
   if (!s || !ticket || (nq > 0 && !d_query)) return HG_ERR_INVALID_ARGUMENT;
   if (nq > s->max_keys) return lib_fail(HG_ERR_TOO_LARGE, "hg_server_intersect: more queries than max_keys");
-  if (s->batching && nq <= s->batch_small) {
-    *ticket = s->next_ticket++;
-    return enqueue(s, QueuedReq{1, table_id, d_query, nq, 0, 0, d_pairs, pair_cap, arrival_s, *ticket});
-  }
-  if (!s->queue.empty()) {  // queued requests go first
+  *ticket = s->next_ticket++;
+  const QueuedReq r{1, table_id, d_query, nq, 0, 0, d_pairs, pair_cap, arrival_s, *ticket};
+  if (s->batching && nq <= s->batch_small) return enqueue(s, r);
+  if (queue_touches(s, table_id)) {  // a queued build of this table goes first
     hg_status qs = flush_queue(s);
     if (qs != HG_OK) return qs;
   }
-  uint32_t slot = 0;
-  hg_status hs = reserve_slot(s, &slot);
-  if (hs != HG_OK) return hs;
-  auto it = s->tables.find(table_id);
-  const int si = pick_stream(s, 20e-6 + double(nq) * 4e-11);
-  cudaStream_t st = s->streams[si];
-  ServerReq r{s->next_ticket++, 1, 0, arrival_s, take_event(s), slot};
-  if (it == s->tables.end()) {
-    r.missed = 1;
-  } else {
-    ServerTable& t = it->second;
-    s->lru.splice(s->lru.end(), s->lru, t.lru);  // most recently used
-    cudaStreamWaitEvent(st, t.ready, 0);
-    uint32_t* pairs = d_pairs ? d_pairs : s->pair_buf[si];
-    const uint64_t cap = d_pairs ? pair_cap : std::min<uint64_t>(pair_cap, s->max_keys);
-    hs = hg_intersect_into(t.offsets, t.keys, t.idx, t.n, t.n_buckets, s->key_bytes, d_query, nq, nullptr, pairs, cap,
-                           s->d_counts + slot, s->ws[si], s->ws_bytes, reinterpret_cast<hg_stream_t>(st));
-    if (hs != HG_OK) {
-      s->free_events.push_back(r.done);
-      s->slot_busy[slot] = 0;
-      return hs;
-    }
-    cudaMemcpyAsync(s->h_counts + slot, s->d_counts + slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-  }
-  cudaEventRecord(r.done, st);
-  s->inflight.push_back(r);
-  *ticket = r.ticket;
-  return HG_OK;
+  return direct_intersect(s, r);
 }
 
 extern "C" hg_status hg_server_poll(hg_server* s, int block, hg_server_done* out, int max_out, int* n_out) {
@@ -602,7 +663,11 @@ extern "C" hg_status hg_server_poll(hg_server* s, int block, hg_server_done* out
     d.count = it->kind == 1 && !it->missed ? s->h_counts[it->slot] : 0ull;
     d.latency_s = std::max(0.0, s->ref_host + 1e-3 * double(ms) - it->arrival);
     if (it->kind == 1) s->slot_busy[it->slot] = 0;
-    s->free_events.push_back(it->done);
+    auto ref = s->event_refs.find(it->done);
+    if (ref == s->event_refs.end() || --ref->second == 0) {  // the last request on its event
+      if (ref != s->event_refs.end()) s->event_refs.erase(ref);
+      s->free_events.push_back(it->done);
+    }
     it = s->inflight.erase(it);
   }
   // re-based only when every completed request has been reported against the

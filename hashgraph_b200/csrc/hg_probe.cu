@@ -43,15 +43,20 @@ constexpr uint64_t PROBE_TILE = uint64_t(PROBE_BLOCK) * PROBE_QPT;
 //                  and counts it (a warp per bucket; buckets of more than
 //                  HEAVY_HUGE entries shared by all CTAs in chunks).
 // All copies of a key sit in its bucket, so the counts are exact.  A query
-// whose bucket is long takes its count from the set; if its key is not
-// there, the key has no copy in A -- unless the set filled up (flagged), in
-// which case the query's bucket is scanned.  Buckets of COOP_MIN_LEN entries
-// or more are scanned by the whole warp (32 entries per step, coalesced),
-// shorter ones by the thread.  The count is exact in every case.
+// whose key the set holds takes its count from there without reading its
+// bucket bounds; a key the set does not hold whose bucket is long has no copy
+// in A.  If a key found no slot (the set is not complete: flagged), counting
+// stops and the set is not used: every query scans its bucket.  Buckets of
+// COOP_MIN_LEN entries or more are scanned by the whole warp (32 entries per
+// step, coalesced), shorter ones by the thread.  The count is exact in every
+// case.  Thresholds measured on 2^28 Zipf(1.1) keys over 2^24 (count-only
+// probe + set): long buckets from 64 entries and warp scans from 64, 8.07 +
+// 1.81 ms; from 32 and 8, 5.82 + 1.78 ms; from 16 and 8 with the set looked
+// up before the bounds, 4.90 + 2.05 ms.
 // ---------------------------------------------------------------------------
 constexpr uint32_t HEAVY_PROBES = 32;          // bound on a set lookup / insertion
-constexpr uint32_t HEAVY_MIN_LEN = 64;         // buckets at least this long are counted into the set
-constexpr uint32_t COOP_MIN_LEN = 64;          // buckets at least this long are scanned by a warp
+constexpr uint32_t HEAVY_MIN_LEN = 16;         // buckets at least this long are counted into the set
+constexpr uint32_t COOP_MIN_LEN = 8;           // buckets at least this long are scanned by a warp
 constexpr uint32_t HEAVY_HUGE = 1u << 16;      // longer listed buckets are counted by all CTAs
 constexpr uint32_t HEAVY_HUGE_MAX = 1u << 16;  // listed huge buckets (n_a < 2^32)
 constexpr uint32_t HEAVY_CHUNK = 1u << 14;     // bucket entries per counting work item of a huge bucket
@@ -223,6 +228,8 @@ __global__ void __launch_bounds__(256) k_heavy_count(const KeyT* __restrict__ a_
   const uint32_t n_b = min(*reinterpret_cast<volatile unsigned*>(hs.state), hs.list_cap);
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n_b; c += warps) {
+    // a set that found no slot for a key is not used: stop counting
+    if (__any_sync(FULL_MASK, reinterpret_cast<volatile unsigned*>(hs.state)[3] != 0)) break;
     const uint2 bk = hs.bucket[c];
     heavy_count_range(a_keys, hs, bk.x + lane_id(), bk.y, 32u);
   }
@@ -241,6 +248,7 @@ __global__ void __launch_bounds__(BLOCK) k_heavy_count_huge(const KeyT* __restri
     const uint2 bk = hs.huge[c];
     const uint32_t chunks = (bk.y - bk.x + HEAVY_CHUNK - 1) / HEAVY_CHUNK;
     for (uint32_t j = (blockIdx.x + grid - c % grid) % grid; j < chunks; j += grid) {
+      if (__any_sync(FULL_MASK, reinterpret_cast<volatile unsigned*>(hs.state)[3] != 0)) return;  // set not used
       const uint32_t x0 = bk.x + j * HEAVY_CHUNK;
       heavy_count_range(a_keys, hs, x0 + threadIdx.x, min(bk.y, x0 + HEAVY_CHUNK), uint32_t(BLOCK));
     }
@@ -270,30 +278,42 @@ __global__ void __launch_bounds__(PROBE_BLOCK)
     uint32_t lo[PROBE_QPT], hi[PROBE_QPT];
     uint64_t c = 0;
 #pragma unroll
+    for (int j = 0; j < PROBE_QPT; j++) key[j] = q0 + j < nq ? __ldcs(q + q0 + j) : KeyT(0);
+    // count only: a key a complete heavy-key set holds takes its count from
+    // there and reads no bucket bounds
+    uint32_t resolved = 0;
+    if constexpr (!EMIT) {
+      if (heavy_complete(hs)) {
+#pragma unroll
+        for (int j = 0; j < PROBE_QPT; j++) {
+          const uint32_t h = q0 + j < nq ? heavy_find(hs, key[j]) : ~0u;
+          if (h != ~0u) {
+            c += hs.count[h];
+            resolved |= 1u << j;
+          }
+        }
+      }
+    }
+#pragma unroll
     for (int j = 0; j < PROBE_QPT; j++) {
-      const uint64_t i = q0 + j;
       lo[j] = hi[j] = 0;
-      key[j] = 0;
-      if (i < nq) {
-        key[j] = __ldcs(q + i);
+      if (q0 + j < nq && !((resolved >> j) & 1u)) {
         const uint32_t b = bm.of_key(key[j]);
         lo[j] = a_off[b];
         hi[j] = a_off[b + 1];
       }
     }
     if constexpr (!EMIT) {
-      // count only: keys of long buckets take their count from the set
-      // (absent from a complete set: no copy in A), other long buckets are
-      // scanned by the warp, short ones by the thread
+      // count only, keys the set does not hold: a long bucket of a complete
+      // set has no copy of the key; other long buckets are scanned by the
+      // warp, short ones by the thread
       const bool complete = heavy_complete(hs);
       uint32_t pend = 0, own = 0;
 #pragma unroll
       for (int j = 0; j < PROBE_QPT; j++) {
         const uint32_t len = hi[j] - lo[j];
-        const uint32_t h = len >= HEAVY_MIN_LEN ? heavy_find(hs, key[j]) : ~0u;
-        if (h != ~0u) c += hs.count[h];
-        else if (len >= HEAVY_MIN_LEN && complete && static_cast<unsigned long long>(key[j]) != ~0ull) continue;
-        else if (len >= COOP_MIN_LEN) pend |= 1u << j;
+        if (len >= HEAVY_MIN_LEN && complete && static_cast<unsigned long long>(key[j]) != ~0ull) continue;
+        if (len >= COOP_MIN_LEN) pend |= 1u << j;
         else if (len) own |= 1u << j;
       }
       KeyT first[PROBE_QPT];
@@ -764,7 +784,7 @@ __global__ void __launch_bounds__(CPROBE_BLOCK)
   constexpr int NW = CPROBE_BLOCK / 32;
   constexpr uint32_t TILE = uint32_t(CPROBE_BLOCK) * QPT;
   __shared__ uint64_t red[NW + 1];
-  __shared__ unsigned s_vt[2];
+  __shared__ unsigned s_vt[3];
   const uint32_t tiles_per_part = tpp.d;
   const uint64_t vtiles = uint64_t(n_parts) * tiles_per_part;  // below 2^32 (the planner keeps it so)
   const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
@@ -772,16 +792,40 @@ __global__ void __launch_bounds__(CPROBE_BLOCK)
     if constexpr (A_IDX) return a_idx[x];
     else return x;
   };
+  // 128-byte lines of one tile's query keys (and positions, when emitting)
+  constexpr uint32_t KEY_LINES = TILE * sizeof(KeyT) / 128, POS_LINES = EMIT ? TILE * 4 / 128 : 0;
+  static_assert(KEY_LINES + POS_LINES <= CPROBE_BLOCK, "one prefetch per thread");
   uint64_t counted = 0;
-  // the ticket of iteration i sits in s_vt[i & 1]; thread 0 takes the next
-  // one while the tile is probed, and the barrier that closes the tile
-  // publishes it
-  if (threadIdx.x == 0) s_vt[0] = atomicAdd(ticket, 1u);
+  // tickets are taken a tile ahead: iteration i probes s_vt[i % 3] while its
+  // first KEY_LINES + POS_LINES threads prefetch the query lines of the next
+  // tile (s_vt[(i + 1) % 3]) into L2, and thread 0 takes the ticket after
+  // that; the barrier that closes a tile publishes the ticket taken in it
+  if (threadIdx.x == 0) {
+    s_vt[0] = atomicAdd(ticket, 1u);
+    s_vt[1] = atomicAdd(ticket, 1u);
+  }
   __syncthreads();
+  uint32_t cur = 0;  // it % 3
   for (uint32_t it = 0;; it++) {
-    const uint64_t vt = s_vt[it & 1];
+    const uint64_t vt = s_vt[cur];
     if (vt >= vtiles) break;
-    if (threadIdx.x == 0) s_vt[(it + 1) & 1] = atomicAdd(ticket, 1u);
+    const uint32_t nxt = cur == 2 ? 0 : cur + 1;
+    if (threadIdx.x == 0) s_vt[nxt == 2 ? 0 : nxt + 1] = atomicAdd(ticket, 1u);
+    if (threadIdx.x < KEY_LINES + POS_LINES) {
+      const uint32_t vt2 = s_vt[nxt];
+      if (vt2 < vtiles) {
+        const uint32_t p2 = tpp.div(vt2);
+        const uint32_t line = threadIdx.x < KEY_LINES ? threadIdx.x : threadIdx.x - KEY_LINES;
+        const uint64_t e = uint64_t(vt2 - p2 * tiles_per_part) * TILE +
+                           line * (threadIdx.x < KEY_LINES ? 128 / sizeof(KeyT) : 32);
+        if (e < part_cap) {  // a line that starts inside the partition's slots
+          const void* a = threadIdx.x < KEY_LINES ? static_cast<const void*>(pkeys + uint64_t(p2) * part_cap + e)
+                                                  : static_cast<const void*>(pidx + uint64_t(p2) * part_cap + e);
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+        }
+      }
+    }
+    cur = nxt;
     const uint32_t part32 = tpp.div(static_cast<uint32_t>(vt));
     const uint64_t part = part32;
     const uint32_t r0 = (static_cast<uint32_t>(vt) - part32 * tiles_per_part) * TILE;
@@ -798,11 +842,6 @@ __global__ void __launch_bounds__(CPROBE_BLOCK)
     for (int j = 0; j < QPT; j++) {
       const uint32_t r = r0 + j * CPROBE_BLOCK + threadIdx.x;
       key[j] = r < m ? __ldcs(qk + r) : KeyT(0);
-      // the position is read only at emission, after the tile's scan: bring
-      // its line into L2 now (no register held), so that read waits on L2
-      if constexpr (EMIT) {
-        if (r < m) asm volatile("prefetch.global.L2 [%0];" ::"l"(qi + r));
-      }
     }
 #pragma unroll
     for (int j = 0; j < QPT; j++) {

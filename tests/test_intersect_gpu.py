@@ -235,12 +235,32 @@ def test_intersect_count_absent_keys_in_long_buckets(hg, kb):
 @pytest.mark.parametrize("n_buckets", [1, 64])
 def test_intersect_count_many_long_buckets(hg, n_buckets):
     """Every bucket long, with far more distinct keys in them than the
-    heavy-key set holds (keys that find no slot are scanned by their warp):
-    the count stays exact."""
+    heavy-key set holds: a key finds no slot, the set is not used, and every
+    bucket is scanned by its warp.  The count stays exact."""
     a = (oracle.gen_uniform(1 << 20, 8, 63) % np.uint64(1 << 16)).astype(np.uint64)
     q = (oracle.gen_uniform(1 << 15, 8, 64) % np.uint64(1 << 17)).astype(np.uint64)
     t = hg.Table.build(from_np_u(a), n_buckets, with_index=False)
     count, _ = t.intersect(from_np_u(q), emit=False, path=0)
+    assert int(count.item()) == oracle.join_count(a, q)
+    assert hg.device_error() == 0
+
+
+@pytest.mark.parametrize("probe_path", [0, -1])
+@pytest.mark.parametrize("kb", [4, 8])
+def test_intersect_count_mid_length_buckets(hg, probe_path, kb):
+    """Count only, buckets of 16 to 63 entries (keys with 16 to 48 copies
+    among unique keys): their keys go into the heavy-key set and take their
+    counts from it; queries of unique keys, of keys A lacks, and of
+    duplicated keys all count exactly."""
+    rng = np.random.default_rng(81)
+    uniq = oracle.gen_uniform(1 << 19, kb, 82)
+    dup = oracle.gen_uniform(1 << 13, kb, 83)
+    a = np.concatenate([uniq, np.repeat(dup, rng.integers(16, 49, dup.size))])
+    a = a[rng.permutation(a.size)]
+    absent = oracle.gen_uniform(1 << 14, kb, 84)
+    q = np.concatenate([dup[rng.integers(0, dup.size, 1 << 16)], uniq[: 1 << 15], absent])
+    t = hg.Table.build(from_np_u(a), 1 << 20, with_index=False)
+    count, _ = t.intersect(from_np_u(q), emit=False, path=probe_path)
     assert int(count.item()) == oracle.join_count(a, q)
     assert hg.device_error() == 0
 

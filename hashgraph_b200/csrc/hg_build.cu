@@ -422,14 +422,15 @@ struct TableTiles {
 };
 
 // Before pass 1: SKEW_SAMPLES evenly spaced keys are histogrammed by coarse
-// partition.  A partition whose sampled share, scaled to n, passes four
-// times its slots would overflow for certain, so the overflow flag is set at
-// once: pass 1 and the partitioned kernels then return at entry and the
-// gated direct kernels do the work without a wasted pass (2^28 Zipf keys:
-// 1.2 ms saved on each side of a build + probe).  On a uniform input a
-// partition expects S / n_parts samples (16 at 512 partitions) and reaches
-// four times its slots with a probability below 10^-15; a skew the sample
-// misses still overflows in pass 1, which the fallback handles as before.
+// partition.  A partition whose sampled count passes c + 8 sqrt(c) + 8, c =
+// the samples its slots would hold (cap * S / n), overflows for certain, so
+// the overflow flag is set at once: pass 1 and the partitioned kernels then
+// return at entry and the gated direct kernels do the work without a wasted
+// pass (2^28 Zipf keys: 1.2 ms saved on each side of a build + probe).  A
+// partition that fits its slots draws at most c samples on average (a
+// binomial count; c >= 4 with at most 2048 partitions) and passes the bound
+// with a probability below 10^-10 (Chernoff); a skew the sample misses
+// still overflows in pass 1, which the fallback handles as before.
 constexpr uint32_t SKEW_SAMPLES = 8192;
 constexpr int SKEW_CHECK_BLOCK = 1024;
 
@@ -456,8 +457,10 @@ __global__ void __launch_bounds__(SKEW_CHECK_BLOCK)
     if (x < S && p < n_parts) atomicAdd(&h[p], 1u);
   }
   __syncthreads();
+  const double c = double(cap) * double(S) / double(n);
+  const double bound = c + 8.0 * sqrt(c) + 8.0;
   for (uint32_t j = threadIdx.x; j < n_parts; j += SKEW_CHECK_BLOCK)
-    if (uint64_t(h[j]) * n > 4 * cap * S) atomicOr(flags, FLAG_OVERFLOW);
+    if (double(h[j]) > bound) atomicOr(flags, FLAG_OVERFLOW);
 }
 
 template <typename KeyT, bool WITH_IDX, int BLOCK, int KPT, bool BULK, typename Src>

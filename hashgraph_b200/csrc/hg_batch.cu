@@ -740,8 +740,8 @@ static hg_status batch_plan(const hg_batch_pair* pairs, int n_pairs, int key_byt
     const BatchPairDev& d = (*dev)[i];
     std::fill(lmap->begin() + d.ltile0, lmap->begin() + d.ltile0 + d.ltiles, uint32_t(i));
   }
-  p.smem1b = pass1_smem(p.max_pb, key_bytes);
-  p.smem1q = pass1_smem(p.max_pq, key_bytes);
+  p.smem1b = pass1_smem(p.max_pb, key_bytes, PASS1_TILE);
+  p.smem1q = pass1_smem(p.max_pq, key_bytes, PASS1_TILE);
   mtmap->resize(p.n_mt);
   mqmap->resize(p.n_mq);
   fbmap->resize(p.n_fb);

@@ -464,10 +464,10 @@ __global__ void __launch_bounds__(SKEW_CHECK_BLOCK)
 }
 
 template <typename KeyT, bool WITH_IDX, int BLOCK, int KPT, bool BULK, typename Src>
-__global__ void __launch_bounds__(BLOCK, 2) k_multisplit(Src src, uint32_t max_parts, uint32_t* flags) {
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_multisplit(Src src, uint32_t max_parts, uint32_t* flags) {
   if (entry_skip_on_overflow(flags)) return;
   constexpr uint32_t TILE = BLOCK * KPT;
-  constexpr uint32_t APT = PASS1_APT;
+  constexpr uint32_t APT = PASS1_MAX_PARTS / BLOCK;  // partition reservations per thread and tile
   extern __shared__ __align__(16) unsigned char smem_raw[];
   int64_t* eoff = reinterpret_cast<int64_t*>(smem_raw);  // element offset of sorted position 0, per partition
   uint32_t* hist = reinterpret_cast<uint32_t*>(eoff + max_parts);
@@ -547,7 +547,7 @@ __global__ void __launch_bounds__(BLOCK, 2) k_multisplit(Src src, uint32_t max_p
     }
     __syncthreads();
     // reservations: issued now, consumed after the local scan and sort
-    // (n_parts <= PASS1_APT * BLOCK)
+    // (n_parts <= APT * BLOCK)
     uint32_t g[APT], hh[APT];
 #pragma unroll
     for (uint32_t a = 0; a < APT; a++) {
@@ -1092,8 +1092,8 @@ static uint32_t ceil_log2_u64(uint64_t x) {
   return l;
 }
 
-size_t pass1_smem(uint64_t n_parts, int key_bytes) {
-  return align_up(16 * n_parts, 16) + size_t(PASS1_TILE) * (2 * key_bytes + 6);
+size_t pass1_smem(uint64_t n_parts, int key_bytes, int tile) {
+  return align_up(16 * n_parts, 16) + size_t(tile) * (2 * key_bytes + 6);
 }
 
 size_t split_smem(uint32_t split_log2, int key_bytes, bool with_index, uint64_t n_parts) {
@@ -1193,7 +1193,8 @@ hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_in
   // ranks within a bucket and local bucket numbers are packed in 16 bits
   if (part_ok && (p.g.fine_cap >= 65536 || p.g.fine_log2 > 16)) part_ok = false;
   if (part_ok) {
-    p.g.smem1 = pass1_smem(p.g.n_parts, key_bytes);
+    p.g.tile1 = pass1_tile(key_bytes);
+    p.g.smem1 = pass1_smem(p.g.n_parts, key_bytes, p.g.tile1);
     p.g.smem2 = split_smem(p.g.split_log2, key_bytes, with_index, p.g.n_parts);
     part_ok = p.g.smem1 <= SMEM_BUDGET && p.g.smem2 <= SMEM_BUDGET;
   }
@@ -1270,19 +1271,20 @@ static hg_status launch_pass1(const PartGeometry& g, uint64_t n, const KeyT* key
                               BucketMap bm, uint32_t* pcount, KeyT* pkeys, uint32_t* pidx, uint32_t* flags,
                               const char* name, cudaStream_t s) {
   if (n == 0) return HG_OK;
-  auto kern = k_multisplit<KeyT, WI, PASS1_BLOCK, PASS1_KPT, (V > 1), TableTiles<KeyT, PASS1_TILE>>;
-  const int bps = blocks_per_sm(kern, PASS1_BLOCK, g.smem1);
+  constexpr int BLK = pass1_block(sizeof(KeyT)), TILE = pass1_tile(sizeof(KeyT));
+  auto kern = k_multisplit<KeyT, WI, BLK, PASS1_KPT, (V > 1), TableTiles<KeyT, TILE>>;
+  const int bps = blocks_per_sm(kern, BLK, g.smem1);
   if (bps <= 0) return lib_fail(HG_ERR_CUDA, "multisplit kernel cannot be resident");
-  const uint64_t ntiles = (n + PASS1_TILE - 1) / PASS1_TILE;
+  const uint64_t ntiles = (n + TILE - 1) / TILE;
   const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ntiles, uint64_t(device_sm_count()) * bps));
   Phase ph(s, name);
   count_launch();
   k_skew_check<KeyT><<<1, SKEW_CHECK_BLOCK, 0, s>>>(keys, n, bm, g.coarse_log2, static_cast<uint32_t>(g.n_parts),
                                                     g.part_cap, flags);
   count_launch();
-  using Src = TableTiles<KeyT, PASS1_TILE>;
+  using Src = TableTiles<KeyT, TILE>;
   const Src src{keys, key_idx, n, bm, g.coarse_log2, static_cast<uint32_t>(g.n_parts), g.part_cap, pcount, pkeys, pidx};
-  kern<<<grid, PASS1_BLOCK, g.smem1, s>>>(src, static_cast<uint32_t>(g.n_parts), flags);
+  kern<<<grid, BLK, g.smem1, s>>>(src, static_cast<uint32_t>(g.n_parts), flags);
   HG_CUDA(cudaPeekAtLastError(), "multisplit launch");
   return HG_OK;
 }

@@ -24,12 +24,19 @@ constexpr size_t FINE_SMEM_BUDGET = 100 * 1024;        // pass-3 build CTAs: two
 constexpr size_t FINE_PROBE_SMEM_BUDGET = 220 * 1024;  // pass-3 probe CTAs: one per SM (double-buffered)
 // coarse probe: bytes of the table per bucket range, read from L2 by every CTA at once
 constexpr size_t COARSE_SLICE_BUDGET = size_t(24) << 20;
-constexpr int PASS1_BLOCK = 512;
+constexpr int PASS1_BLOCK = 512;                 // pass-1 CTA for 8-byte keys (and every batch)
 constexpr int PASS1_KPT = 8;                     // pass-1 keys per thread per tile (registers)
 constexpr int PASS1_TILE = PASS1_BLOCK * PASS1_KPT;
-constexpr int PASS1_APT = 4;                     // pass-1 partition reservations per thread and tile
-constexpr uint64_t PASS1_MAX_PARTS = uint64_t(PASS1_APT) * PASS1_BLOCK;
-constexpr uint64_t PASS1_GOOD_PARTS = PASS1_BLOCK;  // one partition per pass-1 thread
+constexpr uint64_t PASS1_MAX_PARTS = 2048;       // coarse partitions pass 1 can reserve runs in
+constexpr uint64_t PASS1_GOOD_PARTS = 512;       // above this many, runs get short and pass 1 slow
+// Pass 1 of a table or a query set: 4-byte keys take one 1024-thread CTA per
+// SM over 8192-key tiles, so that a tile's run in each of 512 partitions is
+// 16 keys (64 bytes per array) instead of 8 (2^30 u32 keys + index: 8.47 ->
+// 5.56 ms for the table, 8.45 -> 5.56 ms for the queries); 8-byte keys keep
+// two 512-thread CTAs over 4096-key tiles (the larger tile measured 1.26 ->
+// 1.31 ms at 2^28 u64, and 1.37 -> 1.51 ms for the queries).
+constexpr int pass1_block(int key_bytes) { return key_bytes == 4 ? 1024 : PASS1_BLOCK; }
+constexpr int pass1_tile(int key_bytes) { return pass1_block(key_bytes) * PASS1_KPT; }
 constexpr int SPLIT_BLOCK = 512;
 constexpr int SPLIT_TILE = 8 * SPLIT_BLOCK;     // k_split sorts a tile in registers: 8 records per thread
 constexpr int FINE_BLOCK = 512;
@@ -116,7 +123,7 @@ bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size
                    size_t stream_smem, uint64_t n_buckets, bool staged_may_spill, PartGeometry* g,
                    size_t fine_budget = FINE_SMEM_BUDGET);
 uint64_t slack_capacity(double mean, uint64_t margin, double sigmas = 8.0);
-size_t pass1_smem(uint64_t n_parts, int key_bytes);
+size_t pass1_smem(uint64_t n_parts, int key_bytes, int tile);
 size_t split_smem(uint32_t split_log2, int key_bytes, bool with_index, uint64_t n_parts);
 
 // Kernel launchers (hg_build.cu / hg_probe.cu).  Workspace pointers are

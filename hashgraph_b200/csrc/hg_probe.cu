@@ -1001,8 +1001,8 @@ static bool plan_coarse(uint64_t nq, uint64_t n_a, size_t a_rec, uint64_t n_buck
   if (g.n_parts > PASS1_MAX_PARTS) return false;
   g.part_cap = slack_capacity(double(nq) * double(std::min<uint64_t>(1ull << c, n_buckets)) / double(n_buckets), 256);
   if (g.part_cap >= (1ull << 32)) return false;
-  g.tile1 = PASS1_TILE;
-  g.smem1 = pass1_smem(g.n_parts, key_bytes);
+  g.tile1 = pass1_tile(key_bytes);
+  g.smem1 = pass1_smem(g.n_parts, key_bytes, g.tile1);
   if (g.smem1 > SMEM_BUDGET) return false;
   *out = g;
   return true;
@@ -1028,7 +1028,8 @@ hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, 
   bool part_ok = plan_geometry(nq, q_rec, n_a, 2 * a_rec, 8, 2 * (key_bytes + (emit ? 4 : 0)), n_buckets, true,
                                &p.g, probe_smem_budget());
   if (part_ok) {
-    p.g.smem1 = pass1_smem(p.g.n_parts, key_bytes);
+    p.g.tile1 = pass1_tile(key_bytes);
+    p.g.smem1 = pass1_smem(p.g.n_parts, key_bytes, p.g.tile1);
     p.g.smem2 = split_smem(p.g.split_log2, key_bytes, true, p.g.n_parts);
     p.g.smem3 = fine_probe_smem(p.g.fine_log2, p.g.smem_cap, p.g.fine_cap, key_bytes, a_idx, emit);
     part_ok = p.g.smem1 <= SMEM_BUDGET && p.g.smem2 <= SMEM_BUDGET && p.g.smem3 <= SMEM_BUDGET;

@@ -1096,9 +1096,22 @@ size_t pass1_smem(uint64_t n_parts, int key_bytes, int tile) {
   return align_up(16 * n_parts, 16) + size_t(tile) * (2 * key_bytes + 6);
 }
 
-size_t split_smem(uint32_t split_log2, int key_bytes, bool with_index, uint64_t n_parts) {
-  return align_up(16 * (size_t(1) << split_log2), 16) +
-         size_t(SPLIT_TILE) * (2 * key_bytes + (with_index ? 8 : 0) + 2) + (n_parts + 1) * 4;
+size_t split_smem(uint32_t split_log2, int key_bytes, bool with_index, uint64_t n_parts, int tile) {
+  return align_up(16 * (size_t(1) << split_log2), 16) + size_t(tile) * (2 * key_bytes + (with_index ? 8 : 0) + 2) +
+         (n_parts + 1) * 4;
+}
+
+// Splits of 512 or 1024 ways take one 1024-thread CTA per SM over 8192-record
+// tiles when that fits in shared memory, so that a tile's run in each fine
+// partition stays 8 or more records long (2^30 u32 keys + index, 1024 ways:
+// the split's runs were 4 records); narrower splits keep 512-thread CTAs.
+void plan_split(PartGeometry& g, int key_bytes, bool with_index) {
+  g.split_block = SPLIT_BLOCK;
+  if (g.split_log2 >= 9) {
+    const size_t wide = split_smem(g.split_log2, key_bytes, with_index, g.n_parts, 8 * SPLIT_BLOCK_WIDE);
+    if (wide <= SMEM_BUDGET) g.split_block = SPLIT_BLOCK_WIDE;
+  }
+  g.smem2 = split_smem(g.split_log2, key_bytes, with_index, g.n_parts, 8 * g.split_block);
 }
 
 bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size_t smem_rec, size_t per_bucket,
@@ -1195,7 +1208,7 @@ hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_in
   if (part_ok) {
     p.g.tile1 = pass1_tile(key_bytes);
     p.g.smem1 = pass1_smem(p.g.n_parts, key_bytes, p.g.tile1);
-    p.g.smem2 = split_smem(p.g.split_log2, key_bytes, with_index, p.g.n_parts);
+    plan_split(p.g, key_bytes, with_index);
     part_ok = p.g.smem1 <= SMEM_BUDGET && p.g.smem2 <= SMEM_BUDGET;
   }
   // the partitioned path pays off with many keys; a sparse table (few keys,
@@ -1313,20 +1326,26 @@ static hg_status run_partition_passes(const PartGeometry& g, uint64_t n, const K
   if (st != HG_OK) return st;
   launch_scan(pcount, g.n_parts, pstatus, ticket + 1, nullptr, pcount + g.n_parts, nullptr, s,
               who[0] == 'b' ? "part_scan" : "probe_part_scan");
-  {
-    auto kern = k_split<KeyT, WI, SPLIT_BLOCK>;
-    const int bps = blocks_per_sm(kern, SPLIT_BLOCK, g.smem2);
+  auto split = [&](auto block_c) -> hg_status {
+    constexpr int BLK = decltype(block_c)::value;
+    auto kern = k_split<KeyT, WI, BLK>;
+    const int bps = blocks_per_sm(kern, BLK, g.smem2);
     if (bps <= 0) return lib_fail(HG_ERR_CUDA, "split kernel cannot be resident");
-    const uint32_t tiles_per_part = static_cast<uint32_t>((g.part_cap + SPLIT_TILE - 1) / SPLIT_TILE);
+    const uint32_t tile = 8 * BLK;
+    const uint32_t tiles_per_part = static_cast<uint32_t>((g.part_cap + tile - 1) / tile);
     const uint64_t vt = g.n_parts * tiles_per_part;
     const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(vt, uint64_t(device_sm_count()) * bps));
     Phase ph(s, who[0] == 'b' ? "split" : "probe_split");
     count_launch();
-    k_split<KeyT, WI, SPLIT_BLOCK><<<std::max(grid, 1u), SPLIT_BLOCK, g.smem2, s>>>(
+    kern<<<std::max(grid, 1u), BLK, g.smem2, s>>>(
         pkeys, pidx, pcount, static_cast<uint32_t>(g.n_parts), g.part_cap, Div32::make(tiles_per_part), bm, g.fine_log2,
         g.split_log2, g.fine_cap, fcount, fkeys, fidx, flags);
     HG_CUDA(cudaPeekAtLastError(), "split launch");
-  }
+    return HG_OK;
+  };
+  st = g.split_block == SPLIT_BLOCK_WIDE ? split(std::integral_constant<int, SPLIT_BLOCK_WIDE>{})
+                                         : split(std::integral_constant<int, SPLIT_BLOCK>{});
+  if (st != HG_OK) return st;
   launch_scan(fcount, g.n_fine, fstatus, ticket + 2, nullptr, fcount + g.n_fine, nullptr, s,
               who[0] == 'b' ? "fine_scan" : "probe_fine_scan");
   return HG_OK;

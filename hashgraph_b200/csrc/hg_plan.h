@@ -39,6 +39,7 @@ constexpr int pass1_block(int key_bytes) { return key_bytes == 4 ? 1024 : PASS1_
 constexpr int pass1_tile(int key_bytes) { return pass1_block(key_bytes) * PASS1_KPT; }
 constexpr int SPLIT_BLOCK = 512;
 constexpr int SPLIT_TILE = 8 * SPLIT_BLOCK;     // k_split sorts a tile in registers: 8 records per thread
+constexpr int SPLIT_BLOCK_WIDE = 1024;
 constexpr int FINE_BLOCK = 512;
 constexpr int FINE_PROBE_BLOCK = 1024;          // one 1024-thread probe CTA per SM
 constexpr uint32_t SPLIT_LOG2_MAX = 8;          // pass 2 splits a coarse partition 256 ways (up to 1024)
@@ -55,6 +56,7 @@ struct PartGeometry {
   uint32_t smem_cap = 0;                // records pass 3 stages in shared memory
   uint32_t tile1 = 0;                   // pass-1 keys per CTA per tile
   size_t smem1 = 0, smem2 = 0, smem3 = 0;
+  int split_block = SPLIT_BLOCK;        // k_split CTA (SPLIT_BLOCK or SPLIT_BLOCK_WIDE threads, 8 records each)
   uint64_t pscan_tiles = 0, fscan_tiles = 0;
 };
 
@@ -124,7 +126,9 @@ bool plan_geometry(uint64_t n_stream, size_t stream_rec, uint64_t n_staged, size
                    size_t fine_budget = FINE_SMEM_BUDGET);
 uint64_t slack_capacity(double mean, uint64_t margin, double sigmas = 8.0);
 size_t pass1_smem(uint64_t n_parts, int key_bytes, int tile);
-size_t split_smem(uint32_t split_log2, int key_bytes, bool with_index, uint64_t n_parts);
+// Sets g.split_block and g.smem2 for a split of g.split_log2 ways.
+void plan_split(PartGeometry& g, int key_bytes, bool with_index);
+size_t split_smem(uint32_t split_log2, int key_bytes, bool with_index, uint64_t n_parts, int tile);
 
 // Kernel launchers (hg_build.cu / hg_probe.cu).  Workspace pointers are
 // already carved by the caller; all launches go to `stream`.

@@ -1030,7 +1030,7 @@ hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, 
   if (part_ok) {
     p.g.tile1 = pass1_tile(key_bytes);
     p.g.smem1 = pass1_smem(p.g.n_parts, key_bytes, p.g.tile1);
-    p.g.smem2 = split_smem(p.g.split_log2, key_bytes, true, p.g.n_parts);
+    plan_split(p.g, key_bytes, true);
     p.g.smem3 = fine_probe_smem(p.g.fine_log2, p.g.smem_cap, p.g.fine_cap, key_bytes, a_idx, emit);
     part_ok = p.g.smem1 <= SMEM_BUDGET && p.g.smem2 <= SMEM_BUDGET && p.g.smem3 <= SMEM_BUDGET;
   }

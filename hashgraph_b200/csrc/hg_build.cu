@@ -421,6 +421,28 @@ struct TableTiles {
   }
 };
 
+// The partitioned build's fallback (gated: runs only after an overflow)
+// first counts the keys of every coarse partition: a shared-memory histogram
+// per CTA, one global add per partition and CTA.
+constexpr int PART_HIST_BLOCK = 512;
+template <typename KeyT>
+__global__ void __launch_bounds__(PART_HIST_BLOCK)
+    k_part_hist(const KeyT* __restrict__ keys, uint64_t n, BucketMap bm, uint32_t shift, uint32_t n_parts,
+                uint32_t* __restrict__ hist, const uint32_t* gate) {
+  if (entry_skip(gate)) return;
+  __shared__ uint32_t h[PASS1_MAX_PARTS];
+  for (uint32_t j = threadIdx.x; j < n_parts; j += PART_HIST_BLOCK) h[j] = 0u;
+  __syncthreads();
+  for (uint64_t i = uint64_t(blockIdx.x) * PART_HIST_BLOCK + threadIdx.x; i < n;
+       i += uint64_t(gridDim.x) * PART_HIST_BLOCK) {
+    const uint32_t p = bm.of_key(__ldcs(keys + i)) >> shift;
+    if (p < n_parts) atomicAdd(&h[p], 1u);
+  }
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j < n_parts; j += PART_HIST_BLOCK)
+    if (h[j]) atomicAdd(hist + j, h[j]);
+}
+
 // Before pass 1: SKEW_SAMPLES evenly spaced keys are histogrammed by coarse
 // partition.  A partition whose sampled count passes c + 8 sqrt(c) + 8, c =
 // the samples its slots would hold (cap * S / n), overflows for certain, so
@@ -463,9 +485,13 @@ __global__ void __launch_bounds__(SKEW_CHECK_BLOCK)
     if (double(h[j]) > bound) atomicOr(flags, FLAG_OVERFLOW);
 }
 
-template <typename KeyT, bool WITH_IDX, int BLOCK, int KPT, bool BULK, typename Src>
+// EXACT: the partitions' counts are known and pcount holds their starts in
+// one flat record array (the fallback after an overflow groups the keys that
+// way, every partition exactly sized): the kernel then runs only while the
+// overflow flag is set, and no run can overflow.
+template <typename KeyT, bool WITH_IDX, int BLOCK, int KPT, bool BULK, typename Src, bool EXACT = false>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_multisplit(Src src, uint32_t max_parts, uint32_t* flags) {
-  if (entry_skip_on_overflow(flags)) return;
+  if (EXACT ? entry_skip(flags) : entry_skip_on_overflow(flags)) return;
   constexpr uint32_t TILE = BLOCK * KPT;
   constexpr uint32_t APT = PASS1_MAX_PARTS / BLOCK;  // partition reservations per thread and tile
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -591,9 +617,13 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_multisplit(Src src, uin
     for (uint32_t a = 0; a < APT; a++) {
       const uint32_t j = a * BLOCK + threadIdx.x;
       if (j < n_parts) {
-        const bool fits = uint64_t(g[a]) + hh[a] <= cap;
-        overflow |= !fits;
-        eoff[j] = fits ? int64_t(j) * int64_t(cap) + int64_t(g[a]) - int64_t(lp[j]) : EOFF_NONE;
+        if constexpr (EXACT) {
+          eoff[j] = int64_t(g[a]) - int64_t(lp[j]);
+        } else {
+          const bool fits = uint64_t(g[a]) + hh[a] <= cap;
+          overflow |= !fits;
+          eoff[j] = fits ? int64_t(j) * int64_t(cap) + int64_t(g[a]) - int64_t(lp[j]) : EOFF_NONE;
+        }
       }
     }
     __syncthreads();
@@ -1062,7 +1092,7 @@ static void launch_scan(uint32_t* data, uint64_t count, uint64_t* status, unsign
 
 template <typename KeyT, int V, bool WI>
 static hg_status run_direct(const BuildPlan& p, const KeyT* keys, uint32_t* offsets, KeyT* keys_out, uint32_t* idx_out,
-                            char* ws, const uint32_t* gate, cudaStream_t s) {
+                            char* ws, const uint32_t* gate, cudaStream_t s, const uint32_t* key_idx) {
   const BucketMap bm = p.bucket_map();
   uint64_t* status = reinterpret_cast<uint64_t*>(ws + p.off_status);
   unsigned* ticket = reinterpret_cast<unsigned*>(ws + p.off_ticket);
@@ -1077,7 +1107,7 @@ static hg_status run_direct(const BuildPlan& p, const KeyT* keys, uint32_t* offs
   HG_CUDA(cudaMemsetAsync(ws + p.off_status, 0, p.off_flags - p.off_status, s), "build: scan state memset");
   if (p.n > 0) launch_direct_count<KeyT, V>(keys, p.n, bm, offsets + 1, gate, s);
   launch_scan(offsets + 1, p.n_buckets, status, ticket, offsets, nullptr, gate, s);
-  if (p.n > 0) launch_direct_scatter<KeyT, V, WI>(keys, p.n, bm, offsets + 1, keys_out, idx_out, p.key_idx, gate, s);
+  if (p.n > 0) launch_direct_scatter<KeyT, V, WI>(keys, p.n, bm, offsets + 1, keys_out, idx_out, key_idx, gate, s);
   return HG_OK;
 }
 
@@ -1225,7 +1255,7 @@ hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_in
   size_t off = 0;
   p.scan_tiles = (n_buckets + SCAN_TILE - 1) / SCAN_TILE;
   p.off_status = off;  off = align_up(off + p.scan_tiles * 8);
-  p.off_ticket = off;  off = align_up(off + 4 * sizeof(unsigned));
+  p.off_ticket = off;  off = align_up(off + 8 * sizeof(unsigned));
   p.off_flags = off;   off = align_up(off + sizeof(uint32_t));
   if (path == BUILD_PARTITIONED) {
     const PartGeometry& g = p.g;
@@ -1233,12 +1263,15 @@ hg_status plan_build(uint64_t n, int key_bytes, uint64_t n_buckets, bool with_in
     p.off_pstatus = off; off = align_up(off + g.pscan_tiles * 8);
     p.off_fcount = off;  off = align_up(off + (g.n_fine + 1) * 4);
     p.off_fstatus = off; off = align_up(off + g.fscan_tiles * 8);
+    p.off_gcount = off;  off = align_up(off + (g.n_parts + 1) * 4);
+    p.off_gstatus = off; off = align_up(off + g.pscan_tiles * 8);
     p.off_pkeys = off;   off = align_up(off + g.n_parts * g.part_cap * key_bytes);
     if (with_index) { p.off_pidx = off; off = align_up(off + g.n_parts * g.part_cap * 4); }
     p.off_fkeys = off;   off = align_up(off + g.n_fine * g.fine_cap * key_bytes);
     if (with_index) { p.off_fidx = off; off = align_up(off + g.n_fine * g.fine_cap * 4); }
   } else {
     p.off_pcount = p.off_pstatus = p.off_fcount = p.off_fstatus = off;
+    p.off_gcount = p.off_gstatus = off;
     p.off_pkeys = p.off_pidx = p.off_fkeys = p.off_fidx = off;
   }
   p.total = std::max<size_t>(off, WS_ALIGN);
@@ -1389,9 +1422,42 @@ static hg_status run_partitioned(const BuildPlan& p, const KeyT* keys, uint32_t*
     if (lst != HG_OK) return lst;
     HG_CUDA(cudaPeekAtLastError(), "fine-build launch");
   }
-  // Fallback for an overflowed partition (heavy duplicates): the direct build,
-  // gated on the flag.
-  return run_direct<KeyT, V, WI>(p, keys, offsets, keys_out, idx_out, ws, flags, s);
+  // Fallback for an overflowed partition (heavy duplicates), gated on the
+  // flag: the keys are first grouped by coarse partition into exactly sized
+  // runs of the partition buffer (a histogram, its scan, pass 1 with exact
+  // starts), then the direct build runs over the grouped keys, so that its
+  // counter and cursor atomics and its key writes stay within the buckets of
+  // the few partitions in flight, which sit in L2.
+  if (p.n == 0) return run_direct<KeyT, V, WI>(p, keys, offsets, keys_out, idx_out, ws, flags, s, p.key_idx);
+  uint32_t* gcount = reinterpret_cast<uint32_t*>(ws + p.off_gcount);
+  uint64_t* gstatus = reinterpret_cast<uint64_t*>(ws + p.off_gstatus);
+  unsigned* ticket = reinterpret_cast<unsigned*>(ws + p.off_ticket);
+  KeyT* gkeys = reinterpret_cast<KeyT*>(ws + p.off_pkeys);
+  uint32_t* gidx = WI ? reinterpret_cast<uint32_t*>(ws + p.off_pidx) : nullptr;
+  {
+    Phase ph(s, "fallback_group_count");
+    count_launch();
+    const unsigned hgrid = static_cast<unsigned>(std::max<uint64_t>(
+        1, std::min<uint64_t>((p.n + PART_HIST_BLOCK - 1) / PART_HIST_BLOCK, uint64_t(device_sm_count()) * 4)));
+    k_part_hist<KeyT><<<hgrid, PART_HIST_BLOCK, 0, s>>>(keys, p.n, bm, g.coarse_log2, static_cast<uint32_t>(g.n_parts),
+                                                         gcount, flags);
+  }
+  launch_scan(gcount, g.n_parts, gstatus, ticket + 4, nullptr, gcount + g.n_parts, flags, s, "fallback_group_scan");
+  {
+    Phase ph(s, "fallback_group");
+    constexpr int BLK = pass1_block(sizeof(KeyT)), TILE = pass1_tile(sizeof(KeyT));
+    auto kern = k_multisplit<KeyT, WI, BLK, PASS1_KPT, (V > 1), TableTiles<KeyT, TILE>, true>;
+    const int bps = blocks_per_sm(kern, BLK, g.smem1);
+    if (bps <= 0) return lib_fail(HG_ERR_CUDA, "multisplit kernel cannot be resident");
+    const uint64_t ntiles = (p.n + TILE - 1) / TILE;
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ntiles, uint64_t(device_sm_count()) * bps));
+    using Src = TableTiles<KeyT, TILE>;
+    const Src src{keys, p.key_idx, p.n, bm, g.coarse_log2, static_cast<uint32_t>(g.n_parts), 0, gcount, gkeys, gidx};
+    count_launch();
+    kern<<<grid, BLK, g.smem1, s>>>(src, static_cast<uint32_t>(g.n_parts), flags);
+    HG_CUDA(cudaPeekAtLastError(), "grouping multisplit launch");
+  }
+  return run_direct<KeyT, 16 / sizeof(KeyT), WI>(p, gkeys, offsets, keys_out, idx_out, ws, flags, s, gidx);
 }
 
 template <typename KeyT, bool WI>
@@ -1405,8 +1471,8 @@ static hg_status dispatch(const BuildPlan& p, const void* keys, uint32_t* offset
     return aligned ? run_partitioned<KeyT, V, WI>(p, k, offsets, ko, idx_out, ws, s)
                    : run_partitioned<KeyT, 1, WI>(p, k, offsets, ko, idx_out, ws, s);
   }
-  return aligned ? run_direct<KeyT, V, WI>(p, k, offsets, ko, idx_out, ws, nullptr, s)
-                 : run_direct<KeyT, 1, WI>(p, k, offsets, ko, idx_out, ws, nullptr, s);
+  return aligned ? run_direct<KeyT, V, WI>(p, k, offsets, ko, idx_out, ws, nullptr, s, p.key_idx)
+                 : run_direct<KeyT, 1, WI>(p, k, offsets, ko, idx_out, ws, nullptr, s, p.key_idx);
 }
 
 hg_status launch_build(const BuildPlan& p, const void* d_keys, uint32_t* d_offsets, void* d_keys_out,

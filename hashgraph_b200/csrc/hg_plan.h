@@ -79,6 +79,7 @@ struct BuildPlan {
   // workspace byte offsets
   size_t off_status = 0, off_ticket = 0, off_flags = 0;
   size_t off_pcount = 0, off_pstatus = 0, off_fcount = 0, off_fstatus = 0;
+  size_t off_gcount = 0, off_gstatus = 0;  // partitioned path's fallback: exact partition counts
   size_t off_pkeys = 0, off_pidx = 0, off_fkeys = 0, off_fidx = 0;
   size_t total = 0;
 };

@@ -78,14 +78,17 @@ inline size_t heavy_bytes(uint64_t n_a) {
 // The set lives in the workspace, zeroed before the probe: a slot holds ~key
 // (0 = empty, so the all-ones 64-bit key is kept out of the set) and its count.
 struct HeavySet {
-  unsigned long long* key;    // [slots] ~key
-  unsigned long long* count;  // [slots] copies in A
+  // [slots][2]: ~key, then the key's copies in A -- one 16-byte slot, so a
+  // found key's count sits in the sector its key was read from
+  unsigned long long* slot;
   uint2* bucket;              // [list_cap] listed buckets {lo, hi} of at most HEAVY_HUGE entries
   uint2* huge;                // [HEAVY_HUGE_MAX] listed longer buckets
   unsigned* state;            // [0] listed buckets, [1] listed huge buckets, [2] a long bucket was
                               // sampled, [3] a key found no slot (the set is not complete)
   uint32_t mask;              // slots - 1
   uint32_t list_cap;
+  __device__ __forceinline__ unsigned long long* key_at(uint32_t h) const { return slot + 2ull * h; }
+  __device__ __forceinline__ unsigned long long* count_at(uint32_t h) const { return slot + 2ull * h + 1; }
 };
 
 __device__ __forceinline__ uint32_t heavy_slot(uint64_t key, uint32_t mask) {
@@ -96,10 +99,10 @@ __device__ __forceinline__ uint32_t heavy_slot(uint64_t key, uint32_t mask) {
 template <typename KeyT>
 __device__ __forceinline__ uint32_t heavy_find(const HeavySet& hs, KeyT key) {
   const unsigned long long stored = ~static_cast<unsigned long long>(key);
-  if (stored == 0 || hs.key == nullptr) return ~0u;
+  if (stored == 0 || hs.slot == nullptr) return ~0u;
   uint32_t h = heavy_slot(static_cast<uint64_t>(key), hs.mask);
   for (uint32_t p = 0; p < HEAVY_PROBES; p++) {
-    const unsigned long long v = hs.key[h];
+    const unsigned long long v = *hs.key_at(h);
     if (v == stored) return h;
     if (v == 0) return ~0u;
     h = (h + 1) & hs.mask;
@@ -115,10 +118,10 @@ __device__ __forceinline__ uint32_t heavy_insert(const HeavySet& hs, KeyT key) {
   if (stored != 0) {
     uint32_t h = heavy_slot(static_cast<uint64_t>(key), hs.mask);
     for (uint32_t p = 0; p < HEAVY_PROBES; p++) {
-      const unsigned long long v = hs.key[h];
+      const unsigned long long v = *hs.key_at(h);
       if (v == stored) return h;
       if (v == 0) {
-        const unsigned long long prev = atomicCAS(hs.key + h, 0ull, stored);
+        const unsigned long long prev = atomicCAS(hs.key_at(h), 0ull, stored);
         if (prev == 0 || prev == stored) return h;
       }
       h = (h + 1) & hs.mask;
@@ -131,7 +134,7 @@ __device__ __forceinline__ uint32_t heavy_insert(const HeavySet& hs, KeyT key) {
 // Whether the set answers for every key of every long bucket (a key it does
 // not hold has no copy in A).
 __device__ __forceinline__ bool heavy_complete(const HeavySet& hs) {
-  if (hs.key == nullptr) return false;
+  if (hs.slot == nullptr) return false;
   const volatile unsigned* st = hs.state;
   return st[2] != 0 && st[3] == 0;
 }
@@ -237,7 +240,7 @@ __device__ __forceinline__ void heavy_count_range(const KeyT* __restrict__ a_key
         have_last = true;
       }
       if (h != run_slot) {
-        if (run) atomicAdd(hs.count + run_slot, run);
+        if (run) atomicAdd(hs.count_at(run_slot), run);
         run_slot = h;
         run = 0;
       }
@@ -247,9 +250,9 @@ __device__ __forceinline__ void heavy_count_range(const KeyT* __restrict__ a_key
   const uint32_t lead_slot = __shfl_sync(FULL_MASK, run_slot, 0);
   if (__all_sync(FULL_MASK, run_slot == lead_slot)) {
     run = warp_sum(run);
-    if (lane_id() == 0 && run) atomicAdd(hs.count + lead_slot, run);
+    if (lane_id() == 0 && run) atomicAdd(hs.count_at(lead_slot), run);
   } else if (run) {
-    atomicAdd(hs.count + run_slot, run);
+    atomicAdd(hs.count_at(run_slot), run);
   }
 }
 
@@ -321,7 +324,7 @@ __global__ void __launch_bounds__(PROBE_BLOCK)
         for (int j = 0; j < PROBE_QPT; j++) {
           const uint32_t h = q0 + j < nq ? heavy_find(hs, key[j]) : ~0u;
           if (h != ~0u) {
-            c += hs.count[h];
+            c += *hs.count_at(h);
             resolved |= 1u << j;
           }
         }
@@ -1082,12 +1085,11 @@ hg_status plan_probe(uint64_t n_a, bool a_idx, uint64_t n_buckets, uint64_t nq, 
 }
 
 static HeavySet heavy_set(const ProbePlan& p, char* ws) {
-  HeavySet hs{nullptr, nullptr, nullptr, nullptr, nullptr, 0u, 0u};
+  HeavySet hs{nullptr, nullptr, nullptr, nullptr, 0u, 0u};
   if (p.emit) return hs;
   const size_t slots = heavy_slots(p.n_a), cap = heavy_list_cap(p.n_a);
   char* h = ws + p.off_heavy;
-  hs.key = reinterpret_cast<unsigned long long*>(h);
-  hs.count = reinterpret_cast<unsigned long long*>(h + slots * 8);
+  hs.slot = reinterpret_cast<unsigned long long*>(h);
   hs.bucket = reinterpret_cast<uint2*>(h + slots * 16);
   hs.huge = reinterpret_cast<uint2*>(h + slots * 16 + cap * 8);
   hs.state = reinterpret_cast<unsigned*>(h + slots * 16 + cap * 8 + size_t(HEAVY_HUGE_MAX) * 8);
@@ -1104,7 +1106,7 @@ static void launch_probe_direct(const ProbePlan& p, const uint32_t* a_off, const
   const BucketMap bm = p.bucket_map();
   if constexpr (!EMIT) {
     // the heavy keys of A (their set was zeroed with the workspace)
-    if (p.n_a > 0 && hs.key != nullptr) {
+    if (p.n_a > 0 && hs.slot != nullptr) {
       Phase ph(s, gate ? "fallback_heavy_keys" : "heavy_keys");
       count_launch();
       k_heavy_find<KeyT><<<HEAVY_SAMPLES / 256, 256, 0, s>>>(a_off, a_keys, p.n_a, bm, hs, gate);

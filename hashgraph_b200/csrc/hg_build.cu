@@ -299,9 +299,11 @@ __global__ void __launch_bounds__(SKEW_BLOCK) k_scatter_skew(const KeyT* __restr
 
 // In-place exclusive scan of data[0..count) (uint32 values, total < 2^32).
 // first_slot (optional) receives 0; total_out (optional) receives the sum.
-// Persistent: each CTA takes tiles in ticket order until none is left.
+// Persistent: each CTA takes tiles in ticket order until none is left.  Four
+// CTAs per SM (64 registers) and the L2 prefetch of the tile one ticket round
+// ahead: 2^28 counts 1.27 -> 1.04 ms.
 template <int BLOCK, int ITEMS>
-__global__ void __launch_bounds__(BLOCK) k_scan_u32(uint32_t* __restrict__ data, uint64_t count,
+__global__ void __launch_bounds__(BLOCK, 4) k_scan_u32(uint32_t* __restrict__ data, uint64_t count,
                                                     uint64_t* __restrict__ status, unsigned* ticket,
                                                     uint32_t* first_slot, uint32_t* total_out,
                                                     const uint32_t* gate) {
@@ -311,12 +313,22 @@ __global__ void __launch_bounds__(BLOCK) k_scan_u32(uint32_t* __restrict__ data,
   __shared__ uint32_t red[BLOCK / 32 + 1];
   __shared__ uint64_t s_tile, s_prefix;
   const uint64_t ntiles = (count + TILE - 1) / TILE;
+  constexpr int LINES = TILE * 4 / 128;  // 128-byte lines of a tile
+  static_assert(LINES <= BLOCK, "one prefetch per thread");
   while (true) {
     if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
     __syncthreads();
     const uint64_t tile = s_tile;
     if (tile >= ntiles) break;
     const uint64_t base = tile * TILE;
+    // the tile a CTA takes about one round of tickets from now (tile +
+    // gridDim.x) is brought into L2 here, so that whoever takes it loads from
+    // L2; no ticket is held ahead, so every look-back still waits only on
+    // tiles that have started
+    if (threadIdx.x < LINES) {
+      const uint64_t e = (tile + gridDim.x) * TILE + uint64_t(threadIdx.x) * 32;
+      if (e < count) asm volatile("prefetch.global.L2 [%0];" ::"l"(data + e));
+    }
 #pragma unroll
     for (int k = 0; k < ITEMS; k++) {
       const int si = k * BLOCK + threadIdx.x;

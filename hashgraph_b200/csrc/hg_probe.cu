@@ -70,7 +70,11 @@ inline uint32_t heavy_slots(uint64_t n_a) {
   while (s < (n_a >> 5) && s < (1ull << 22)) s <<= 1;
   return static_cast<uint32_t>(s);
 }
-inline uint64_t heavy_list_cap(uint64_t n_a) { return n_a / HEAVY_MIN_LEN + 1; }
+// A listed bucket of at most HEAVY_HUGE entries is cut into items of at
+// most HEAVY_ITEM entries, one warp each, so that no warp walks a long bucket
+// alone (at 2^28 Zipf keys the warps' longest buckets set the kernel's time).
+constexpr uint32_t HEAVY_ITEM = 1024;
+inline uint64_t heavy_list_cap(uint64_t n_a) { return n_a / HEAVY_MIN_LEN + n_a / HEAVY_ITEM + 1; }
 inline size_t heavy_bytes(uint64_t n_a) {
   return size_t(heavy_slots(n_a)) * 16 + size_t(heavy_list_cap(n_a)) * 8 + size_t(HEAVY_HUGE_MAX) * 8 + 16;
 }
@@ -81,7 +85,8 @@ struct HeavySet {
   // [slots][2]: ~key, then the key's copies in A -- one 16-byte slot, so a
   // found key's count sits in the sector its key was read from
   unsigned long long* slot;
-  uint2* bucket;              // [list_cap] listed buckets {lo, hi} of at most HEAVY_HUGE entries
+  uint2* bucket;              // [list_cap] listed items {lo, hi}: pieces of at most HEAVY_ITEM entries of the
+                              // buckets of at most HEAVY_HUGE entries
   uint2* huge;                // [HEAVY_HUGE_MAX] listed longer buckets
   unsigned* state;            // [0] listed buckets, [1] listed huge buckets, [2] a long bucket was
                               // sampled, [3] a key found no slot (the set is not complete)
@@ -153,10 +158,11 @@ __global__ void __launch_bounds__(256)
 }
 
 // Lists every bucket of HEAVY_MIN_LEN entries or more (when the sample saw
-// one).  A CTA takes 2048 consecutive buckets at a time (8 per thread); one
-// block scan places its long buckets and one atomic per list reserves their
-// slots (an atomic per long bucket on one counter serialised: 0.78 ms over
-// 2^28 Zipf buckets).
+// one): buckets of at most HEAVY_HUGE entries as items of at most HEAVY_ITEM
+// entries, longer ones whole.  A CTA takes 2048 consecutive buckets at a time
+// (8 per thread); one block scan places its items and one atomic per list
+// reserves their slots (an atomic per long bucket on one counter
+// serialised: 0.78 ms over 2^28 Zipf buckets).
 constexpr int HEAVY_LIST_BLOCK = 256;
 constexpr int HEAVY_LIST_BPT = 8;
 __global__ void __launch_bounds__(HEAVY_LIST_BLOCK)
@@ -171,32 +177,39 @@ __global__ void __launch_bounds__(HEAVY_LIST_BLOCK)
     uint32_t off[HEAVY_LIST_BPT + 1];
 #pragma unroll
     for (int u = 0; u <= HEAVY_LIST_BPT; u++) off[u] = b0 + u <= n_buckets ? a_off[b0 + u] : 0u;
-    uint32_t normal = 0, huge = 0;  // this thread's long buckets (bit u: bucket b0 + u)
+    uint32_t normal = 0, huge = 0, items = 0;  // this thread's long buckets (bit u: bucket b0 + u)
 #pragma unroll
     for (int u = 0; u < HEAVY_LIST_BPT; u++) {
       if (b0 + u < n_buckets) {
         const uint32_t len = off[u + 1] - off[u];
         if (len >= HEAVY_MIN_LEN) {
-          if (len <= HEAVY_HUGE) normal |= 1u << u;
-          else huge |= 1u << u;
+          if (len <= HEAVY_HUGE) {
+            normal |= 1u << u;
+            items += (len + HEAVY_ITEM - 1) / HEAVY_ITEM;
+          } else {
+            huge |= 1u << u;
+          }
         }
       }
     }
-    // both counts in one scan: normal in the low 16 bits, huge in the high
+    // both counts in one scan: items in the low 20 bits (at most 2048 * 64),
+    // huge buckets in the high 12 (at most 2048)
     uint32_t total;
-    const uint32_t excl = block_exclusive_scan<HEAVY_LIST_BLOCK>(
-        uint32_t(__popc(normal)) | (uint32_t(__popc(huge)) << 16), red, &total);
+    const uint32_t excl =
+        block_exclusive_scan<HEAVY_LIST_BLOCK>(items | (uint32_t(__popc(huge)) << 20), red, &total);
     if (threadIdx.x == 0) {
-      s_base[0] = (total & 0xffffu) ? atomicAdd(hs.state, total & 0xffffu) : 0u;
-      s_base[1] = (total >> 16) ? atomicAdd(hs.state + 1, total >> 16) : 0u;
+      s_base[0] = (total & 0xfffffu) ? atomicAdd(hs.state, total & 0xfffffu) : 0u;
+      s_base[1] = (total >> 20) ? atomicAdd(hs.state + 1, total >> 20) : 0u;
     }
     __syncthreads();
-    uint32_t cn = s_base[0] + (excl & 0xffffu), ch = s_base[1] + (excl >> 16);
+    uint32_t cn = s_base[0] + (excl & 0xfffffu), ch = s_base[1] + (excl >> 20);
 #pragma unroll
     for (int u = 0; u < HEAVY_LIST_BPT; u++) {
       if ((normal >> u) & 1u) {
-        if (cn < hs.list_cap) hs.bucket[cn] = make_uint2(off[u], off[u + 1]);
-        cn++;
+        for (uint32_t x = off[u]; x < off[u + 1]; x += HEAVY_ITEM) {
+          if (cn < hs.list_cap) hs.bucket[cn] = make_uint2(x, min(off[u + 1], x + HEAVY_ITEM));
+          cn++;
+        }
       } else if ((huge >> u) & 1u) {
         if (ch < HEAVY_HUGE_MAX) hs.huge[ch] = make_uint2(off[u], off[u + 1]);
         ch++;
@@ -256,7 +269,7 @@ __device__ __forceinline__ void heavy_count_range(const KeyT* __restrict__ a_key
   }
 }
 
-// Listed buckets of at most HEAVY_HUGE entries: one warp each.
+// Listed items (pieces of the buckets of at most HEAVY_HUGE entries): one warp each.
 template <typename KeyT>
 __global__ void __launch_bounds__(256) k_heavy_count(const KeyT* __restrict__ a_keys, HeavySet hs,
                                                      const uint32_t* gate) {

@@ -315,6 +315,7 @@ __global__ void __launch_bounds__(PROBE_BLOCK)
   if (entry_skip(gate)) return;
   __shared__ uint64_t red[PROBE_BLOCK / 32 + 1];
   __shared__ uint64_t s_tile, s_prefix;
+  __shared__ KeyT s_queue[EMIT ? 1 : PROBE_BLOCK / 32][EMIT ? 1 : 32 * PROBE_QPT];  // count only: per-warp queue
   const uint64_t ntiles = (nq + PROBE_TILE - 1) / PROBE_TILE;
   uint64_t counted = 0;
   while (true) {
@@ -328,78 +329,70 @@ __global__ void __launch_bounds__(PROBE_BLOCK)
     uint64_t c = 0;
 #pragma unroll
     for (int j = 0; j < PROBE_QPT; j++) key[j] = q0 + j < nq ? __ldcs(q + q0 + j) : KeyT(0);
-    // count only: a key a complete heavy-key set holds takes its count from
-    // there and reads no bucket bounds
-    uint32_t resolved = 0;
     if constexpr (!EMIT) {
-      if (heavy_complete(hs)) {
+      // count only.  A key a complete heavy-key set holds takes its count
+      // from there and reads no bucket bounds.  The warp's other queries go
+      // through a queue in shared memory and are then taken 32 at a time,
+      // one per lane, so that the bucket work runs once per 32 such queries
+      // rather than once per query slot of every lane.  For a key the set
+      // does not hold, a long bucket of a complete set has no copy of it;
+      // other buckets of COOP_MIN_LEN entries or more are scanned by the
+      // whole warp, shorter ones by the lane.
+      const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+      const bool complete = heavy_complete(hs);
+      KeyT* queue = s_queue[warp];
+      uint32_t n_q = 0;
 #pragma unroll
-        for (int j = 0; j < PROBE_QPT; j++) {
-          const uint32_t h = q0 + j < nq ? heavy_find(hs, key[j]) : ~0u;
+      for (int j = 0; j < PROBE_QPT; j++) {
+        bool need = q0 + j < nq;
+        if (need && complete) {
+          const uint32_t h = heavy_find(hs, key[j]);
           if (h != ~0u) {
             c += *hs.count_at(h);
-            resolved |= 1u << j;
+            need = false;
           }
         }
+        const unsigned b = __ballot_sync(FULL_MASK, need);
+        if (need) queue[n_q + __popc(b & ((1u << lane) - 1u))] = key[j];
+        n_q += __popc(b);
       }
-    }
-#pragma unroll
-    for (int j = 0; j < PROBE_QPT; j++) {
-      lo[j] = hi[j] = 0;
-      if (q0 + j < nq && !((resolved >> j) & 1u)) {
-        const uint32_t b = bm.of_key(key[j]);
-        lo[j] = a_off[b];
-        hi[j] = a_off[b + 1];
-      }
-    }
-    if constexpr (!EMIT) {
-      // count only, keys the set does not hold: a long bucket of a complete
-      // set has no copy of the key; other long buckets are scanned by the
-      // warp, short ones by the thread
-      const bool complete = heavy_complete(hs);
-      uint32_t pend = 0, own = 0;
-#pragma unroll
-      for (int j = 0; j < PROBE_QPT; j++) {
-        const uint32_t len = hi[j] - lo[j];
-        if (len >= HEAVY_MIN_LEN && complete && static_cast<unsigned long long>(key[j]) != ~0ull) continue;
-        if (len >= COOP_MIN_LEN) pend |= 1u << j;
-        else if (len) own |= 1u << j;
-      }
-      KeyT first[PROBE_QPT];
-#pragma unroll
-      for (int j = 0; j < PROBE_QPT; j++) first[j] = (own >> j) & 1u ? a_keys[lo[j]] : KeyT(0);
-#pragma unroll
-      for (int j = 0; j < PROBE_QPT; j++) {
-        if ((own >> j) & 1u) {
-          c += (first[j] == key[j]);
-          for (uint32_t x = lo[j] + 1; x < hi[j]; x++) c += (a_keys[x] == key[j]);
+      __syncwarp();
+      for (uint32_t r = 0; r < n_q; r += 32) {
+        const bool act = r + lane < n_q;
+        const KeyT kq = act ? queue[r + lane] : KeyT(0);
+        uint32_t lo = 0, hi = 0;
+        if (act) {
+          const uint32_t b = bm.of_key(kq);
+          lo = a_off[b];
+          hi = a_off[b + 1];
+        }
+        const uint32_t len = hi - lo;
+        const bool absent = len >= HEAVY_MIN_LEN && complete && static_cast<unsigned long long>(kq) != ~0ull;
+        const bool pend = !absent && len >= COOP_MIN_LEN;
+        if (!absent && !pend)
+          for (uint32_t x = lo; x < hi; x++) c += (a_keys[x] == kq);
+        unsigned who = __ballot_sync(FULL_MASK, pend);
+        while (who) {
+          const int leader = __ffs(who) - 1;
+          who &= who - 1;
+          const KeyT kk = __shfl_sync(FULL_MASK, kq, leader);
+          const uint32_t x0 = __shfl_sync(FULL_MASK, lo, leader), x1 = __shfl_sync(FULL_MASK, hi, leader);
+          for (uint32_t x = x0 + lane; x < x1; x += 32) c += (a_keys[x] == kk);
         }
       }
-      const unsigned lane = lane_id();
-      while (true) {
-        const unsigned who = __ballot_sync(FULL_MASK, pend != 0);
-        if (!who) break;
-        const int leader = __ffs(who) - 1;
-        const int jl = __shfl_sync(FULL_MASK, pend ? __ffs(pend) - 1 : 0, leader);
-        KeyT kk = key[0];
-        uint32_t x0 = lo[0], x1 = hi[0];
-#pragma unroll
-        for (int j = 1; j < PROBE_QPT; j++) {
-          if (jl == j) {
-            kk = key[j];
-            x0 = lo[j];
-            x1 = hi[j];
-          }
-        }
-        if (lane == static_cast<unsigned>(leader)) pend &= pend - 1;
-        kk = __shfl_sync(FULL_MASK, kk, leader);
-        x0 = __shfl_sync(FULL_MASK, x0, leader);
-        x1 = __shfl_sync(FULL_MASK, x1, leader);
-        for (uint32_t x = x0 + lane; x < x1; x += 32) c += (a_keys[x] == kk);
-      }
+      __syncwarp();  // the queue is refilled by the next tile
       counted += c;
       __syncthreads();
     } else {
+#pragma unroll
+      for (int j = 0; j < PROBE_QPT; j++) {
+        lo[j] = hi[j] = 0;
+        if (q0 + j < nq) {
+          const uint32_t b = bm.of_key(key[j]);
+          lo[j] = a_off[b];
+          hi[j] = a_off[b + 1];
+        }
+      }
       // first bucket entries of all the thread's queries are loaded together
       KeyT first[PROBE_QPT];
 #pragma unroll

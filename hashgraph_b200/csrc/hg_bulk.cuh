@@ -69,24 +69,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-// Per-thread asynchronous copy of BYTES (4, 8 or 16; both addresses aligned to
-// BYTES) from global to shared memory (cp.async: no register holds the data
-// while it is in flight).  Only src_bytes are read, the rest of the BYTES is
-// zero-filled (src_bytes = 0: nothing is read).  The issuing thread completes
-// its groups with cp_async_wait<N>(), after which it may read what it copied.
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void* dst, const void* src, uint32_t src_bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES),
-               "r"(src_bytes)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// Waits until at most N of this thread's committed groups are still in flight.
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 // Issues a bulk copy of `bytes` (multiple of 16, both ends 16-byte aligned)
 // from src to dst completing on `bar`; called by one thread.
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {

@@ -445,10 +445,19 @@ __global__ void __launch_bounds__(PART_HIST_BLOCK)
   __shared__ uint32_t h[PASS1_MAX_PARTS];
   for (uint32_t j = threadIdx.x; j < n_parts; j += PART_HIST_BLOCK) h[j] = 0u;
   __syncthreads();
-  for (uint64_t i = uint64_t(blockIdx.x) * PART_HIST_BLOCK + threadIdx.x; i < n;
-       i += uint64_t(gridDim.x) * PART_HIST_BLOCK) {
-    const uint32_t p = bm.of_key(__ldcs(keys + i)) >> shift;
-    if (p < n_parts) atomicAdd(&h[p], 1u);
+  constexpr int PER = 8;  // keys per thread and step, all loaded before any is counted
+  const uint64_t stride = uint64_t(gridDim.x) * PART_HIST_BLOCK;
+  for (uint64_t i0 = uint64_t(blockIdx.x) * PART_HIST_BLOCK + threadIdx.x; i0 < n; i0 += PER * stride) {
+    KeyT k[PER];
+#pragma unroll
+    for (int u = 0; u < PER; u++) k[u] = i0 + u * stride < n ? __ldcs(keys + i0 + u * stride) : KeyT(0);
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+      if (i0 + u * stride < n) {
+        const uint32_t p = bm.of_key(k[u]) >> shift;
+        if (p < n_parts) atomicAdd(&h[p], 1u);
+      }
+    }
   }
   __syncthreads();
   for (uint32_t j = threadIdx.x; j < n_parts; j += PART_HIST_BLOCK)

@@ -293,13 +293,24 @@ __global__ void __launch_bounds__(BLOCK) k_heavy_count_huge(const KeyT* __restri
   if (entry_skip(gate)) return;
   const uint32_t n_b = min(*reinterpret_cast<volatile unsigned*>(hs.state + 1), HEAVY_HUGE_MAX);
   const uint32_t grid = gridDim.x;
-  for (uint32_t c = 0; c < n_b; c++) {
-    const uint2 bk = hs.huge[c];
-    const uint32_t chunks = (bk.y - bk.x + HEAVY_CHUNK - 1) / HEAVY_CHUNK;
-    for (uint32_t j = (blockIdx.x + grid - c % grid) % grid; j < chunks; j += grid) {
-      if (__any_sync(FULL_MASK, reinterpret_cast<volatile unsigned*>(hs.state)[3] != 0)) return;  // set not used
-      const uint32_t x0 = bk.x + j * HEAVY_CHUNK;
-      heavy_count_range(a_keys, hs, x0 + threadIdx.x, min(bk.y, x0 + HEAVY_CHUNK), uint32_t(BLOCK));
+  // the list is read into shared memory BLOCK entries at a time, so the walk
+  // over it waits on no global load per bucket
+  __shared__ uint2 s_huge[BLOCK];
+  bool stop = false;  // a key found no slot: the set is not used (the warp's lanes agree)
+  for (uint32_t c0 = 0; c0 < n_b; c0 += BLOCK) {
+    const uint32_t nb = min(uint32_t(BLOCK), n_b - c0);
+    __syncthreads();  // the previous batch is read
+    if (threadIdx.x < nb) s_huge[threadIdx.x] = hs.huge[c0 + threadIdx.x];
+    __syncthreads();
+    for (uint32_t c = c0; c < c0 + nb; c++) {
+      const uint2 bk = s_huge[c - c0];
+      const uint32_t chunks = (bk.y - bk.x + HEAVY_CHUNK - 1) / HEAVY_CHUNK;
+      for (uint32_t j = (blockIdx.x + grid - c % grid) % grid; j < chunks; j += grid) {
+        if (!stop) stop = __any_sync(FULL_MASK, reinterpret_cast<volatile unsigned*>(hs.state)[3] != 0);
+        if (stop) continue;
+        const uint32_t x0 = bk.x + j * HEAVY_CHUNK;
+        heavy_count_range(a_keys, hs, x0 + threadIdx.x, min(bk.y, x0 + HEAVY_CHUNK), uint32_t(BLOCK));
+      }
     }
   }
 }

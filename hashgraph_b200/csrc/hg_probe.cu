@@ -1127,11 +1127,11 @@ static void launch_probe_direct(const ProbePlan& p, const uint32_t* a_off, const
       Phase ph(s, gate ? "fallback_heavy_keys" : "heavy_keys");
       count_launch();
       k_heavy_find<KeyT><<<HEAVY_SAMPLES / 256, 256, 0, s>>>(a_off, a_keys, p.n_a, bm, hs, gate);
-      const unsigned grid = static_cast<unsigned>(device_sm_count()) * 4;
+      const unsigned grid = static_cast<unsigned>(device_sm_count()) * 8;  // 8 resident 256-thread CTAs per SM
       count_launch();
       constexpr uint64_t LIST_CHUNK = uint64_t(HEAVY_LIST_BLOCK) * HEAVY_LIST_BPT;
       k_heavy_list<<<static_cast<unsigned>(std::min<uint64_t>((p.n_buckets + LIST_CHUNK - 1) / LIST_CHUNK,
-                                                              uint64_t(grid) * 4)),
+                                                              uint64_t(grid) * 2)),
                      HEAVY_LIST_BLOCK, 0, s>>>(a_off, p.n_buckets, hs, gate);
       count_launch();
       k_heavy_count<KeyT><<<grid, 256, 0, s>>>(a_keys, hs, gate);

@@ -55,6 +55,13 @@ class BatchPair(ctypes.Structure):
     ]
 
 
+class ServerRequest(ctypes.Structure):
+    """hg_server_request of include/hashgraph_b200.h."""
+    _fields_ = [("kind", ctypes.c_int), ("with_index", ctypes.c_int), ("table_id", ctypes.c_uint64),
+                ("d_data", ctypes.c_void_p), ("n", ctypes.c_uint64), ("n_buckets", ctypes.c_uint64),
+                ("d_pairs", ctypes.c_void_p), ("pair_cap", ctypes.c_uint64), ("arrival_s", ctypes.c_double)]
+
+
 class ServerDone(ctypes.Structure):
     """hg_server_done of include/hashgraph_b200.h."""
     _fields_ = [("ticket", ctypes.c_uint64), ("kind", ctypes.c_int), ("missed", ctypes.c_int),
@@ -116,6 +123,7 @@ SIGNATURES = {
     "hg_server_reserve": (_i32, [_p, _sz]),
     "hg_server_build": (_i32, [_p, _u64, _p, _u64, _u64, _int, ctypes.c_double, ctypes.POINTER(_u64)]),
     "hg_server_intersect": (_i32, [_p, _u64, _p, _u64, _p, _u64, ctypes.c_double, ctypes.POINTER(_u64)]),
+    "hg_server_submit": (_i32, [_p, ctypes.POINTER(ServerRequest), _int, ctypes.POINTER(_u64), ctypes.POINTER(_int)]),
     "hg_server_poll": (_i32, [_p, _int, ctypes.POINTER(ServerDone), _int, ctypes.POINTER(_int)]),
     "hg_server_set_batching": (_i32, [_p, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double]),
     "hg_server_batch_stats": (_i32, [_p, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),

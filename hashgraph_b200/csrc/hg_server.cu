@@ -27,9 +27,11 @@
 // its oldest request has waited `batch_wait` seconds (checked at every poll),
 // before any request that is launched on its own (so requests keep their
 // order), and when the caller blocks for completions.  A flush is cut into
-// segments of builds followed by intersects, in submission order, so every
-// intersect sees the tables the requests before it left: a build after an
-// intersect, or a second build of one table, starts a new segment.  Each
+// segments in submission order; a batch builds all its tables before it
+// probes, so that every intersect sees the tables the requests before it
+// left, a build starts a new segment when the segment already builds that
+// table or one of its intersects reads it (any other build joins, and the
+// tables the segment's intersects read are kept from eviction).  Each
 // segment takes one stream, waits for the builds (on other streams) of the
 // tables it probes, and uploads its descriptors from a pinned ring buffer
 // without synchronising.
@@ -340,6 +342,7 @@ static hg_status launch_segment(hg_server* s, const QueuedReq* q, size_t n) {
   std::vector<hg_batch_pair> pairs;
   std::vector<ServerReq> reqs;
   std::vector<uint64_t> built;  // table ids this segment builds
+  std::vector<uint64_t> pinned;  // ... and the ids its intersects read: not evicted to make room
   // on failure: the segment's count slots are freed and the tables it
   // registered (never built) are dropped; its requests are not reported
   auto fail = [&](hg_status status) {
@@ -354,8 +357,8 @@ static hg_status launch_segment(hg_server* s, const QueuedReq* q, size_t n) {
     ServerReq sr{r.ticket, r.kind, 0, r.arrival, nullptr, 0};
     if (r.kind == 0) {
       const size_t bytes = (r.n_buckets + 1) * 4 + r.n * (s->key_bytes + (r.with_index ? 4 : 0));
-      if (s->tables.count(r.table_id)) evict(s, r.table_id);  // replaced (not built in this segment)
-      make_room(s, bytes, &built);
+      if (s->tables.count(r.table_id)) evict(s, r.table_id);  // replaced (neither built nor read in this segment)
+      make_room(s, bytes, &pinned);
       ServerTable t;
       t.n = r.n;
       t.n_buckets = r.n_buckets;
@@ -379,11 +382,13 @@ static hg_status launch_segment(hg_server* s, const QueuedReq* q, size_t n) {
       s->bytes += bytes;
       s->tables.emplace(r.table_id, t);
       built.push_back(r.table_id);
+      pinned.push_back(r.table_id);
       pairs.push_back(hg_batch_pair{r.data, r.n, r.n_buckets, nullptr, 0, t.offsets, t.keys, t.idx, nullptr, 0,
                                     nullptr});
     } else {
       const uint32_t slot = slot0 + n_isect++;
       sr.slot = slot;
+      pinned.push_back(r.table_id);
       auto it = s->tables.find(r.table_id);
       if (it == s->tables.end()) {
         sr.missed = 1;
@@ -431,25 +436,38 @@ static hg_status launch_segment(hg_server* s, const QueuedReq* q, size_t n) {
   return HG_OK;
 }
 
-// Launches every queued request, one segment per run of builds followed by
-// intersects (a build after an intersect, or a second build of one table,
-// starts the next segment), at most batch_max requests each.
+// Launches every queued request in segments of at most batch_max requests
+// (a build of a table the segment already builds or reads starts the next
+// one, and so does a request that would take the segment's tables to the
+// table limit or its builds past half the budget).
 static hg_status flush_queue(hg_server* s) {
   size_t i = 0;
   const size_t n = s->queue.size();
   hg_status st = HG_OK;
   while (i < n && st == HG_OK) {
     size_t j = i;
-    bool seen_intersect = false;
-    std::vector<uint64_t> ids;
+    std::vector<uint64_t> builds, reads;
+    size_t pinned = 0, build_bytes = 0;  // distinct tables the segment holds; bytes it builds
+    auto has = [](const std::vector<uint64_t>& v, uint64_t id) { return std::find(v.begin(), v.end(), id) != v.end(); };
     while (j < n && j - i < s->batch_max) {
       const QueuedReq& r = s->queue[j];
+      const bool fresh = !has(builds, r.table_id) && !has(reads, r.table_id);
+      // the tables a segment builds or reads cannot be evicted while it is
+      // planned: it stops short of the table limit and of half the budget
+      if (fresh && j > i && pinned + 1 >= size_t(s->max_tables)) break;
       if (r.kind == 0) {
-        if (seen_intersect || std::find(ids.begin(), ids.end(), r.table_id) != ids.end()) break;
-        ids.push_back(r.table_id);
+        // a batch builds all its tables before it probes: a build joins the
+        // segment unless the segment builds the same table already or one of
+        // its intersects reads that table (it must see the version before)
+        if (!fresh) break;
+        const size_t bytes = (r.n_buckets + 1) * 4 + r.n * (s->key_bytes + (r.with_index ? 4 : 0));
+        if (!builds.empty() && build_bytes + bytes > s->budget / 2) break;
+        build_bytes += bytes;
+        builds.push_back(r.table_id);
       } else {
-        seen_intersect = true;
+        reads.push_back(r.table_id);
       }
+      pinned += fresh;
       j++;
     }
     if (j - i < BATCH_MIN_REQUESTS) {  // too few to pay for a batch's fixed launches
@@ -641,6 +659,25 @@ extern "C" hg_status hg_server_intersect(hg_server* s, uint64_t table_id, const 
     if (qs != HG_OK) return qs;
   }
   return direct_intersect(s, r);
+}
+
+extern "C" hg_status hg_server_submit(hg_server* s, const hg_server_request* reqs, int n, uint64_t* tickets,
+                                      int* n_done) {
+  if (!s || n < 0 || (n > 0 && (!reqs || !tickets)) || !n_done) return HG_ERR_INVALID_ARGUMENT;
+  *n_done = 0;
+  for (int i = 0; i < n; i++) {
+    const hg_server_request& r = reqs[i];
+    hg_status st;
+    if (r.kind == 0)
+      st = hg_server_build(s, r.table_id, r.d_data, r.n, r.n_buckets, r.with_index, r.arrival_s, tickets + i);
+    else if (r.kind == 1)
+      st = hg_server_intersect(s, r.table_id, r.d_data, r.n, r.d_pairs, r.pair_cap, r.arrival_s, tickets + i);
+    else
+      st = lib_fail(HG_ERR_INVALID_ARGUMENT, "hg_server_submit: kind is neither 0 (build) nor 1 (intersect)");
+    if (st != HG_OK) return st;
+    *n_done = i + 1;
+  }
+  return HG_OK;
 }
 
 extern "C" hg_status hg_server_poll(hg_server* s, int block, hg_server_done* out, int max_out, int* n_out) {

@@ -18,7 +18,7 @@ import time
 from dataclasses import dataclass, field
 
 from . import _ptr, check, lib
-from ._capi import ServerDone
+from ._capi import ServerDone, ServerRequest
 
 
 @dataclass
@@ -84,6 +84,34 @@ class Server:
                                         r.arrival, ctypes.byref(t)), "hg_server_intersect")
         r.ticket = t.value
         self._pending[r.ticket] = r
+
+    def submit_many(self, reqs: list[Request]) -> None:
+        """Submits the requests in order with one call into the engine
+        (hg_server_submit): the same as submit() on each, without the host's
+        per-call cost."""
+        if not reqs:
+            return
+        arr = (ServerRequest * len(reqs))()
+        for a, r in zip(arr, reqs):
+            a.arrival_s = r.arrival
+            a.table_id = r.table_id
+            if r.kind == "build":
+                a.kind, a.with_index, a.d_data, a.n = 0, int(r.with_index), r.keys.data_ptr(), r.keys.numel()
+                a.n_buckets = r.n_buckets
+            else:
+                a.kind, a.d_data, a.n = 1, r.queries.data_ptr(), r.queries.numel()
+                if r.pairs is not None:
+                    a.d_pairs = r.pairs.data_ptr()
+                    a.pair_cap = min(r.pair_cap, r.pairs.shape[0])
+                else:
+                    a.pair_cap = r.pair_cap
+        tickets = (ctypes.c_uint64 * len(reqs))()
+        done = ctypes.c_int(0)
+        st = lib().hg_server_submit(self._h, arr, len(reqs), tickets, ctypes.byref(done))
+        for i in range(done.value):
+            reqs[i].ticket = tickets[i]
+            self._pending[tickets[i]] = reqs[i]
+        check(st, "hg_server_submit")
 
     def poll(self, block: bool = False) -> list[Request]:
         """Completed requests (block: wait until at least the oldest one is)."""

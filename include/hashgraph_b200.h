@@ -423,6 +423,25 @@ hg_status hg_server_build(hg_server* server, uint64_t table_id, const void* d_ke
  * one launched on its own). */
 hg_status hg_server_intersect(hg_server* server, uint64_t table_id, const void* d_query, uint64_t nq,
                               uint32_t* d_pairs, uint64_t pair_cap, double arrival_s, uint64_t* ticket);
+/* One request of hg_server_submit. */
+typedef struct hg_server_request {
+  int kind;              /* 0 build, 1 intersect */
+  int with_index;        /* build */
+  uint64_t table_id;
+  const void* d_data;    /* build: the keys; intersect: the queries */
+  uint64_t n;            /* keys or queries */
+  uint64_t n_buckets;    /* build */
+  uint32_t* d_pairs;     /* intersect: as for hg_server_intersect */
+  uint64_t pair_cap;     /* intersect */
+  double arrival_s;
+} hg_server_request;
+/* Submits reqs[0..n) in order, exactly as that many hg_server_build /
+ * hg_server_intersect calls would (one call for a whole arrival burst, so
+ * the host's per-call cost does not bound a saturated server).  Stops at the
+ * first request refused: *n_done gets the requests submitted, tickets[i]
+ * their tickets, and the refusal's status is returned. */
+hg_status hg_server_submit(hg_server* server, const hg_server_request* reqs, int n, uint64_t* tickets,
+                           int* n_done);
 /* Reports up to max_out completed requests (block: wait for the oldest). */
 hg_status hg_server_poll(hg_server* server, int block, hg_server_done* out, int max_out, int* n_out);
 hg_status hg_server_stats(const hg_server* server, uint64_t* resident_tables, size_t* resident_bytes,

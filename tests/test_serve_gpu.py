@@ -96,6 +96,50 @@ def _served_specs(n_req, seed):
     return specs
 
 
+def test_submit_many_equals_submit(hg):
+    """hg_server_submit (one call for a burst) serves the same requests as
+    one hg_server_build / hg_server_intersect call each: identical counts
+    and pairs, the same misses."""
+    import numpy as np
+    import torch
+
+    import oracle
+    from hashgraph_b200.serve import Request, Server, now
+    from tests.conftest import to_np_u
+    arena_h = oracle.gen_uniform(1 << 20, 8, 41)
+    arena = torch.from_numpy(arena_h.view(np.int64)).cuda()
+    specs = _served_specs(200, 43)
+
+    def make(sp):
+        kind, tid, off, size = sp
+        sl = arena[off:off + size]
+        if kind == "build":
+            return Request("build", tid, now(), keys=sl, n_buckets=size, with_index=True)
+        return Request("intersect", tid, now(), queries=sl, pair_cap=size,
+                       pairs=torch.full((size, 2), -1, dtype=torch.int32, device="cuda"))
+
+    torch.cuda.synchronize()
+    results = []
+    for many in (False, True):
+        srv = Server(budget_bytes=1 << 30, max_tables=64, n_streams=4, max_keys=1 << 15)
+        reqs = [make(sp) for sp in specs]
+        if many:
+            srv.submit_many(reqs)
+        else:
+            for r in reqs:
+                srv.submit(r)
+        srv.drain()
+        out = []
+        for r in reqs:
+            if r.kind == "intersect":
+                p = to_np_u(r.pairs[:r.count], 4).astype(np.uint64)
+                out.append((r.count, r.missed, np.sort(p[:, 0] << 32 | p[:, 1]).tobytes()))
+        results.append(out)
+        srv.free()
+    assert results[0] == results[1] and len(results[0]) > 50
+    assert hg.device_error() == 0
+
+
 def test_served_pairs_equal_oracle_and_alone(hg):
     """Saturated load: every request submitted at once, so the engine
     coalesces them into batched launches (continuous batching).  Each served

@@ -163,6 +163,11 @@ def test_server_argument_checks_without_device(capi):
     assert L.hg_server_build(None, 0, None, 0, 1, 0, 0.0, ctypes.byref(t)) == -1
     assert L.hg_server_intersect(None, 0, None, 0, None, 0, 0.0, ctypes.byref(t)) == -1
     assert L.hg_server_poll(None, 0, None, 0, ctypes.byref(n)) == -1
+    from hashgraph_b200._capi import ServerRequest
+    reqs = (ServerRequest * 1)()
+    tick = (ctypes.c_uint64 * 1)()
+    assert L.hg_server_submit(None, reqs, 1, tick, ctypes.byref(n)) == -1
+    assert L.hg_server_submit(None, None, 0, None, None) == -1
     assert L.hg_server_stats(None, None, None, None, None) == -1
     assert L.hg_server_reserve(None, 1 << 20) == -1
     L.hg_server_free(None)

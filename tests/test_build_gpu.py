@@ -68,6 +68,35 @@ def test_build_zipf(hg, path):
     _check_table(t, keys, 1 << 18, True)
 
 
+@pytest.mark.parametrize("kb", [4, 8])
+def test_build_zipf_grouped_fallback(hg, kb):
+    """Partitioned build of skewed keys with an index: the skew check flags
+    the overflow before pass 1 and the fallback groups the keys by coarse
+    partition into exactly sized runs before its direct build."""
+    cdf = oracle.zipf_cdf(1 << 16, 1.1)
+    n = 1 << 22
+    keys = oracle.gen_zipf(n, kb, cdf, 17)
+    t = hg.Table.build(from_np_u(keys), n, with_index=True, path=1)
+    _check_table(t, keys, n, True)
+    assert hg.device_error() == 0
+
+
+def test_build_late_overflow_grouped_fallback(hg):
+    """A partition a little over its slots: the 8192-key sample does not flag
+    it, pass 1 overflows, and the fallback (grouping, then the direct build)
+    redoes the table from the input."""
+    n = B = 1 << 22
+    base = oracle.gen_uniform(n, 8, 23)
+    extra = oracle.gen_uniform(1 << 18, 8, 24)
+    # about 2% more keys in the first of the 8 coarse partitions (2^19 buckets)
+    extra = extra[oracle.buckets(extra, B) < (1 << 19)][:10_000]
+    keys = np.concatenate([base[: n - extra.size], extra])
+    keys = keys[np.random.default_rng(25).permutation(keys.size)]
+    t = hg.Table.build(from_np_u(keys), B, with_index=True, path=1)
+    _check_table(t, keys, B, True)
+    assert hg.device_error() == 0
+
+
 def test_build_unaligned_input(hg):
     """Keys that do not start on a 16-byte boundary take the scalar-load path."""
     import torch

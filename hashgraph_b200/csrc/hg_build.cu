@@ -232,6 +232,7 @@ __global__ void __launch_bounds__(SKEW_BLOCK) k_scatter_skew(const KeyT* __restr
     s_c[i] = 0;
   }
   __syncthreads();
+  const unsigned lane = lane_id();
   for (uint64_t base = uint64_t(blockIdx.x) * SKEW_CHUNK; base < n; base += uint64_t(gridDim.x) * SKEW_CHUNK) {
     KeyT k[SKEW_KPT];
     uint32_t where[SKEW_KPT];  // slot << 16 | rank, or the position taken by a global atomic
@@ -239,16 +240,30 @@ __global__ void __launch_bounds__(SKEW_BLOCK) k_scatter_skew(const KeyT* __restr
 #pragma unroll
     for (int u = 0; u < SKEW_KPT; u++) {
       const uint64_t i = base + uint64_t(u) * SKEW_BLOCK + threadIdx.x;
-      k[u] = KeyT(0);
+      k[u] = i < n ? __ldcs(keys + i) : KeyT(0);
+    }
+#pragma unroll
+    for (int u = 0; u < SKEW_KPT; u++) {
+      // the warp's lanes with the same bucket take consecutive ranks: their
+      // lowest lane claims the slot and reserves the group's ranks at once
+      const bool valid = base + uint64_t(u) * SKEW_BLOCK + threadIdx.x < n;
+      const uint32_t b = valid ? bm.of_key(k[u]) : 0u;
+      const unsigned peers = __match_any_sync(FULL_MASK, valid ? uint64_t(b) : (1ull << 40));
+      const unsigned leader = __ffs(peers) - 1;
+      uint32_t h = SKEW_SLOTS, first = 0;
+      if (valid && lane == leader) {
+        h = skew_place(s_b, b);
+        first = h < SKEW_SLOTS ? atomicAdd(s_c + h, uint32_t(__popc(peers)))
+                               : atomicAdd(cursor + b, uint32_t(__popc(peers)));
+      }
+      h = __shfl_sync(FULL_MASK, h, leader);
+      first = __shfl_sync(FULL_MASK, first, leader) + __popc(peers & lanemask_lt());
       where[u] = 0;
-      if (i < n) {
-        k[u] = __ldcs(keys + i);
-        const uint32_t b = bm.of_key(k[u]);
-        const uint32_t h = skew_place(s_b, b);
+      if (valid) {
         if (h < SKEW_SLOTS) {
-          where[u] = (h << 16) | atomicAdd(s_c + h, 1u);
+          where[u] = (h << 16) | first;
         } else {
-          where[u] = atomicAdd(cursor + b, 1u);
+          where[u] = first;
           direct |= 1u << u;
         }
       }

@@ -192,12 +192,23 @@ __global__ void __launch_bounds__(SKEW_BLOCK) k_count_skew(const KeyT* __restric
     s_c[i] = 0;
   }
   __syncthreads();
+  const unsigned lane = lane_id();
   for (uint64_t base = uint64_t(blockIdx.x) * SKEW_CHUNK; base < n; base += uint64_t(gridDim.x) * SKEW_CHUNK) {
 #pragma unroll
     for (int u = 0; u < SKEW_KPT; u++) {
       const uint64_t i = base + uint64_t(u) * SKEW_BLOCK + threadIdx.x;
-      if (i < n) {
-        const uint32_t b = bm.of_key(__ldcs(keys + i));
+      const bool valid = i < n;
+      const uint32_t b = valid ? bm.of_key(__ldcs(keys + i)) : 0u;
+      // a warp whose 32 keys share one bucket (a hot key's run in grouped
+      // input) counts them with one atomic; other warps key by key
+      const uint32_t b0 = __shfl_sync(FULL_MASK, b, 0);
+      if (__all_sync(FULL_MASK, valid && b == b0)) {
+        if (lane == 0) {
+          const uint32_t h = skew_place(s_b, b0);
+          if (h < SKEW_SLOTS) atomicAdd(s_c + h, 32u);
+          else atomicAdd(cnt + b0, 32u);
+        }
+      } else if (valid) {
         const uint32_t h = skew_place(s_b, b);
         if (h < SKEW_SLOTS) atomicAdd(s_c + h, 1u);
         else atomicAdd(cnt + b, 1u);

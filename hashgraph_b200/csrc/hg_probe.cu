@@ -824,7 +824,7 @@ __global__ void __launch_bounds__(BLOCK)
 // pair count reserve a tile's output; pairs come out grouped by tile (no
 // query order).  The kernel waits on L2 reads (bucket bounds and entries,
 // about two sectors per query), not on HBM.
-constexpr int CPROBE_BLOCK = 256;  // 512 and 1024 measured slower (3.50, 3.75 against 3.36 ms)
+constexpr int CPROBE_BLOCK = 128;  // 256 / 512 / 1024 measured slower (3.10, 3.50, 3.75 ms against 3.00 at 2^28)
 
 template <typename KeyT, bool EMIT, bool A_IDX, int QPT>
 __global__ void __launch_bounds__(CPROBE_BLOCK)

@@ -126,7 +126,7 @@ class ClockSampler:
 MEASURED_TRAFFIC_PER_KEY = {
     (8, False): {"multisplit": 14.5, "split": 14.4, "fine_build": 18.5,
                  "probe_multisplit": 18.3, "probe_split": 22.4, "fine_probe_emit": 25.8,
-                 "coarse_probe_emit": 26.2},
+                 "coarse_probe_emit": 26.1},
 }
 
 

@@ -17,20 +17,26 @@
 // Partitioned (large tables; replaces the LRB locality pass
 // lrbCountHashD/lrbRehashD/lrbCountHashGlobalD/lrbCopyToGraphD,
 // include/SingleHashGraphOperators.cuh:102-154, and the 1-GPU multi pipeline):
-//   1. k_multisplit: tiles of 4096 keys per CTA are ranked per coarse
-//                 partition (2^coarse_log2 buckets) in shared memory, one
-//                 global atomic per (tile, partition) reserves the run, and
-//                 the tile leaves partition-sorted as coalesced runs.
+//   0. k_skew_check: 8192 sampled keys; a partition certain to overflow
+//                 sets the overflow flag before any pass runs.
+//   1. k_multisplit: tiles of 4096 keys (8-byte keys) or 8192 keys (4-byte
+//                 keys) per CTA are ranked per coarse partition
+//                 (2^coarse_log2 buckets) in shared memory, one global atomic
+//                 per (tile, partition) reserves the run, and the tile leaves
+//                 partition-sorted as coalesced runs.
 //   2. k_scan_u32 over the coarse partition sizes.
-//   3. k_split:   each coarse partition is split up to 256 ways into fine
-//                 partitions of W = 2^fine_log2 buckets the same way.
+//   3. k_split:   each coarse partition is split 256 ways (up to 1024) into
+//                 fine partitions of W = 2^fine_log2 buckets the same way.
 //   4. k_scan_u32 over the fine partition sizes.
 //   5. k_fine_build: one CTA per fine partition: bucket histogram in shared
 //                 memory, segmented block scan, coalesced offsets write, then
 //                 the scatter of the partition's keys into its output slice.
 //   If any partition overflowed its slot range (heavy duplicates), pass 5
-//   stands down and gated copies of the direct kernels rebuild the table;
-//   the decision is taken on the device, so the launch sequence is fixed.
+//   stands down and a gated fallback rebuilds the table: the keys grouped by
+//   coarse partition into exactly sized runs (k_part_hist, a scan,
+//   k_multisplit in exact mode), then the direct kernels over the grouped
+//   keys.  The decision is taken on the device, so the launch sequence is
+//   fixed.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>

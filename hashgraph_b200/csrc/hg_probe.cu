@@ -8,9 +8,19 @@
 //
 // Here every query key is hashed to its bucket in A, the bucket range is
 // scanned for equal keys, and the matches are counted and emitted in ONE
-// pass: each tile of queries counts its matches, takes its output offset from
-// the decoupled look-back over tiles, and writes its pairs in query order.
-// The count-only form skips the look-back and adds tile sums atomically.
+// pass.  Three forms:
+//   direct (k_probe): each tile of queries counts its matches, takes its
+//     output offset from the decoupled look-back over tiles, and writes its
+//     pairs in query order; the count-only form skips the look-back, first
+//     looks keys up in the set of A's long-bucket keys (skew) and sends the
+//     rest through a per-warp queue;
+//   coarse (k_multisplit over the queries, then k_coarse_probe): the queries
+//     grouped by L2-sized bucket ranges of A and probed from L2 -- the
+//     default for large probes;
+//   partitioned (pass 1, k_split, k_fine_probe): both sides staged in shared
+//     memory per fine partition.
+// The partitioned forms fall back to a gated direct probe when a query
+// partition overflows (heavy duplicates among the queries).
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
